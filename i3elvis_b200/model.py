@@ -1,0 +1,346 @@
+"""Synthetic model builder: grid, seeded markers, rock types and boundary conditions.
+
+This writes the same kind of restart image that the reference's initial-condition
+generator produces (``in3mg.c:25-1055``), for the synthetic workloads used by the tests
+and the benchmark:
+
+* grid lines ``gx, gy, gz`` uniform as in ``in3mg.c:96-101`` (stored as FP32 like the
+  ``.prn`` writer does),
+* markers on a regular sub-grid per cell, cell-major order, jittered by
+  ``(r % (2n+1) - n)/n * frac * spacing`` as in ``in3mg.c:131-187`` (``r`` from a seeded
+  generator instead of unseeded ``rand()``),
+* boundary-condition boxes expanded onto every multigrid level with the index mapping of
+  ``in3mg.c:313-408``,
+* the multigrid level geometry of ``gridcheck`` (``load3mg.c:1162-1283``).
+
+Nodal fields are left at zero; ``prepare`` in the runtime fills them from the markers the
+way ``in3mg.c:990-1031`` does (marker->node average, hydrostatic pressure, average again).
+The vertical axis is the reference's ``y`` (gravity ``GYKOEF`` > 0 points to larger y).
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+from .prn import Prn, ROCK_FIELDS, empty_bond
+
+
+def level_dims(n0: int, multinum: int):
+    """``mgx[n]=((mgx[n-1]-5)/2)+5`` (``load3mg.c:1228``)."""
+    dims = [n0]
+    for _ in range(multinum):
+        dims.append((dims[-1] - 5) // 2 + 5)
+    return dims
+
+
+def level_coords(g: np.ndarray, multinum: int):
+    """Per-level grid coordinates keeping 3 outer nodes per side (``load3mg.c:1235-1282``)."""
+    g = np.asarray(g, np.float64)
+    n = g.size
+    out = []
+    for lev, m in enumerate(level_dims(n, multinum)):
+        s = 1 << lev
+        c = np.empty(m)
+        c[0:3] = g[0:3]
+        c[m - 3:] = g[n - 3:]
+        for i in range(3, m - 3):
+            c[i] = g[(i - 2) * s + 2]
+        out.append(c)
+    return out
+
+
+@dataclasses.dataclass
+class BcBox:
+    """One boundary-condition box: ``var`` is P, Vx, Vy, Vz or T; the row is
+    ``x_i = c + k * x_(i+shift)`` over the inclusive node box (``in3mg.c:266-300``)."""
+    var: str
+    x0: int
+    x1: int
+    y0: int
+    y1: int
+    z0: int
+    z1: int
+    c: float = 0.0
+    k: float = 0.0
+    shift: tuple = (0, 0, 0)
+
+
+_VAR_INDEX = {"P": 0, "Vx": 1, "Vy": 2, "Vz": 3, "T": 4}
+
+
+def free_slip_boxes(nx, ny, nz, t_top, t_bottom):
+    """Free-slip box with fixed top/bottom temperature and insulating sides.
+
+    Same box list as the reference specimen's boundary block (``init.t3c:132-168``) with
+    the internal box removed, free slip (``k=1``) on the bottom too and no flow through
+    the bottom wall."""
+    x, y, z = nx - 1, ny - 1, nz - 1
+    B = BcBox
+    boxes = []
+    for yy, s in ((1, None), (y, None)):
+        boxes += [B("P", 1, x, yy, yy, 1, 1, 0, 1, (0, 0, 1)),
+                  B("P", 1, 1, yy, yy, 2, z - 1, 0, 1, (1, 0, 0)),
+                  B("P", 1, x, yy, yy, z, z, 0, 1, (0, 0, -1)),
+                  B("P", x, x, yy, yy, 2, z - 1, 0, 1, (-1, 0, 0))]
+        if yy == 1:
+            boxes += [B("Vx", 1, x - 1, 0, 0, 0, z - 1, 0, 1, (0, 1, 0)),
+                      B("Vy", 0, x - 1, 0, 0, 0, z - 1, 0, 0),
+                      B("Vz", 0, x - 1, 0, 0, 1, z - 1, 0, 1, (0, 1, 0)),
+                      B("T", 0, x, 0, 0, 0, z, t_top, 0)]
+        else:
+            boxes += [B("Vx", 1, x - 1, y - 1, y - 1, 0, z - 1, 0, 1, (0, -1, 0)),
+                      B("Vy", 0, x - 1, y, y, 0, z - 1, 0, 0),
+                      B("Vz", 0, x - 1, y - 1, y - 1, 1, z - 1, 0, 1, (0, -1, 0)),
+                      B("T", 0, x, y, y, 0, z, t_bottom, 0)]
+    boxes += [B("P", 1, 1, 2, y - 1, 1, 1, 0, 1, (1, 0, 1)),
+              B("P", 1, 1, 2, y - 1, z, z, 0, 1, (1, 0, -1)),
+              B("Vx", 0, 0, 0, y - 1, 0, z - 1, 0, 0),
+              B("Vy", 0, 0, 1, y - 1, 0, z - 1, 0, 1, (1, 0, 0)),
+              B("Vz", 0, 0, 0, y - 1, 1, z - 1, 0, 1, (1, 0, 0)),
+              B("T", 0, 0, 1, y - 1, 0, z, 0, 1, (1, 0, 0))]
+    boxes += [B("P", x, x, 2, y - 1, 1, 1, 0, 1, (-1, 0, 1)),
+              B("P", x, x, 2, y - 1, z, z, 0, 1, (-1, 0, -1)),
+              B("Vx", x, x, 0, y - 1, 0, z - 1, 0, 0),
+              B("Vy", x - 1, x - 1, 1, y - 1, 0, z - 1, 0, 1, (-1, 0, 0)),
+              B("Vz", x - 1, x - 1, 0, y - 1, 1, z - 1, 0, 1, (-1, 0, 0)),
+              B("T", x, x, 1, y - 1, 0, z, 0, 1, (-1, 0, 0))]
+    boxes += [B("Vx", 1, x - 1, 0, y - 1, 0, 0, 0, 1, (0, 0, 1)),
+              B("Vy", 0, x - 1, 1, y - 1, 0, 0, 0, 1, (0, 0, 1)),
+              B("Vz", 0, x - 1, 0, y - 1, 0, 0, 0, 0),
+              B("T", 1, x - 1, 1, y - 1, 0, 0, 0, 1, (0, 0, 1))]
+    boxes += [B("Vx", 1, x - 1, 0, y - 1, z - 1, z - 1, 0, 1, (0, 0, -1)),
+              B("Vy", 0, x - 1, 1, y - 1, z - 1, z - 1, 0, 1, (0, 0, -1)),
+              B("Vz", 0, x - 1, 0, y - 1, z, z, 0, 0),
+              B("T", 1, x - 1, 1, y - 1, z, z, 0, 1, (0, 0, -1))]
+    return boxes
+
+
+def _lim(m, n, mg, s):
+    """Fine box limit -> level limit (``in3mg.c:319-336``); C division truncates toward 0."""
+    if m < 3:
+        return m
+    if m > n - 4:
+        return mg - (n - m)
+    return int((m - 2) / s) + 2
+
+
+def expand_bc(boxes, shape, multinum):
+    """Expand BC boxes onto all multigrid levels (``in3mg.c:313-408``).
+
+    Returns the ``.prn`` boundary records sorted by row: ``row`` indexes ``bondm``
+    (``4*node + var`` for P/Vx/Vy/Vz, ``8*nodenum + node`` for T, node numbers counting
+    all levels), ``partner1`` is the partner row + 1 (0 = none)."""
+    nx, ny, nz = shape
+    dx, dy, dz = (level_dims(n, multinum) for n in shape)
+    nodenum = nx * ny * nz
+    mgp = [0]
+    for l in range(multinum):
+        mgp.append(mgp[-1] + dx[l] * dy[l] * dz[l])
+    bondm = {}
+    vals = {}
+    bid = 0
+    for b in boxes:
+        var = _VAR_INDEX[b.var]
+        has_shift = any(b.shift)
+        for l in range(multinum + 1):
+            s = 1 << l
+            x0, x1 = _lim(b.x0, nx, dx[l], s), _lim(b.x1, nx, dx[l], s)
+            y0, y1 = _lim(b.y0, ny, dy[l], s), _lim(b.y1, ny, dy[l], s)
+            z0, z1 = _lim(b.z0, nz, dz[l], s), _lim(b.z1, nz, dz[l], s)
+            mgy, mgxy = dy[l], dx[l] * dy[l]
+            for k3 in range(z0, z1 + 1):
+                for k1 in range(x0, x1 + 1):
+                    for k2 in range(y0, y1 + 1):
+                        m4 = mgp[l] + k3 * mgxy + k1 * mgy + k2
+                        m6 = m4 + b.shift[2] * mgxy + b.shift[0] * mgy + b.shift[1]
+                        bid += 1
+                        if var < 4:
+                            row = m4 * 4 + var
+                            partner1 = m6 * 4 + var + 1 if has_shift else 0
+                        else:
+                            row = 8 * nodenum + m4
+                            partner1 = m6 + 1 if has_shift else 0
+                        bondm[row] = bid
+                        vals[bid] = (b.c, b.k if has_shift else 0.0, partner1)
+    rows = sorted(bondm)
+    bond = empty_bond(len(rows))
+    for i, r in enumerate(rows):
+        c, k, p1 = vals[bondm[r]]
+        bond[i] = (r, bondm[r], c, k, p1)
+    return bond
+
+
+@dataclasses.dataclass
+class Rock:
+    """One rock type (columns of the reference's rock table, ``in3mg.c:201-234``)."""
+    n0: float = 1e18
+    n1: float = 1e26
+    s0: float = 0.0
+    s1: float = 5e29
+    nu: float = 1e21
+    dh: float = 0.0
+    dv: float = 0.0
+    ss: float = 0.0
+    mm: float = 1.0
+    ll: float = 0.0
+    a0: float = 0.0
+    a1: float = 0.0
+    b0: float = 0.0
+    b1: float = 0.0
+    e0: float = 0.0
+    e1: float = 1.0
+    ro: float = 3300.0
+    bb: float = 0.0
+    aa: float = 0.0
+    cp: float = 1000.0
+    kt: float = 3.0
+    kf: float = 0.0
+    kp: float = 0.0
+    ht: float = 0.0
+
+
+@dataclasses.dataclass
+class ModelSpec:
+    shape: tuple
+    size: tuple              # xsize, ysize, zsize in metres
+    mnum: tuple = (3, 3, 3)  # markers per cell along x, y, z
+    jitter: float = 0.5      # fraction of the marker spacing (in3mg ``xnonstab``)
+    nonstab: int = 100
+    gravity: tuple = (0.0, 10.0, 0.0)
+    pinit_cell: tuple = (2, 1, 2)
+    pinit: float = 1e5
+    t_top: float = 273.0
+    t_bottom: float = 1573.0
+    multinum: int = 2
+
+
+def _uniform_grid(n, size):
+    step = size / (n - 1)
+    g = np.zeros(n)
+    for i in range(1, n):
+        g[i] = g[i - 1] + step
+    g[-1] = size
+    return g.astype(np.float32)
+
+
+def build_markers(spec: ModelSpec, seed: int):
+    nx, ny, nz = spec.shape
+    xs, ys, zs = spec.size
+    mx, my, mz = spec.mnum
+    stp = (xs / (nx - 1), ys / (ny - 1), zs / (nz - 1))
+    d = (stp[0] / mx, stp[1] / my, stp[2] / mz)
+    # cell-major order: cell (z, x, y), inside a cell (z, x, y) as in in3mg.c:141-175
+    c3, c1, c2, s5, s6, s7 = np.meshgrid(np.arange(nz - 1), np.arange(nx - 1), np.arange(ny - 1),
+                                         np.arange(mz), np.arange(mx), np.arange(my), indexing="ij")
+    x = c1 * stp[0] + d[0] / 2.0 + s6 * d[0]
+    y = c2 * stp[1] + d[1] / 2.0 + s7 * d[1]
+    z = c3 * stp[2] + d[2] / 2.0 + s5 * d[2]
+    x, y, z = (np.ascontiguousarray(a.reshape(-1)).astype(np.float32) for a in (x, y, z))
+    if spec.nonstab:
+        n = spec.nonstab
+        rng = np.random.default_rng(seed)
+        for arr, dd in ((x, d[0]), (y, d[1]), (z, d[2])):
+            r = rng.integers(0, 2 * n + 1, size=arr.size)
+            jit = ((r - n).astype(np.float32) / np.float32(n)) * np.float32(spec.jitter * dd)
+            arr += jit.astype(np.float32)
+    return x, y, z
+
+
+def make_prn(spec: ModelSpec, rocks: dict, types: np.ndarray, marks_xyz, seed: int = 0) -> Prn:
+    nx, ny, nz = spec.shape
+    x, y, z = marks_xyz
+    nmark = x.size
+    gx, gy, gz = (_uniform_grid(n, s) for n, s in zip(spec.shape, spec.size))
+    rocknum = max(rocks) + 1
+    rtab = {f: np.zeros(rocknum) for f in ROCK_FIELDS}
+    for t, r in rocks.items():
+        for f in ROCK_FIELDS:
+            rtab[f][t] = getattr(r, f)
+    nodenum = nx * ny * nz
+    nodes = {f: np.zeros(nodenum, np.float32) for f in
+             ("pr", "vx", "vy", "vz", "ro", "nu", "nxx", "nxy", "nxz", "nyz", "tk", "cp", "et",
+              "kt", "ht", "rr")}
+    # linear temperature between the top and bottom walls, on nodes and markers
+    ty = spec.t_top + (spec.t_bottom - spec.t_top) * gy.astype(np.float64) / spec.size[1]
+    nodes["tk"][:] = np.broadcast_to(ty[None, None, :], (nz, nx, ny)).reshape(-1)
+    mk = spec.t_top + (spec.t_bottom - spec.t_top) * y.astype(np.float64) / spec.size[1]
+    marks = {f: np.zeros(nmark, np.float32) for f in
+             ("x", "y", "z", "k", "w", "d", "v", "e", "ex", "ft", "rr", "rn")}
+    marks["x"], marks["y"], marks["z"] = x, y, z
+    marks["k"] = mk.astype(np.float32)
+    marks["t"] = types.astype(np.int8)
+    bond = expand_bc(free_slip_boxes(nx, ny, nz, spec.t_top, spec.t_bottom), spec.shape, spec.multinum)
+    head = dict(xnumx=nx, ynumy=ny, znumz=nz, mnumx=spec.mnum[0], mnumy=spec.mnum[1],
+                mnumz=spec.mnum[2], xsize=float(spec.size[0]), ysize=float(spec.size[1]),
+                zsize=float(spec.size[2]), pxinit=spec.pinit_cell[0], pyinit=spec.pinit_cell[1],
+                pzinit=spec.pinit_cell[2], pinit=spec.pinit, gxkoef=spec.gravity[0],
+                gykoef=spec.gravity[1], gzkoef=spec.gravity[2], rocknum=rocknum,
+                bondnum=len(bond), marknum=nmark, cycle=0, timesum_yr=0.0, gridcur=0.0, gridtot=0.0)
+    return Prn(head, rtab, nodes, gx, gy, gz, bond, marks)
+
+
+# ---------------------------------------------------------------------------------------
+# Named workloads
+# ---------------------------------------------------------------------------------------
+MATRIX, SPHERE = 2, 3
+INCLUSION_TYPES = (3, 4, 5, 6, 9, 10, 11, 12, 13, 14, 15, 19)
+
+
+def sinking_sphere(n=33, size_km=100.0, mnum=3, multinum=2, seed=1, radius_km=20.0):
+    """Plain sinking sphere: eta 1e23 / rho 3400 sphere in eta 1e21 / rho 3300 matrix,
+    g = 10 along the vertical, free slip, linear T 273 -> 1573 K, k = 3, cp = 1000."""
+    L = size_km * 1e3
+    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum)
+    xyz = build_markers(spec, seed)
+    x, y, z = (a.astype(np.float64) for a in xyz)
+    r = np.sqrt((x - L / 2) ** 2 + (y - L / 2) ** 2 + (z - L / 2) ** 2)
+    types = np.where(r <= radius_km * 1e3, SPHERE, MATRIX)
+    rocks = {MATRIX: Rock(nu=1e21, ro=3300.0), SPHERE: Rock(nu=1e23, ro=3400.0)}
+    return make_prn(spec, rocks, types, xyz, seed), spec
+
+
+def random_inclusions(n=129, size_km=200.0, mnum=3, multinum=4, seed=7, count=100,
+                      r_km=(2.0, 8.0), rho=(3250.0, 3450.0), contrast=None,
+                      arrhenius=True, activation=5e5, eta_ref=1e21, t_ref=923.0):
+    """Random spherical inclusions in an Arrhenius matrix.
+
+    Inclusion centres, radii and densities are seeded; densities (and, when ``contrast``
+    is given, log-uniform viscosity contrasts up to ``contrast``) are binned into at most
+    12 rock types because the reference keeps rock properties per type."""
+    L = size_km * 1e3
+    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum)
+    rng = np.random.default_rng(seed)
+    cen = rng.uniform(0.1 * L, 0.9 * L, size=(count, 3))
+    rad = rng.uniform(r_km[0] * 1e3, r_km[1] * 1e3, size=count)
+    dens = rng.uniform(rho[0], rho[1], size=count)
+    logc = rng.uniform(0.0, np.log10(contrast), size=count) if contrast else np.zeros(count)
+    nbin = len(INCLUSION_TYPES)
+    # joint bins: density quantile x contrast quantile, at most 12 types
+    if contrast:
+        nd, nc = 4, 3
+    else:
+        nd, nc = nbin, 1
+    dbin = np.minimum(((dens - rho[0]) / (rho[1] - rho[0]) * nd).astype(int), nd - 1)
+    cbin = np.minimum((logc / max(np.log10(contrast), 1e-30) * nc).astype(int), nc - 1) if contrast else np.zeros(count, int)
+    tbin = dbin * nc + cbin
+    A = eta_ref / np.exp(activation / (8.314 * t_ref)) if arrhenius else eta_ref
+    mat = Rock(nu=A, dh=activation if arrhenius else 0.0, mm=1.0, n0=1e18, n1=1e24, ro=3300.0)
+    rocks = {MATRIX: mat}
+    for b in range(nd * nc):
+        sel = tbin == b
+        d_mean = dens[sel].mean() if sel.any() else rho[0] + (b // nc + 0.5) * (rho[1] - rho[0]) / nd
+        c_mean = 10 ** logc[sel].mean() if (sel.any() and contrast) else (
+            10 ** ((b % nc + 0.5) * np.log10(contrast) / nc) if contrast else 1.0)
+        rocks[INCLUSION_TYPES[b]] = dataclasses.replace(mat, nu=A * c_mean, ro=float(d_mean))
+    xyz = build_markers(spec, seed)
+    x, y, z = (a.astype(np.float64) for a in xyz)
+    types = np.full(x.size, MATRIX, np.int64)
+    for i in range(count):
+        # cheap bounding-box prefilter before the distance test
+        r = rad[i]
+        sel = ((np.abs(x - cen[i, 0]) <= r) & (np.abs(y - cen[i, 1]) <= r) & (np.abs(z - cen[i, 2]) <= r))
+        idx = np.nonzero(sel)[0]
+        if idx.size:
+            d2 = (x[idx] - cen[i, 0]) ** 2 + (y[idx] - cen[i, 1]) ** 2 + (z[idx] - cen[i, 2]) ** 2
+            types[idx[d2 <= r * r]] = INCLUSION_TYPES[tbin[i]]
+    return make_prn(spec, rocks, types, xyz, seed), spec

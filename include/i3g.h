@@ -1,0 +1,207 @@
+/*
+ * i3g.h -- C ABI of the B200 time-step library for I3ELVIS-style marker-in-cell models.
+ *
+ * The reference has no plugin interface: its time step is four internal calls made by the
+ * host loop, which share state through static arrays (head3mg.c:33-288):
+ *
+ *     vpiterate(n0, f0)   i3mg.c:98    Stokes + continuity multigrid   (move3mg.c:1585-2636)
+ *     titerate(n0)        i3mg.c:112   implicit heat solve + marker T  (heat3mg.c:287-788)
+ *     movemark()          i3mg.c:125   RK4 marker advection + rheology (mark3mg.c:2-397)
+ *     ronurecalc()        i3mg.c:137   marker -> node averaging        (mark3mg.c:404-1015)
+ *
+ * This header replaces those globals with one explicit model description (i3g_model, plain
+ * pointers to host arrays in the .prn layout) and one opaque context that owns the device
+ * copies.  Every entry point returns 0 on success or a negative I3G_E* code; the message of
+ * the last failure is available from i3g_last_error().  The reference reports failures with
+ * printf + exit(0) (gaus3mg.c:86-90, move3mg.c:2272); here nothing exits.
+ *
+ * All calls are made from one host thread and are ordered on the context's CUDA stream.
+ * Host arrays are read by i3g_create()/i3g_upload() and written by i3g_download() only.
+ */
+#ifndef I3G_H
+#define I3G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define I3G_MAXLEV 12
+
+/* ---- error codes ------------------------------------------------------------------ */
+enum {
+    I3G_OK = 0,
+    I3G_E_ARG = -1,          /* invalid argument or size                                    */
+    I3G_E_CUDA = -2,         /* CUDA runtime error (message has the CUDA error string)     */
+    I3G_E_NOMEM = -3,        /* device allocation failed                                   */
+    I3G_E_UNSUPPORTED = -4,  /* model feature outside the implemented physics              */
+    I3G_E_NOCONV = -5,       /* iteration cap reached before the tolerance                 */
+    I3G_E_NAN = -6,          /* NaN or Inf detected in a solution vector                   */
+    I3G_E_PRESSURE = -7,     /* |P| > 1e12 Pa after a solve (reference exits: move3mg.c:2272) */
+    I3G_E_BC = -8            /* boundary-condition table inconsistent (cycle, bad partner) */
+};
+
+/* ---- model: host image of one .prn file (load3mg.c:704-892) ----------------------- */
+typedef struct i3g_model {
+    /* grid (load3mg.c:739-751) */
+    int64_t xnumx, ynumy, znumz;        /* nodes along x, y (vertical, y fastest), z     */
+    int64_t mnumx, mnumy, mnumz;        /* markers per cell (used by the water level test)*/
+    double xsize, ysize, zsize;         /* box size, m                                   */
+    int64_t pxinit, pyinit, pzinit;     /* pressure-pinning cell                          */
+    double pinit;                       /* pressure in that cell, Pa                     */
+    double gxkoef, gykoef, gzkoef;      /* gravity, m/s^2                                */
+    double timesum;                     /* model time, s                                 */
+    const float *gx, *gy, *gz;          /* grid lines as stored in the file (FP32)      */
+    /* nodal fields, level 0, node = z*(xnumx*ynumy) + x*ynumy + y (head3mg.c:70-80)     */
+    double *pr;                         /* pressure (FP64 like the reference)            */
+    float *vx, *vy, *vz;
+    float *ro, *nu, *nxx, *nxy, *nxz, *nyz;
+    float *tk, *cp, *et, *kt, *ht, *rr;
+    /* stresses and strain rates written by the Stokes step (head3mg.c:81-82); may be NULL */
+    float *exx, *eyy, *ezz, *exy, *exz, *eyz;
+    float *sxx, *syy, *szz, *sxy, *sxz, *syz;
+    /* boundary rows (load3mg.c:828-838): row index into bondm, x_row = c + k*x_(partner1-1) */
+    int64_t bondnum;
+    const int64_t *bond_row;
+    const float *bond_c, *bond_k;
+    const int64_t *bond_partner1;       /* 0 = no partner                                */
+    /* markers (load3mg.c:845-859), structure of arrays */
+    int64_t marknum;
+    float *markx, *marky, *markz, *markk, *markw, *markd, *markv, *marke;
+    float *markex, *markft, *markrr, *markrn;
+    int8_t *markt;
+    /* rock types: 24 tables of rocknum doubles in file order n0 n1 s0 s1 nu dh dv ss mm ll
+     * a0 a1 b0 b1 e0 e1 ro bb aa cp kt kf kp ht (load3mg.c:766-789)                     */
+    int32_t rocknum;
+    const double *rock[24];
+} i3g_model;
+
+/* ---- run parameters: mode.t3c (load3mg.c:2-170) ------------------------------------ */
+typedef struct i3g_params {
+    int32_t printmod, movemod, tempmod, markmod, gridmod, outgrid, densimod;
+    double stp100, eroslev, sedilev, waterlev;
+    double DIVVMIN, STOKSMIN, DIVVMAX, STOKSMAX;
+    int32_t multimax;                   /* levels built (multinum of the V_P block)      */
+    int32_t multicyc;                   /* V-cycles per convergence check                */
+    int32_t multinnn[2][I3G_MAXLEV];    /* sweeps per level: [0] down leg, [1] up leg    */
+    double p0koef, p1koef, p2koef, v0koef, v1koef;
+    double nubeg, nuend, nukoef;
+    int32_t viscmod;                    /* 0 arithmetic, 1 geometric, 2 harmonic          */
+    double HEATMIN;
+    int32_t multicyct, multittt0;       /* heat: cycles per check, sweeps per cycle      */
+    double t0koef, heatdif;
+    int32_t frictyn, adiabyn;
+    double zdeep, vdeep, tdeep, nudeep, healrate, teclmin, teclmax;
+    double timebeg, timeend, tempend;   /* plume BC schedule, s / K                       */
+    /* ---- solver controls of this library (no reference counterpart) ---- */
+    double stokes_rtol;                 /* > 0: stop on relative residual (see i3g_stokes)*/
+    int32_t stokes_maxcyc;              /* cap on V-cycles per solve (0 = 2000)          */
+    double heat_rtol;                   /* > 0: stop on relative heat residual           */
+    int32_t heat_maxcyc;                /* cap on heat V-cycles (0 = 2000)               */
+    int32_t precision;                  /* 0: FP64 multigrid, 1: FP32 MG inside FP64 defect correction */
+    int32_t warm_start;                 /* 1: start from the previous step's v,P (reference behaviour) */
+} i3g_params;
+
+/* ---- per output file row (load3mg.c:25-58, applied at i3mg.c:64-77) ---------------- */
+typedef struct i3g_file_params {
+    int32_t cyc0max;
+    double maxxystep, maxtkstep, maxtmstep;   /* m, K, s */
+    double nubeg, nuend;
+    double p0koef, p1koef, p2koef;             /* until multstp outer iterations          */
+    double p0koef2, p1koef2, p2koef2;          /* afterwards (move3mg.c:2585-2593)        */
+    int32_t multinum, multstp, multinum2;
+} i3g_file_params;
+
+/* ---- statistics of the last solves -------------------------------------------------- */
+typedef struct i3g_stats {
+    int32_t stokes_cycles;              /* V-cycles in the last i3g_stokes                */
+    int32_t stokes_outer;               /* outer (defect-correction / check) iterations   */
+    double stokes_rel0, stokes_rel;     /* relative residual before / after               */
+    double stokes_mom_rel, stokes_cont_rel;
+    int32_t heat_cycles, heat_substeps;
+    double heat_rel;
+    double ms_stokes, ms_heat, ms_move, ms_r2n;   /* device time of the last calls        */
+    int64_t kernel_launches;            /* kernels launched by this context so far        */
+} i3g_stats;
+
+typedef struct i3g_ctx i3g_ctx;
+
+/* Create a context on the current CUDA device: checks the model, builds the multigrid
+ * geometry (gridcheck, load3mg.c:1162-1283), flattens boundary rows and uploads all
+ * arrays.  Replaces loader()+gridcheck() state setup for the device. */
+int i3g_create(const i3g_model *m, const i3g_params *p, i3g_ctx **out);
+void i3g_destroy(i3g_ctx *c);
+const char *i3g_last_error(const i3g_ctx *c);   /* valid for c == NULL too */
+
+/* Per-output-file parameters (i3mg.c:64-77). */
+int i3g_set_file_params(i3g_ctx *c, const i3g_file_params *f);
+
+/* vpiterate(n0,f0) (move3mg.c:1585-2636): Stokes + continuity on the staggered grid.
+ * Stops when the relative residual (momentum ||b-Ax||/||b|| and continuity
+ * ||div v|| * h / ||v||, both <= stokes_rtol) is met, or -- when stokes_rtol <= 0 -- on the
+ * reference's absolute criteria (move3mg.c:2596).  Lowers *timestep to the CFL limit
+ * maxxystep / max|v| (move3mg.c:2608-2632).  Writes v, P, stresses, strain rates. */
+int i3g_stokes(i3g_ctx *c, int n0, double *timestep);
+
+/* titerate(n0) (heat3mg.c:287-788): implicit heat step with substeps limited by
+ * maxtkstep, geometric multigrid solve, then the marker temperature update with subgrid
+ * diffusion.  *timestep is left unchanged on return, as in the reference. */
+int i3g_heat(i3g_ctx *c, int n0, double *timestep);
+
+/* movemark() (mark3mg.c:2-397): per-marker rheology update and RK4 advection. */
+int i3g_move_markers(i3g_ctx *c, double timestep);
+
+/* ronurecalc() (mark3mg.c:404-1015): marker -> node averages + tkrecalc T boundaries. */
+int i3g_markers_to_nodes(i3g_ctx *c, double timestep);
+
+/* Advance model time (i3mg.c:146). */
+int i3g_add_time(i3g_ctx *c, double timestep);
+
+/* Host <-> device copies of the model arrays.  mask: I3G_SYNC_* bits. */
+enum { I3G_SYNC_NODES = 1, I3G_SYNC_STRESS = 2, I3G_SYNC_MARKERS = 4, I3G_SYNC_ALL = 7 };
+int i3g_download(i3g_ctx *c, i3g_model *m, unsigned mask);
+int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask);
+
+int i3g_get_stats(const i3g_ctx *c, i3g_stats *s);
+
+/* ---- kernel-level entry points (parity tests and benchmarks) ------------------------- */
+/* Level arrays addressable by i3g_get_array / i3g_set_array (element type in brackets). */
+enum {
+    I3G_A_SOL = 0,      /* [double, 4*N_l] unknowns P,Vx,Vy,Vz interleaved per node (sol0) */
+    I3G_A_RHS = 1,      /* [double, 4*N_l] right-hand sides (fre1)                        */
+    I3G_A_RES = 2,      /* [double, 4*N_l] residual b - A x (fre0)                        */
+    I3G_A_NU = 3,       /* [float, N_l] nodal viscosity (nu, restricted on l > 0)          */
+    I3G_A_ETA = 4,      /* [double, 4*N_l] clamped stress-point viscosities c, xy, xz, yz  */
+    I3G_A_TK = 5        /* [double, N_0] temperature solution                              */
+};
+int i3g_get_array(i3g_ctx *c, int which, int level, void *dst, int64_t nbytes);
+int i3g_set_array(i3g_ctx *c, int which, int level, const void *src, int64_t nbytes);
+
+/* Build level operators for the current nodal fields: ronurestrict (move3mg.c:2642-2741),
+ * stress-point viscosities, right-hand side (move3mg.c:2029-2159) and load the current
+ * v,P into the level-0 solution (move3mg.c:1969-2019). */
+int i3g_stokes_setup(i3g_ctx *c);
+/* fre0 = fre1 - A sol0 on a level (gausmat4 residual pass, move3mg.c:3136-3157). */
+int i3g_stokes_residual(i3g_ctx *c, int level);
+/* nsweeps multicolour relaxation sweeps on a level (gausmat4 relaxation formula,
+ * move3mg.c:3087-3131, in red-black order per velocity component, then pressure). */
+int i3g_stokes_smooth(i3g_ctx *c, int level, int nsweeps);
+/* vprestrict(level) (move3mg.c:3165-3520) and vpprolong(level,0) (move3mg.c:2748-3063). */
+int i3g_stokes_restrict(i3g_ctx *c, int level);
+int i3g_stokes_prolong(i3g_ctx *c, int level);
+/* ncycles V-cycles with the schedule of move3mg.c:2170-2223. */
+int i3g_stokes_vcycles(i3g_ctx *c, int ncycles);
+/* Relative residuals of the level-0 system for the current solution. */
+int i3g_stokes_relres(i3g_ctx *c, double *mom_rel, double *cont_rel);
+
+/* Time reps launches of one kernel class on the level-0 data with CUDA events on the
+ * context stream; returns the mean duration per launch and the algorithmic bytes that one
+ * launch must move.  kind: 0 smoother sweep, 1 residual, 2 restriction, 3 prolongation,
+ * 4 marker->node, 5 RK4 advection, 6 heat sweep. */
+int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, double *bytes_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* I3G_H */

@@ -1,0 +1,28 @@
+#!/bin/sh
+# Builds oracle/_ref/ref_harness: the reference's own solver functions, compiled from the
+# reference sources where they lie, driven by oracle/ref_harness.c (test infrastructure).
+# The only change is to the static array sizes of head3mg.c:8-20 (the shipped sizes need
+# 78 GB of static storage); the size-patched copy is a temporary build input and is removed
+# after compilation.  Outputs go to oracle/_ref/ only.
+set -e
+REF=${I3G_REFERENCE_DIR:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+if [ ! -f "$REF/move3mg.c" ]; then
+    echo "reference sources not found in $REF; oracle/_ref not rebuilt" >&2
+    exit 0
+fi
+mkdir -p "$OUT/gen"
+sed -e 's/^#define MAXMAT .*/#define MAXMAT  160000000/' \
+    -e 's/^#define MAXNOD .*/#define MAXNOD   5000000/' \
+    -e 's/^#define MAXNNN .*/#define MAXNNN   2300000/' \
+    -e 's/^#define MAXPAR .*/#define MAXPAR  40000000/' \
+    -e 's/^#define MAXPPP .*/#define MAXPPP  16000000/' \
+    -e 's/^#define MAXMRK .*/#define MAXMRK  60000000/' \
+    -e 's/^#define MAXBON .*/#define MAXBON   4000000/' \
+    "$REF/head3mg.c" > "$OUT/gen/head3mg.c"
+gcc -O2 -fopenmp -mcmodel=medium -w -I"$OUT/gen" -I"$REF" "$HERE/ref_harness.c" \
+    -o "$OUT/ref_harness" -lm
+rm -f "$OUT/gen/head3mg.c"
+rmdir "$OUT/gen" 2>/dev/null || true
+echo "built $OUT/ref_harness"
