@@ -1,0 +1,134 @@
+// i3g_internal.cuh -- device-side data layout of the B200 time-step library.
+//
+// Every multigrid level keeps the reference's node numbering (node = z*NX*NY + x*NY + y,
+// y fastest: move3mg.c:1632) so that a warp reads consecutive y.  Unknowns are stored as
+// separate arrays per component (P, Vx, Vy, Vz) instead of the reference's interleaved
+// sol0[4*node+k] (head3mg.c:33), which keeps every component load unit-stride.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include "../../include/i3g.h"
+
+#define I3G_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call, __FILE__, __LINE__);        \
+    } while (0)
+
+namespace i3g {
+
+constexpr int kMaxBcDepth = 4;   // boundary chains x_a = c + k x_b, x_b = c' + k' x_c, ...
+
+// Boundary rows of one component on one level, flattened to an interior partner.
+struct BcList {
+    int n = 0;
+    int *node = nullptr;        // row node (level-local)
+    int *pnode = nullptr;       // interior partner node, -1: constant
+    int *depth = nullptr;       // number of (c,k) pairs in the chain (1..kMaxBcDepth)
+    double *c = nullptr;        // [n*kMaxBcDepth] chain constants, outermost first
+    double *k = nullptr;        // [n*kMaxBcDepth] chain factors
+    int *onode = nullptr;       // original partner node (unflattened), -1: none
+    int *ocomp = nullptr;       // original partner component
+    double *oc = nullptr, *ok = nullptr;   // original constant and factor (level 0 residual)
+};
+
+template <typename T>
+struct Fields {
+    T *u[4] = {nullptr, nullptr, nullptr, nullptr};    // solution: P, Vx, Vy, Vz
+    T *f[4] = {nullptr, nullptr, nullptr, nullptr};    // right-hand side (fre1)
+    T *r[4] = {nullptr, nullptr, nullptr, nullptr};    // residual (fre0)
+    T *etac = nullptr, *etaxy = nullptr, *etaxz = nullptr, *etayz = nullptr;
+    T *ix[2] = {nullptr, nullptr};   // per axis x: [0] 1/(g[i]-g[i-1]), [1] 1/(g[i+1]-g[i-1])
+    T *iy[2] = {nullptr, nullptr};
+    T *iz[2] = {nullptr, nullptr};
+    float *nd = nullptr;             // pressure relaxation viscosity (FP32 like the reference's nd[])
+};
+
+// Separable 1-D transfer stencils between a fine level and the next coarse level.
+// For fine index f: coarse cell index a[f] and weights w0[f] (to a) and w1[f] (to a+1).
+// For the gather form, coarse index c lists its fine contributors (ascending f) in
+// [gptr[c], gptr[c+1]) with fine index gf and weight gw.
+struct Transfer1D {
+    int nf = 0, nc = 0;
+    int *a = nullptr;
+    double *w0 = nullptr, *w1 = nullptr;
+    int *gptr = nullptr, *gf = nullptr;
+    double *gw = nullptr;
+};
+
+// staggering kinds: 0 grid line, 1 mid-point, 2 cell centre, 3 grid line with |d| weights
+// (viscosity restriction)
+constexpr int kStagLine = 0, kStagMid = 1, kStagCell = 2, kStagAbs = 3;
+
+struct Level {
+    int nx = 0, ny = 0, nz = 0;
+    long n = 0;
+    double *gx = nullptr, *gy = nullptr, *gz = nullptr;   // level coordinates (host)
+    float *nu = nullptr;               // nodal viscosity of this level
+    uint8_t *bc = nullptr;             // bit v: row v (0 P, 1 Vx, 2 Vy, 3 Vz) is a boundary row
+    Fields<double> d;
+    Fields<float> s;                    // scaled FP32 copy for the mixed-precision solver
+    BcList bcl[4];
+    Transfer1D tr[3][4];               // to the next coarser level: axis x,y,z; staggering
+    long scratch_n = 0;
+    double *red = nullptr;             // reduction scratch
+};
+
+struct KernelTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+}  // namespace i3g
+
+struct i3g_ctx {
+    i3g_model m;
+    i3g_params p;
+    i3g_file_params f;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    long nodenum = 0, marknum = 0;
+    int nlev = 0;
+    i3g::Level lev[I3G_MAXLEV];
+    // level-0 physical fields (device)
+    double *pr = nullptr;
+    float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    float *ro = nullptr, *nxx = nullptr, *nxy = nullptr, *nxz = nullptr, *nyz = nullptr;
+    float *tk = nullptr, *cp = nullptr, *et = nullptr, *kt = nullptr, *ht = nullptr, *rr = nullptr;
+    float *eps[6] = {}, *sig[6] = {};   // exx eyy ezz exy exz eyz / sxx ...
+    double *gx0 = nullptr, *gy0 = nullptr, *gz0 = nullptr;   // level-0 grid lines (device)
+    // host copies of the grid lines
+    double *hgx = nullptr, *hgy = nullptr, *hgz = nullptr;
+    // reductions
+    double *dred = nullptr, *hred = nullptr;    // device scratch and pinned host mirror
+    double *hstage = nullptr;                   // pinned host staging (4 * red_blocks doubles)
+    int red_blocks = 0;
+    double ncont = 0, nvel = 0;                 // level-0 row counts for the continuity norm
+    float **deps = nullptr, **dsig = nullptr;   // device arrays of the 6+6 stress/strain pointers
+    // bookkeeping
+    bool stokes_ready = false;
+    double eta_ref = 1.0, h_ref = 1.0;
+    i3g_stats st_;
+    char err[512] = {0};
+    int64_t launches = 0;
+    void *heat = nullptr;      // heat-solver state
+    void *mk = nullptr;        // marker state
+};
+
+int cuda_fail(i3g_ctx *c, cudaError_t e, const char *what, const char *file, int line);
+int set_error(i3g_ctx *c, int code, const char *fmt, ...);
+
+namespace i3g {
+// stokes.cu
+int stokes_alloc(i3g_ctx *c);
+void stokes_free(i3g_ctx *c);
+int stokes_setup(i3g_ctx *c);
+int stokes_residual(i3g_ctx *c, int level);
+int stokes_smooth(i3g_ctx *c, int level, int nsweeps);
+int stokes_restrict(i3g_ctx *c, int level);
+int stokes_prolong(i3g_ctx *c, int level);
+int stokes_vcycle(i3g_ctx *c, int multinum);
+int stokes_relres(i3g_ctx *c, double *mom, double *cont);
+int stokes_solve(i3g_ctx *c, double *timestep);
+int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes);
+}  // namespace i3g

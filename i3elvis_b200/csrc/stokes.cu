@@ -1,0 +1,1419 @@
+// stokes.cu -- staggered-grid variable-viscosity Stokes multigrid for sm_100a.
+//
+// Replaces vpiterate (move3mg.c:1585-2636).  The reference assembles every row into a
+// 57-slot CSR store (gausmat2, gaus3mg.c:67-127; 684 B/node of matrix traffic per sweep)
+// and relaxes it lexicographically.  Here the rows are never stored: each kernel rebuilds
+// a row's 17 coefficients from the four stress-point viscosity arrays and the 1-D grid
+// tables, and the relaxation runs in multicolour order (red/black per velocity component,
+// then all pressure rows), which parallelises without the data race of the reference's
+// OpenMP sweep (move3mg.c:3089-3130).
+//
+// FP64 arithmetic uses explicitly rounded operations in the reference's operand order, so
+// rows, residuals and relaxation updates agree bit for bit with the CPU oracle.  The FP32
+// path (mixed precision) uses the same stencil code on viscosity and geometry scaled to O(1).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "i3g_internal.cuh"
+
+namespace i3g {
+
+// ------------------------------------------------------------------------------------
+// arithmetic policies
+// ------------------------------------------------------------------------------------
+template <typename T>
+struct Ar;
+template <>
+struct Ar<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <>
+struct Ar<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+};
+
+// Level view passed by value to kernels.
+template <typename T>
+struct View {
+    int nx, ny, nz;
+    long nxy;
+    const uint8_t *bc;
+    T *u0, *u1, *u2, *u3;
+    T *f0, *f1, *f2, *f3;
+    T *r0, *r1, *r2, *r3;
+    const T *etac, *etaxy, *etaxz, *etayz;
+    const T *icx, *isx, *icy, *isy, *icz, *isz;
+    const float *nd;
+};
+
+template <typename T>
+static View<T> view(Level &L, Fields<T> &F)
+{
+    View<T> v;
+    v.nx = L.nx; v.ny = L.ny; v.nz = L.nz; v.nxy = (long)L.nx * L.ny;
+    v.bc = L.bc;
+    v.u0 = F.u[0]; v.u1 = F.u[1]; v.u2 = F.u[2]; v.u3 = F.u[3];
+    v.f0 = F.f[0]; v.f1 = F.f[1]; v.f2 = F.f[2]; v.f3 = F.f[3];
+    v.r0 = F.r[0]; v.r1 = F.r[1]; v.r2 = F.r[2]; v.r3 = F.r[3];
+    v.etac = F.etac; v.etaxy = F.etaxy; v.etaxz = F.etaxz; v.etayz = F.etayz;
+    v.icx = F.ix[0]; v.isx = F.ix[1]; v.icy = F.iy[0]; v.isy = F.iy[1]; v.icz = F.iz[0]; v.isz = F.iz[1];
+    v.nd = F.nd;
+    return v;
+}
+
+// row existence (vpiterate loop guards, move3mg.c:2057-2141)
+__host__ __device__ __forceinline__ bool row_exists(int v, int i, int j, int k, int nx, int ny, int nz)
+{
+    switch (v) {
+    case 0: return i > 0 && j > 0 && k > 0;
+    case 1: return j < ny - 1 && k < nz - 1;
+    case 2: return i < nx - 1 && k < nz - 1;
+    default: return i < nx - 1 && j < ny - 1;
+    }
+}
+
+// accumulate one slot: smoother form s += c*x (starting from -f), residual form s -= c*x
+template <typename T, bool RES>
+__device__ __forceinline__ void acc(T &s, T c, T x)
+{
+    if (RES) s = Ar<T>::sub(s, Ar<T>::mul(c, x));
+    else s = Ar<T>::add(s, Ar<T>::mul(c, x));
+}
+
+template <typename T>
+__device__ __forceinline__ T cf(T a, T n, T k)   // ((a*n)*2)*k: -ynval*nueff*2.0*dk
+{
+    return Ar<T>::mul(Ar<T>::mul(Ar<T>::mul(a, n), T(2)), k);
+}
+
+// x-momentum row at node n = (i,j,k) (xstokserr, move3mg.c:718-903): accumulates the 17
+// slots in the reference's order into s and returns the diagonal.
+template <typename T, bool RES>
+__device__ __forceinline__ T xrow(const View<T> &L, int i, int j, int k, long n, T &s)
+{
+    using A = Ar<T>;
+    const long NY = L.ny, NXY = L.nxy;
+    const T XK = A::mul(T(2), L.isx[i]), YK = L.icy[j + 1], ZK = L.icz[k + 1];
+    const T cA = cf(XK, L.etac[n + NXY + 1], L.icx[i]);
+    const T cB = cf(XK, L.etac[n + NXY + NY + 1], L.icx[i + 1]);
+    const T nS = L.etaxy[n], nN = L.etaxy[n + 1], xkS = L.isx[i];
+    const T cSy = cf(YK, nS, L.isy[j]), cSx = cf(YK, nS, xkS);
+    const T cNy = cf(YK, nN, L.isy[j + 1]), cNx = cf(YK, nN, xkS);
+    const T nF = L.etaxz[n], nK = L.etaxz[n + NXY];
+    const T cFz = cf(ZK, nF, L.isz[k]), cFx = cf(ZK, nF, xkS);
+    const T cKz = cf(ZK, nK, L.isz[k + 1]), cKx = cf(ZK, nK, xkS);
+    T d = -cA;
+    d = A::add(d, -cB); d = A::add(d, -cSy); d = A::add(d, -cNy); d = A::add(d, -cFz); d = A::add(d, -cKz);
+    const T *vx = L.u1, *vy = L.u2, *vz = L.u3, *p = L.u0;
+    acc<T, RES>(s, d, vx[n]);
+    acc<T, RES>(s, cA, vx[n - NY]);
+    acc<T, RES>(s, cB, vx[n + NY]);
+    acc<T, RES>(s, cSy, vx[n - 1]);
+    acc<T, RES>(s, cNy, vx[n + 1]);
+    acc<T, RES>(s, cFz, vx[n - NXY]);
+    acc<T, RES>(s, cKz, vx[n + NXY]);
+    acc<T, RES>(s, cSx, vy[n - NY]);
+    acc<T, RES>(s, -cNx, vy[n - NY + 1]);
+    acc<T, RES>(s, -cSx, vy[n]);
+    acc<T, RES>(s, cNx, vy[n + 1]);
+    acc<T, RES>(s, cFx, vz[n - NY]);
+    acc<T, RES>(s, -cKx, vz[n - NY + NXY]);
+    acc<T, RES>(s, -cFx, vz[n]);
+    acc<T, RES>(s, cKx, vz[n + NXY]);
+    acc<T, RES>(s, XK, p[n + NXY + 1]);
+    acc<T, RES>(s, -XK, p[n + NXY + NY + 1]);
+    return d;
+}
+
+// y-momentum row (ystokserr, move3mg.c:910-1101)
+template <typename T, bool RES>
+__device__ __forceinline__ T yrow(const View<T> &L, int i, int j, int k, long n, T &s)
+{
+    using A = Ar<T>;
+    const long NY = L.ny, NXY = L.nxy;
+    const T XK = L.icx[i + 1], YK = A::mul(T(2), L.isy[j]), ZK = L.icz[k + 1];
+    const T cA = cf(YK, L.etac[n + NY + NXY], L.icy[j]);
+    const T cB = cf(YK, L.etac[n + NY + 1 + NXY], L.icy[j + 1]);
+    const T nW = L.etaxy[n], nE = L.etaxy[n + NY], ykW = L.isy[j];
+    const T cWy = cf(XK, nW, ykW), cWx = cf(XK, nW, L.isx[i]);
+    const T cEy = cf(XK, nE, ykW), cEx = cf(XK, nE, L.isx[i + 1]);
+    const T nF = L.etayz[n], nK = L.etayz[n + NXY];
+    const T cFz = cf(ZK, nF, L.isz[k]), cFy = cf(ZK, nF, ykW);
+    const T cKz = cf(ZK, nK, L.isz[k + 1]), cKy = cf(ZK, nK, ykW);
+    T d = -cA;
+    d = A::add(d, -cB); d = A::add(d, -cWx); d = A::add(d, -cEx); d = A::add(d, -cFz); d = A::add(d, -cKz);
+    const T *vx = L.u1, *vy = L.u2, *vz = L.u3, *p = L.u0;
+    acc<T, RES>(s, d, vy[n]);
+    acc<T, RES>(s, cWx, vy[n - NY]);
+    acc<T, RES>(s, cEx, vy[n + NY]);
+    acc<T, RES>(s, cA, vy[n - 1]);
+    acc<T, RES>(s, cB, vy[n + 1]);
+    acc<T, RES>(s, cFz, vy[n - NXY]);
+    acc<T, RES>(s, cKz, vy[n + NXY]);
+    acc<T, RES>(s, cWy, vx[n - 1]);
+    acc<T, RES>(s, -cWy, vx[n]);
+    acc<T, RES>(s, -cEy, vx[n + NY - 1]);
+    acc<T, RES>(s, cEy, vx[n + NY]);
+    acc<T, RES>(s, cFy, vz[n - 1]);
+    acc<T, RES>(s, -cFy, vz[n]);
+    acc<T, RES>(s, -cKy, vz[n - 1 + NXY]);
+    acc<T, RES>(s, cKy, vz[n + NXY]);
+    acc<T, RES>(s, YK, p[n + NY + NXY]);
+    acc<T, RES>(s, -YK, p[n + NY + 1 + NXY]);
+    return d;
+}
+
+// z-momentum row (zstokserr, move3mg.c:1109-1301)
+template <typename T, bool RES>
+__device__ __forceinline__ T zrow(const View<T> &L, int i, int j, int k, long n, T &s)
+{
+    using A = Ar<T>;
+    const long NY = L.ny, NXY = L.nxy;
+    const T XK = L.icx[i + 1], YK = L.icy[j + 1], ZK = A::mul(T(2), L.isz[k]);
+    const T cA = cf(ZK, L.etac[n + NY + 1], L.icz[k]);
+    const T cB = cf(ZK, L.etac[n + NY + 1 + NXY], L.icz[k + 1]);
+    const T nW = L.etaxz[n], nE = L.etaxz[n + NY], zkW = L.isz[k];
+    const T cWz = cf(XK, nW, zkW), cWx = cf(XK, nW, L.isx[i]);
+    const T cEz = cf(XK, nE, zkW), cEx = cf(XK, nE, L.isx[i + 1]);
+    const T nS = L.etayz[n], nN = L.etayz[n + 1];
+    const T cSz = cf(YK, nS, zkW), cSy = cf(YK, nS, L.isy[j]);
+    const T cNz = cf(YK, nN, zkW), cNy = cf(YK, nN, L.isy[j + 1]);
+    T d = -cA;
+    d = A::add(d, -cB); d = A::add(d, -cWx); d = A::add(d, -cEx); d = A::add(d, -cSy); d = A::add(d, -cNy);
+    const T *vx = L.u1, *vy = L.u2, *vz = L.u3, *p = L.u0;
+    acc<T, RES>(s, d, vz[n]);
+    acc<T, RES>(s, cWx, vz[n - NY]);
+    acc<T, RES>(s, cEx, vz[n + NY]);
+    acc<T, RES>(s, cSy, vz[n - 1]);
+    acc<T, RES>(s, cNy, vz[n + 1]);
+    acc<T, RES>(s, cA, vz[n - NXY]);
+    acc<T, RES>(s, cB, vz[n + NXY]);
+    acc<T, RES>(s, cSz, vy[n - NXY]);
+    acc<T, RES>(s, -cNz, vy[n + 1 - NXY]);
+    acc<T, RES>(s, -cSz, vy[n]);
+    acc<T, RES>(s, cNz, vy[n + 1]);
+    acc<T, RES>(s, cWz, vx[n - NXY]);
+    acc<T, RES>(s, -cWz, vx[n]);
+    acc<T, RES>(s, -cEz, vx[n + NY - NXY]);
+    acc<T, RES>(s, cEz, vx[n + NY]);
+    acc<T, RES>(s, ZK, p[n + NY + 1]);
+    acc<T, RES>(s, -ZK, p[n + NY + 1 + NXY]);
+    return d;
+}
+
+// continuity row of the cell with upper corner n = (i,j,k) (continerr, move3mg.c:1310-1425)
+template <typename T, bool RES>
+__device__ __forceinline__ void crow(const View<T> &L, int i, int j, int k, long n, T &s)
+{
+    const long NY = L.ny, NXY = L.nxy;
+    const long v0 = n - NXY - NY - 1;
+    const T xk = L.icx[i], yk = L.icy[j], zk = L.icz[k];
+    acc<T, RES>(s, -xk, L.u1[v0]);
+    acc<T, RES>(s, xk, L.u1[v0 + NY]);
+    acc<T, RES>(s, -yk, L.u2[v0]);
+    acc<T, RES>(s, yk, L.u2[v0 + 1]);
+    acc<T, RES>(s, -zk, L.u3[v0]);
+    acc<T, RES>(s, zk, L.u3[v0 + NXY]);
+}
+
+// ------------------------------------------------------------------------------------
+// relaxation kernels
+// ------------------------------------------------------------------------------------
+// One colour of one velocity component: thread t handles the row of colour `color` in the
+// y-pair (2*jh, 2*jh+1) of line (i,k), so a warp covers 64 consecutive y.
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_relax_vel(View<T> L, int color, T koef)
+{
+    using A = Ar<T>;
+    const int hy = (L.ny + 1) >> 1;
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long total = (long)hy * L.nx * L.nz;
+    if (t >= total) return;
+    const int jh = (int)(t % hy);
+    const long rest = t / hy;
+    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    const int j = 2 * jh + ((i + k + color) & 1);
+    if (j >= L.ny || !row_exists(V, i, j, k, L.nx, L.ny, L.nz)) return;
+    const long n = (long)k * L.nxy + (long)i * L.ny + j;
+    if (L.bc[n] & (1 << V)) return;
+    T s, d;
+    if (V == 1) { s = -L.f1[n]; d = xrow<T, false>(L, i, j, k, n, s); L.u1[n] = A::sub(L.u1[n], A::mul(A::div(s, d), koef)); }
+    if (V == 2) { s = -L.f2[n]; d = yrow<T, false>(L, i, j, k, n, s); L.u2[n] = A::sub(L.u2[n], A::mul(A::div(s, d), koef)); }
+    if (V == 3) { s = -L.f3[n]; d = zrow<T, false>(L, i, j, k, n, s); L.u3[n] = A::sub(L.u3[n], A::mul(A::div(s, d), koef)); }
+}
+
+// All interior pressure rows: p -= (div v - f) * nd * p0koef (move3mg.c:3105-3116)
+template <typename T>
+__global__ void __launch_bounds__(256) k_relax_p(View<T> L, T koef)
+{
+    using A = Ar<T>;
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = L.nxy * L.nz;
+    if (n >= N) return;
+    const int j = (int)(n % L.ny);
+    const long rest = n / L.ny;
+    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    if (!(i > 0 && j > 0 && k > 0) || (L.bc[n] & 1)) return;
+    T s = -L.f0[n];
+    crow<T, false>(L, i, j, k, n, s);
+    L.u0[n] = A::sub(L.u0[n], A::mul(A::mul(s, (T)L.nd[n]), koef));
+}
+
+// Boundary rows of one component: x = c1 + k1*(c2 + k2*(... x_partner)) evaluated from the
+// innermost link outwards (the fixed point of bonderr rows, move3mg.c:1532-1579).
+template <typename T>
+__global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const int *depth,
+                           const double *cc, const double *kk, int use_c)
+{
+    using A = Ar<T>;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int p = pnode[t];
+    T val = p >= 0 ? u[p] : T(0);
+    for (int d = depth[t] - 1; d >= 0; d--) {
+        const T c0 = use_c ? (T)cc[t * kMaxBcDepth + d] : T(0);
+        val = A::add(c0, A::mul((T)kk[t * kMaxBcDepth + d], val));
+    }
+    u[node[t]] = val;
+}
+
+// ------------------------------------------------------------------------------------
+// residual (gausmat4 residual pass, move3mg.c:3136-3157)
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual(View<T> L)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = L.nxy * L.nz;
+    if (n >= N) return;
+    const int j = (int)(n % L.ny);
+    const long rest = n / L.ny;
+    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    const uint8_t b = L.bc[n];
+    if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) { T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); L.r0[n] = s; }
+    if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(b & 2)) { T s = L.f1[n]; xrow<T, true>(L, i, j, k, n, s); L.r1[n] = s; }
+    if (row_exists(2, i, j, k, L.nx, L.ny, L.nz) && !(b & 4)) { T s = L.f2[n]; yrow<T, true>(L, i, j, k, n, s); L.r2[n] = s; }
+    if (row_exists(3, i, j, k, L.nx, L.ny, L.nz) && !(b & 8)) { T s = L.f3[n]; zrow<T, true>(L, i, j, k, n, s); L.r3[n] = s; }
+}
+
+// residual of boundary rows with their original (unflattened) partner
+template <typename T>
+__global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const int *onode, const int *ocomp,
+                              const double *ok)
+{
+    using A = Ar<T>;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    T *u[4] = {L.u0, L.u1, L.u2, L.u3};
+    T *f[4] = {L.f0, L.f1, L.f2, L.f3};
+    T *r[4] = {L.r0, L.r1, L.r2, L.r3};
+    const int nd = node[t];
+    T s = f[V][nd];
+    s = A::sub(s, A::mul(T(1), u[V][nd]));
+    if (onode[t] >= 0) s = A::sub(s, A::mul((T)(-ok[t]), u[ocomp[t]][onode[t]]));
+    r[V][nd] = s;
+}
+
+// ------------------------------------------------------------------------------------
+// grid transfers in gather form
+// ------------------------------------------------------------------------------------
+struct TrView {
+    const int *gptr, *gf;
+    const double *gw;
+    const int *a;
+    const double *w0, *w1;
+};
+
+static TrView trview(const Transfer1D &t)
+{
+    return TrView{t.gptr, t.gf, t.gw, t.a, t.w0, t.w1};
+}
+
+// vprestrict (move3mg.c:3165-3520): coarse row = sum over fine contributors (fine rows that
+// exist and are not boundary rows), weight-normalised; pressure residuals scaled by
+// nd_fine/nd_coarse.  Contributions are summed in the fine lexicographic order of the
+// reference's scatter loop.  Coarse solution is zeroed.
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz)
+{
+    using A = Ar<T>;
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = Cc.nxy * Cc.nz;
+    if (n >= N) return;
+    const int j = (int)(n % Cc.ny);
+    const long rest = n / Cc.ny;
+    const int i = (int)(rest % Cc.nx), k = (int)(rest / Cc.nx);
+    T *cu = V == 0 ? Cc.u0 : V == 1 ? Cc.u1 : V == 2 ? Cc.u2 : Cc.u3;
+    T *cf_ = V == 0 ? Cc.f0 : V == 1 ? Cc.f1 : V == 2 ? Cc.f2 : Cc.f3;
+    const T *fr = V == 0 ? F.r0 : V == 1 ? F.r1 : V == 2 ? F.r2 : F.r3;
+    cu[n] = T(0);
+    if (!row_exists(V, i, j, k, Cc.nx, Cc.ny, Cc.nz) || (Cc.bc[n] & (1 << V))) { cf_[n] = T(0); return; }
+    T sum = 0, ws = 0;
+    const T ndc = V == 0 ? (T)Cc.nd[n] : T(1);
+    for (int ez = tz.gptr[k]; ez < tz.gptr[k + 1]; ez++) {
+        const int fk = tz.gf[ez];
+        const T wz = (T)tz.gw[ez];
+        for (int ex = tx.gptr[i]; ex < tx.gptr[i + 1]; ex++) {
+            const int fi = tx.gf[ex];
+            const T wx = (T)tx.gw[ex];
+            for (int ey = ty.gptr[j]; ey < ty.gptr[j + 1]; ey++) {
+                const int fj = ty.gf[ey];
+                if (!row_exists(V, fi, fj, fk, F.nx, F.ny, F.nz)) continue;
+                const long m = (long)fk * F.nxy + (long)fi * F.ny + fj;
+                if (F.bc[m] & (1 << V)) continue;
+                const T swt = A::mul(A::mul(wx, (T)ty.gw[ey]), wz);
+                T term;
+                if (V == 0) term = A::mul(A::div(A::mul(fr[m], (T)F.nd[m]), ndc), swt);
+                else term = A::mul(fr[m], swt);
+                sum = A::add(sum, term);
+                ws = A::add(ws, swt);
+            }
+        }
+    }
+    cf_[n] = ws != T(0) ? A::div(sum, ws) : sum;
+}
+
+// vpprolong (move3mg.c:2748-3063): fine += sum_8 coarse * weight * koef
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz, T koef)
+{
+    using A = Ar<T>;
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = F.nxy * F.nz;
+    if (n >= N) return;
+    const int j = (int)(n % F.ny);
+    const long rest = n / F.ny;
+    const int i = (int)(rest % F.nx), k = (int)(rest / F.nx);
+    if (!row_exists(V, i, j, k, F.nx, F.ny, F.nz)) return;
+    T *fu = V == 0 ? F.u0 : V == 1 ? F.u1 : V == 2 ? F.u2 : F.u3;
+    const T *cu = V == 0 ? Cc.u0 : V == 1 ? Cc.u1 : V == 2 ? Cc.u2 : Cc.u3;
+    const int a = tx.a[i], b = ty.a[j], c = tz.a[k];
+    const T wx[2] = {(T)tx.w0[i], (T)tx.w1[i]};
+    const T wy[2] = {(T)ty.w0[j], (T)ty.w1[j]};
+    const T wz[2] = {(T)tz.w0[k], (T)tz.w1[k]};
+    T s = fu[n];
+    for (int dz = 0; dz < 2; dz++)
+        for (int dx = 0; dx < 2; dx++)
+            for (int dy = 0; dy < 2; dy++) {
+                const long m = (long)(c + dz) * Cc.nxy + (long)(a + dx) * Cc.ny + (b + dy);
+                const T swt = A::mul(A::mul(wx[dx], wy[dy]), wz[dz]);
+                s = A::add(s, A::mul(A::mul(cu[m], swt), koef));
+            }
+    fu[n] = s;
+}
+
+// ronurestrict (move3mg.c:2642-2741): FP32 accumulator as in nu[], FP64 weights
+__global__ void k_nu_restrict(const float *nuf, int fnx, int fny, int fnz, float *nuc, int cnx, int cny, int cnz,
+                              TrView tx, TrView ty, TrView tz, int viscmod)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = (long)cnx * cny * cnz;
+    if (n >= N) return;
+    const int j = (int)(n % cny);
+    const long rest = n / cny;
+    const int i = (int)(rest % cnx), k = (int)(rest / cnx);
+    float accu = 0.f;
+    double ws = 0;
+    for (int ez = tz.gptr[k]; ez < tz.gptr[k + 1]; ez++) {
+        const int fk = tz.gf[ez];
+        const double wz = tz.gw[ez];
+        for (int ex = tx.gptr[i]; ex < tx.gptr[i + 1]; ex++) {
+            const int fi = tx.gf[ex];
+            const double wx = tx.gw[ex];
+            for (int ey = ty.gptr[j]; ey < ty.gptr[j + 1]; ey++) {
+                const int fj = ty.gf[ey];
+                const double swt = __dmul_rn(__dmul_rn(wx, ty.gw[ey]), wz);
+                const float nf = nuf[(long)fk * fnx * fny + (long)fi * fny + fj];
+                double iv = viscmod == 0 ? __dmul_rn((double)nf, swt)
+                          : viscmod == 1 ? __dmul_rn(log((double)nf), swt) : __dmul_rn(__ddiv_rn(1.0, (double)nf), swt);
+                accu = (float)__dadd_rn((double)accu, iv);
+                ws = __dadd_rn(ws, swt);
+            }
+        }
+    }
+    float r = (float)__ddiv_rn((double)accu, ws);
+    if (viscmod == 1) r = (float)exp((double)r);
+    if (viscmod == 2) r = (float)__ddiv_rn(1.0, (double)r);
+    nuc[n] = r;
+}
+
+// ------------------------------------------------------------------------------------
+// operator set-up: stress-point viscosities (sxxcalc..syzcalc nueff, move3mg.c:30-46, 402-412)
+// ------------------------------------------------------------------------------------
+struct EtaArgs {
+    int nx, ny, nz, lev0, viscmod;
+    const float *nu, *nxx, *nxy, *nxz, *nyz;
+    double nubeg, nuend;
+    double *etac, *etaxy, *etaxz, *etayz;
+    float *nd;
+};
+
+__device__ __forceinline__ double avg8(const float *nu, long v0, long NY, long NXY, int viscmod)
+{
+    const long v[8] = {v0, v0 + 1, v0 + NY, v0 + NY + 1, v0 + NXY, v0 + NXY + 1, v0 + NXY + NY, v0 + NXY + NY + 1};
+    if (viscmod == 0) {
+        float s = nu[v[0]];
+        for (int q = 1; q < 8; q++) s = __fadd_rn(s, nu[v[q]]);
+        return __ddiv_rn((double)s, 8.0);
+    }
+    double s = 0;
+    if (viscmod == 1) {
+        s = log((double)nu[v[0]]);
+        for (int q = 1; q < 8; q++) s = __dadd_rn(s, log((double)nu[v[q]]));
+        return exp(__ddiv_rn(s, 8.0));
+    }
+    s = __ddiv_rn(1.0, (double)nu[v[0]]);
+    for (int q = 1; q < 8; q++) s = __dadd_rn(s, __ddiv_rn(1.0, (double)nu[v[q]]));
+    return __ddiv_rn(1.0, __ddiv_rn(s, 8.0));
+}
+
+__device__ __forceinline__ double avg2(const float *nu, long a, long b, int viscmod)
+{
+    if (viscmod == 0) return __ddiv_rn((double)__fadd_rn(nu[a], nu[b]), 2.0);
+    if (viscmod == 1) return exp(__ddiv_rn(__dadd_rn(log((double)nu[a]), log((double)nu[b])), 2.0));
+    return __ddiv_rn(1.0, __ddiv_rn(__dadd_rn(__ddiv_rn(1.0, (double)nu[a]), __ddiv_rn(1.0, (double)nu[b])), 2.0));
+}
+
+__device__ __forceinline__ double clampnu(double n, double b, double e)
+{
+    if (n > e) n = e;
+    if (n < b) n = b;
+    return n;
+}
+
+__global__ void k_eta(EtaArgs a)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long NY = a.ny, NXY = (long)a.nx * a.ny, N = NXY * a.nz;
+    if (n >= N) return;
+    const int m2 = (int)(n % NY);
+    const long rest = n / NY;
+    const int m1 = (int)(rest % a.nx), m3 = (int)(rest / a.nx);
+    double ec = 0, exy = 0, exz = 0, eyz = 0;
+    if (m1 > 0 && m2 > 0 && m3 > 0) {
+        double v;
+        if (a.lev0 && m1 > 3 && m2 > 3 && m3 > 3 && m1 < a.nx - 3 && m2 < a.ny - 3 && m3 < a.nz - 3) v = a.nxx[n];
+        else v = avg8(a.nu, n - NXY - NY - 1, NY, NXY, a.viscmod);
+        ec = clampnu(v, a.nubeg, a.nuend);
+    }
+    if (m1 > 0 && m1 < a.nx - 1 && m2 > 0 && m2 < a.ny - 1 && m3 < a.nz - 1) {
+        double v;
+        if (a.lev0 && m1 > 3 && m2 > 3 && m3 > 2 && m1 < a.nx - 4 && m2 < a.ny - 4 && m3 < a.nz - 4) v = a.nxy[n];
+        else v = avg2(a.nu, n, n + NXY, a.viscmod);
+        exy = clampnu(v, a.nubeg, a.nuend);
+    }
+    if (m1 > 0 && m1 < a.nx - 1 && m3 > 0 && m3 < a.nz - 1 && m2 < a.ny - 1) {
+        double v;
+        if (a.lev0 && m1 > 3 && m2 > 2 && m3 > 3 && m1 < a.nx - 4 && m2 < a.ny - 4 && m3 < a.nz - 4) v = a.nxz[n];
+        else v = avg2(a.nu, n, n + 1, a.viscmod);
+        exz = clampnu(v, a.nubeg, a.nuend);
+    }
+    if (m2 > 0 && m2 < a.ny - 1 && m3 > 0 && m3 < a.nz - 1 && m1 < a.nx - 1) {
+        double v;
+        if (a.lev0 && m1 > 2 && m2 > 3 && m3 > 3 && m1 < a.nx - 4 && m2 < a.ny - 4 && m3 < a.nz - 4) v = a.nyz[n];
+        else v = avg2(a.nu, n, n + NY, a.viscmod);
+        eyz = clampnu(v, a.nubeg, a.nuend);
+    }
+    a.etac[n] = ec; a.etaxy[n] = exy; a.etaxz[n] = exz; a.etayz[n] = eyz;
+    a.nd[n] = (float)ec;
+}
+
+// scaled FP32 copies of the level operator data
+__global__ void k_eta_f32(long n, const double *ec, const double *exy, const double *exz, const double *eyz,
+                          const float *nd, float *fc, float *fxy, float *fxz, float *fyz, float *fnd, double inv_ref)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    fc[t] = (float)(ec[t] * inv_ref);
+    fxy[t] = (float)(exy[t] * inv_ref);
+    fxz[t] = (float)(exz[t] * inv_ref);
+    fyz[t] = (float)(eyz[t] * inv_ref);
+    fnd[t] = (float)((double)nd[t] * inv_ref);
+}
+
+// level-0 right-hand side (move3mg.c:751, 942, 1140) and boundary constants
+__global__ void k_rhs0(View<double> L, const float *ro, double gx, double gy, double gz)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long NY = L.ny, NXY = L.nxy, N = NXY * L.nz;
+    if (n >= N) return;
+    const int j = (int)(n % NY);
+    const long rest = n / NY;
+    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    const uint8_t b = L.bc[n];
+    L.f0[n] = 0;
+    L.f1[n] = 0; L.f2[n] = 0; L.f3[n] = 0;
+    if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(b & 2)) {
+        const float s = __fadd_rn(__fadd_rn(__fadd_rn(ro[n], ro[n + 1]), ro[n + NXY]), ro[n + NXY + 1]);
+        L.f1[n] = __ddiv_rn(__dmul_rn(-gx, (double)s), 4.0);
+    }
+    if (row_exists(2, i, j, k, L.nx, L.ny, L.nz) && !(b & 4)) {
+        const float s = __fadd_rn(__fadd_rn(__fadd_rn(ro[n], ro[n + NY]), ro[n + NXY]), ro[n + NXY + NY]);
+        L.f2[n] = __ddiv_rn(__dmul_rn(-gy, (double)s), 4.0);
+    }
+    if (row_exists(3, i, j, k, L.nx, L.ny, L.nz) && !(b & 8)) {
+        const float s = __fadd_rn(__fadd_rn(__fadd_rn(ro[n], ro[n + 1]), ro[n + NY]), ro[n + NY + 1]);
+        L.f3[n] = __ddiv_rn(__dmul_rn(-gz, (double)s), 4.0);
+    }
+}
+
+__global__ void k_bc_rhs(double *f, int n, const int *node, const double *oc)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) f[node[t]] = oc[t];
+}
+
+// load the current v,P into the level-0 solution (move3mg.c:1969-2019)
+__global__ void k_load_sol(View<double> L, const double *pr, const float *vx, const float *vy, const float *vz)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long NY = L.ny, N = L.nxy * L.nz;
+    if (n >= N) return;
+    const int j = (int)(n % NY);
+    const long rest = n / NY;
+    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    L.u0[n] = row_exists(0, i, j, k, L.nx, L.ny, L.nz) ? pr[n] : 0.0;
+    L.u1[n] = row_exists(1, i, j, k, L.nx, L.ny, L.nz) ? (double)vx[n] : 0.0;
+    L.u2[n] = row_exists(2, i, j, k, L.nx, L.ny, L.nz) ? (double)vy[n] : 0.0;
+    L.u3[n] = row_exists(3, i, j, k, L.nx, L.ny, L.nz) ? (double)vz[n] : 0.0;
+}
+
+// ------------------------------------------------------------------------------------
+// norms (deterministic two-pass block reduction)
+// ------------------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+constexpr int kRedQ = 4;   // quantities: sum r_mom^2, sum f_mom^2, sum r_cont^2, sum v^2
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_relres_part(View<T> L, double *part)
+{
+    __shared__ double sh[kRedQ][kRedThreads / 32];
+    double q[kRedQ] = {0, 0, 0, 0};
+    const long N = L.nxy * L.nz;
+    for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % L.ny);
+        const long rest = n / L.ny;
+        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        const uint8_t b = L.bc[n];
+        if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) {
+            T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); q[2] += (double)s * (double)s;
+        }
+        if (row_exists(1, i, j, k, L.nx, L.ny, L.nz)) {
+            q[3] += (double)L.u1[n] * (double)L.u1[n];
+            if (!(b & 2)) { T s = L.f1[n]; xrow<T, true>(L, i, j, k, n, s); q[0] += (double)s * s; q[1] += (double)L.f1[n] * L.f1[n]; }
+        }
+        if (row_exists(2, i, j, k, L.nx, L.ny, L.nz)) {
+            q[3] += (double)L.u2[n] * (double)L.u2[n];
+            if (!(b & 4)) { T s = L.f2[n]; yrow<T, true>(L, i, j, k, n, s); q[0] += (double)s * s; q[1] += (double)L.f2[n] * L.f2[n]; }
+        }
+        if (row_exists(3, i, j, k, L.nx, L.ny, L.nz)) {
+            q[3] += (double)L.u3[n] * (double)L.u3[n];
+            if (!(b & 8)) { T s = L.f3[n]; zrow<T, true>(L, i, j, k, n, s); q[0] += (double)s * s; q[1] += (double)L.f3[n] * L.f3[n]; }
+        }
+    }
+    const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    for (int a = 0; a < kRedQ; a++) {
+        double v = warp_sum(q[a]);
+        if (ln == 0) sh[a][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kRedQ) {
+        double v = 0;
+        for (int a = 0; a < kRedThreads / 32; a++) v += sh[threadIdx.x][a];
+        part[(long)blockIdx.x * kRedQ + threadIdx.x] = v;
+    }
+}
+
+__global__ void k_red_final(const double *part, int nblk, int nq, double *out)
+{
+    // one warp per quantity, fixed order
+    const int qi = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (qi >= nq) return;
+    double v = 0;
+    for (int b = ln; b < nblk; b += 32) v += part[(long)b * nq + qi];
+    v = warp_sum(v);
+    if (ln == 0) out[qi] = v;
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+static inline unsigned nblk(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+template <typename T>
+static T *dalloc(long n)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * (n > 0 ? n : 1)) != cudaSuccess) return nullptr;
+    return (T *)p;
+}
+
+#define ALLOC(ptr, T, n)                                                                   \
+    do {                                                                                   \
+        ptr = dalloc<T>(n);                                                                \
+        if (!ptr) return set_error(c, I3G_E_NOMEM, "cudaMalloc of %ld x %zu bytes failed", (long)(n), sizeof(T)); \
+    } while (0)
+
+template <typename T>
+static int upload(i3g_ctx *c, T *&dst, const std::vector<T> &src)
+{
+    ALLOC(dst, T, (long)src.size());
+    if (!src.empty()) I3G_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, c->st));
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// one-dimensional transfer stencil (host, FP64, the reference's expressions)
+static void build_transfer(const double *gf, int nf, const double *gc, int nc, int stag, Transfer1D &t,
+                           std::vector<int> &ha, std::vector<double> &hw0, std::vector<double> &hw1,
+                           std::vector<int> &gptr, std::vector<int> &gfv, std::vector<double> &gwv)
+{
+    ha.assign(nf, 0); hw0.assign(nf, 0); hw1.assign(nf, 0);
+    for (int m = 0; m < nf; m++) {
+        long a = (m - 2) / 2 + 2;
+        if (m < 3) a = m;
+        if (m > nf - 4) a = nc - (nf - m);
+        double d;
+        if (stag == kStagLine || stag == kStagAbs) {
+            if (a > nc - 2) a = nc - 2;
+            d = gc[a + 1] - gc[a];
+        } else if (stag == kStagMid) {
+            if (a > nc - 3) a = nc - 3;
+            if (m + 1 < nf && (gf[m] + gf[m + 1]) / 2.0 < (gc[a] + gc[a + 1]) / 2.0 && a > 0) a -= 1;
+            d = (gc[a + 2] - gc[a]) / 2.0;
+        } else {
+            if (a > nc - 2) a = nc - 2;
+            if (m > 0 && (gf[m] + gf[m - 1]) / 2.0 < (gc[a] + gc[a - 1]) / 2.0 && a > 1) a -= 1;
+            d = (gc[a + 1] - gc[a - 1]) / 2.0;
+        }
+        double w[2];
+        for (int q = 0; q < 2; q++) {
+            long k = a + q;
+            double dd;
+            if (stag == kStagAbs) {
+                dd = (gc[k] - gf[m]) / d;
+                dd = 1.0 - (dd >= 0 ? dd : -dd);
+            } else {
+                if (stag == kStagLine) dd = (gc[k] - gf[m]) / d;
+                else if (stag == kStagMid) dd = (m + 1 < nf && k + 1 < nc) ? (gc[k] + gc[k + 1] - gf[m] - gf[m + 1]) / 2.0 / d : 0.0;
+                else dd = (m > 0 && k > 0) ? (gc[k] + gc[k - 1] - gf[m] - gf[m - 1]) / 2.0 / d : 0.0;
+                if (k == a) dd = -dd;
+                dd = 1.0 - dd;
+            }
+            w[q] = dd;
+        }
+        ha[m] = (int)a; hw0[m] = w[0]; hw1[m] = w[1];
+    }
+    gptr.assign(nc + 1, 0);
+    std::vector<std::vector<std::pair<int, double>>> lists(nc);
+    for (int m = 0; m < nf; m++) {
+        if (ha[m] >= 0 && ha[m] < nc) lists[ha[m]].push_back({m, hw0[m]});
+        if (ha[m] + 1 >= 0 && ha[m] + 1 < nc) lists[ha[m] + 1].push_back({m, hw1[m]});
+    }
+    gfv.clear(); gwv.clear();
+    for (int q = 0; q < nc; q++) {
+        gptr[q] = (int)gfv.size();
+        for (auto &e : lists[q]) { gfv.push_back(e.first); gwv.push_back(e.second); }
+    }
+    gptr[nc] = (int)gfv.size();
+    t.nf = nf; t.nc = nc;
+}
+
+static int upload_transfer(i3g_ctx *c, const double *gf, int nf, const double *gc, int nc, int stag, Transfer1D &t)
+{
+    std::vector<int> ha, gptr, gfv;
+    std::vector<double> w0, w1, gwv;
+    build_transfer(gf, nf, gc, nc, stag, t, ha, w0, w1, gptr, gfv, gwv);
+    int rc;
+    if ((rc = upload(c, t.a, ha)) || (rc = upload(c, t.w0, w0)) || (rc = upload(c, t.w1, w1)) ||
+        (rc = upload(c, t.gptr, gptr)) || (rc = upload(c, t.gf, gfv)) || (rc = upload(c, t.gw, gwv)))
+        return rc;
+    return 0;
+}
+
+// staggering of each unknown along x, y, z (P cell centre; V along its own axis on grid lines)
+static const int kStag[4][3] = {{kStagCell, kStagCell, kStagCell}, {kStagLine, kStagMid, kStagMid},
+                                {kStagMid, kStagLine, kStagMid}, {kStagMid, kStagMid, kStagLine}};
+
+// inverse spacing tables: [0] 1/(g[i]-g[i-1]) at i >= 1, [1] 1/(g[i+1]-g[i-1]) at 1 <= i <= n-2
+static void inv_tables(const double *g, int n, std::vector<double> &ic, std::vector<double> &is)
+{
+    ic.assign(n + 1, 0.0); is.assign(n + 1, 0.0);
+    for (int i = 1; i < n; i++) ic[i] = 1.0 / (g[i] - g[i - 1]);
+    for (int i = 1; i < n - 1; i++) is[i] = 1.0 / (g[i + 1] - g[i - 1]);
+}
+
+static int upload_f32_scaled(i3g_ctx *c, float *&dst, const std::vector<double> &src, double scale)
+{
+    std::vector<float> f(src.size());
+    for (size_t i = 0; i < src.size(); i++) f[i] = (float)(src[i] * scale);
+    return upload(c, dst, f);
+}
+
+// Boundary rows: flatten chains to an interior partner; reject cycles, partners that are
+// not rows of the system and interior rows whose stencil leaves the grid.
+static int build_bc(i3g_ctx *c)
+{
+    const i3g_model &m = c->m;
+    const long N0 = c->nodenum;
+    long ntot = 0, mgp[I3G_MAXLEV];
+    for (int l = 0; l < c->nlev; l++) { mgp[l] = ntot; ntot += c->lev[l].n; }
+    // row -> bc record index
+    std::vector<int> rid(4 * ntot, -1);
+    for (long b = 0; b < m.bondnum; b++) {
+        long row = m.bond_row[b];
+        if (row < 0) return set_error(c, I3G_E_BC, "negative boundary row %ld", row);
+        if (row >= 8 * N0) continue;   // temperature rows are handled by the heat solver
+        if (row >= 4 * ntot) return set_error(c, I3G_E_BC, "boundary row %ld beyond the multigrid levels", row);
+        rid[row] = (int)b;
+    }
+    for (int l = 0; l < c->nlev; l++) {
+        Level &L = c->lev[l];
+        std::vector<uint8_t> mask(L.n, 0);
+        std::vector<int> node[4], pnode[4], depth[4], onode[4], ocomp[4];
+        std::vector<double> cc[4], kk[4], oc[4], ok[4];
+        for (long q = 0; q < L.n; q++) {
+            const int j = (int)(q % L.ny), i = (int)((q / L.ny) % L.nx), k = (int)(q / ((long)L.ny * L.nx));
+            for (int v = 0; v < 4; v++) {
+                long row = (mgp[l] + q) * 4 + v;
+                if (!row_exists(v, i, j, k, L.nx, L.ny, L.nz)) continue;
+                int b = rid[row];
+                if (l == 0) {
+                    if (v) c->nvel += 1;
+                    else if (b < 0) c->ncont += 1;
+                }
+                if (b < 0) {
+                    // interior row: its stencil must stay on the grid
+                    bool ok_ = true;
+                    if (v == 1) ok_ = i >= 1 && i <= L.nx - 2 && j >= 1 && j <= L.ny - 3 && k >= 1 && k <= L.nz - 3;
+                    if (v == 2) ok_ = i >= 1 && i <= L.nx - 3 && j >= 1 && j <= L.ny - 2 && k >= 1 && k <= L.nz - 3;
+                    if (v == 3) ok_ = i >= 1 && i <= L.nx - 3 && j >= 1 && j <= L.ny - 3 && k >= 1 && k <= L.nz - 2;
+                    if (!ok_) return set_error(c, I3G_E_BC, "level %d: row %d at (%d,%d,%d) has no boundary condition but its stencil leaves the grid", l, v, i, j, k);
+                    continue;
+                }
+                mask[q] |= (uint8_t)(1 << v);
+                node[v].push_back((int)q);
+                // original partner
+                long p1 = m.bond_partner1[b];
+                if (p1 > 0) {
+                    long pr = p1 - 1;
+                    if (pr / 4 < mgp[l] || pr / 4 >= mgp[l] + L.n) return set_error(c, I3G_E_BC, "boundary row %ld partners row %ld on another level", row, pr);
+                    onode[v].push_back((int)(pr / 4 - mgp[l])); ocomp[v].push_back((int)(pr % 4));
+                } else { onode[v].push_back(-1); ocomp[v].push_back(0); }
+                oc[v].push_back((double)m.bond_c[b]);
+                ok[v].push_back((double)m.bond_k[b]);
+                // flatten
+                double chc[kMaxBcDepth], chk[kMaxBcDepth];
+                int dep = 0;
+                long cur = row;
+                int pn = -1;
+                for (;;) {
+                    int bb = rid[cur];
+                    if (dep >= kMaxBcDepth) return set_error(c, I3G_E_BC, "boundary chain from row %ld longer than %d (cycle?)", row, kMaxBcDepth);
+                    chc[dep] = (double)m.bond_c[bb];
+                    long q1 = m.bond_partner1[bb];
+                    chk[dep] = q1 > 0 ? (double)m.bond_k[bb] : 0.0;
+                    dep++;
+                    if (q1 <= 0) { pn = -1; break; }
+                    long pr = q1 - 1;
+                    if (pr % 4 != v) return set_error(c, I3G_E_BC, "boundary row %ld partners another component", row);
+                    long pq = pr / 4 - mgp[l];
+                    const int pj = (int)(pq % L.ny), pi = (int)((pq / L.ny) % L.nx), pk = (int)(pq / ((long)L.ny * L.nx));
+                    if (!row_exists(v, pi, pj, pk, L.nx, L.ny, L.nz)) { pn = -1; break; }   // value stays 0
+                    if (rid[pr] < 0) { pn = (int)pq; break; }
+                    cur = pr;
+                }
+                pnode[v].push_back(pn);
+                depth[v].push_back(dep);
+                for (int d = 0; d < kMaxBcDepth; d++) {
+                    cc[v].push_back(d < dep ? chc[d] : 0.0);
+                    kk[v].push_back(d < dep ? chk[d] : 0.0);
+                }
+            }
+        }
+        int rc = upload(c, L.bc, mask);
+        if (rc) return rc;
+        for (int v = 0; v < 4; v++) {
+            BcList &B = L.bcl[v];
+            B.n = (int)node[v].size();
+            if ((rc = upload(c, B.node, node[v])) || (rc = upload(c, B.pnode, pnode[v])) ||
+                (rc = upload(c, B.depth, depth[v])) || (rc = upload(c, B.c, cc[v])) || (rc = upload(c, B.k, kk[v])) ||
+                (rc = upload(c, B.onode, onode[v])) || (rc = upload(c, B.ocomp, ocomp[v])) ||
+                (rc = upload(c, B.oc, oc[v])) || (rc = upload(c, B.ok, ok[v])))
+                return rc;
+        }
+    }
+    return 0;
+}
+
+int stokes_alloc(i3g_ctx *c)
+{
+    // level geometry (gridcheck, load3mg.c:1220-1282)
+    for (int l = 0; l < c->nlev; l++) {
+        Level &L = c->lev[l];
+        if (l == 0) { L.nx = (int)c->m.xnumx; L.ny = (int)c->m.ynumy; L.nz = (int)c->m.znumz; }
+        else {
+            L.nx = (c->lev[l - 1].nx - 5) / 2 + 5;
+            L.ny = (c->lev[l - 1].ny - 5) / 2 + 5;
+            L.nz = (c->lev[l - 1].nz - 5) / 2 + 5;
+        }
+        if (L.nx < 5 || L.ny < 5 || L.nz < 5) return set_error(c, I3G_E_ARG, "level %d has fewer than 5 nodes along an axis", l);
+        L.n = (long)L.nx * L.ny * L.nz;
+        const long s = 1L << l;
+        const double *g0[3] = {c->hgx, c->hgy, c->hgz};
+        const int n0[3] = {(int)c->m.xnumx, (int)c->m.ynumy, (int)c->m.znumz};
+        const int nl[3] = {L.nx, L.ny, L.nz};
+        double **dst[3] = {&L.gx, &L.gy, &L.gz};
+        for (int d = 0; d < 3; d++) {
+            double *g = new double[nl[d]];
+            g[0] = g0[d][0]; g[1] = g0[d][1]; g[2] = g0[d][2];
+            g[nl[d] - 1] = g0[d][n0[d] - 1]; g[nl[d] - 2] = g0[d][n0[d] - 2]; g[nl[d] - 3] = g0[d][n0[d] - 3];
+            for (int i = 3; i < nl[d] - 3; i++) g[i] = g0[d][(i - 2) * s + 2];
+            *dst[d] = g;
+        }
+    }
+    double hsum = 0;
+    hsum = (c->m.xsize / (c->m.xnumx - 1) + c->m.ysize / (c->m.ynumy - 1) + c->m.zsize / (c->m.znumz - 1)) / 3.0;
+    c->h_ref = hsum;
+    for (int l = 0; l < c->nlev; l++) {
+        Level &L = c->lev[l];
+        const long n = L.n;
+        if (l > 0) ALLOC(L.nu, float, n);
+        for (int v = 0; v < 4; v++) {
+            ALLOC(L.d.u[v], double, n); ALLOC(L.d.f[v], double, n); ALLOC(L.d.r[v], double, n);
+            ALLOC(L.s.u[v], float, n); ALLOC(L.s.f[v], float, n); ALLOC(L.s.r[v], float, n);
+            I3G_CUDA(cudaMemsetAsync(L.d.u[v], 0, n * 8, c->st)); I3G_CUDA(cudaMemsetAsync(L.d.f[v], 0, n * 8, c->st));
+            I3G_CUDA(cudaMemsetAsync(L.d.r[v], 0, n * 8, c->st));
+            I3G_CUDA(cudaMemsetAsync(L.s.u[v], 0, n * 4, c->st)); I3G_CUDA(cudaMemsetAsync(L.s.f[v], 0, n * 4, c->st));
+            I3G_CUDA(cudaMemsetAsync(L.s.r[v], 0, n * 4, c->st));
+        }
+        ALLOC(L.d.etac, double, n); ALLOC(L.d.etaxy, double, n); ALLOC(L.d.etaxz, double, n); ALLOC(L.d.etayz, double, n);
+        ALLOC(L.s.etac, float, n); ALLOC(L.s.etaxy, float, n); ALLOC(L.s.etaxz, float, n); ALLOC(L.s.etayz, float, n);
+        ALLOC(L.s.nd, float, n);
+        ALLOC(L.d.nd, float, n);
+        const double *g[3] = {L.gx, L.gy, L.gz};
+        const int nn[3] = {L.nx, L.ny, L.nz};
+        double **di[3][2] = {{&L.d.ix[0], &L.d.ix[1]}, {&L.d.iy[0], &L.d.iy[1]}, {&L.d.iz[0], &L.d.iz[1]}};
+        float **fi[3][2] = {{&L.s.ix[0], &L.s.ix[1]}, {&L.s.iy[0], &L.s.iy[1]}, {&L.s.iz[0], &L.s.iz[1]}};
+        for (int d = 0; d < 3; d++) {
+            std::vector<double> ic, is;
+            inv_tables(g[d], nn[d], ic, is);
+            int rc;
+            if ((rc = upload(c, *di[d][0], ic)) || (rc = upload(c, *di[d][1], is)) ||
+                (rc = upload_f32_scaled(c, *fi[d][0], ic, c->h_ref)) || (rc = upload_f32_scaled(c, *fi[d][1], is, c->h_ref)))
+                return rc;
+        }
+    }
+    for (int l = 0; l + 1 < c->nlev; l++) {
+        Level &F = c->lev[l], &Cc = c->lev[l + 1];
+        const double *gf[3] = {F.gx, F.gy, F.gz}, *gc[3] = {Cc.gx, Cc.gy, Cc.gz};
+        const int nf[3] = {F.nx, F.ny, F.nz}, ncn[3] = {Cc.nx, Cc.ny, Cc.nz};
+        for (int d = 0; d < 3; d++)
+            for (int s = 0; s < 4; s++) {
+                int rc = upload_transfer(c, gf[d], nf[d], gc[d], ncn[d], s, F.tr[d][s]);
+                if (rc) return rc;
+            }
+    }
+    c->red_blocks = 2 * 148;
+    ALLOC(c->dred, double, (long)c->red_blocks * kRedQ + 16);
+    if (!c->hred) I3G_CUDA(cudaMallocHost((void **)&c->hred, 64 * sizeof(double)));
+    int rc = build_bc(c);
+    if (rc) return rc;
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+void stokes_free(i3g_ctx *c)
+{
+    for (int l = 0; l < c->nlev; l++) {
+        Level &L = c->lev[l];
+        delete[] L.gx; delete[] L.gy; delete[] L.gz;
+        L.gx = L.gy = L.gz = nullptr;
+        if (l > 0) cudaFree(L.nu);
+        cudaFree(L.bc);
+        for (int v = 0; v < 4; v++) {
+            cudaFree(L.d.u[v]); cudaFree(L.d.f[v]); cudaFree(L.d.r[v]);
+            cudaFree(L.s.u[v]); cudaFree(L.s.f[v]); cudaFree(L.s.r[v]);
+            BcList &B = L.bcl[v];
+            cudaFree(B.node); cudaFree(B.pnode); cudaFree(B.depth); cudaFree(B.c); cudaFree(B.k);
+            cudaFree(B.onode); cudaFree(B.ocomp); cudaFree(B.oc); cudaFree(B.ok);
+        }
+        cudaFree(L.d.etac); cudaFree(L.d.etaxy); cudaFree(L.d.etaxz); cudaFree(L.d.etayz); cudaFree(L.d.nd);
+        cudaFree(L.s.etac); cudaFree(L.s.etaxy); cudaFree(L.s.etaxz); cudaFree(L.s.etayz); cudaFree(L.s.nd);
+        for (int a = 0; a < 2; a++) {
+            cudaFree(L.d.ix[a]); cudaFree(L.d.iy[a]); cudaFree(L.d.iz[a]);
+            cudaFree(L.s.ix[a]); cudaFree(L.s.iy[a]); cudaFree(L.s.iz[a]);
+        }
+        for (int d = 0; d < 3; d++)
+            for (int s = 0; s < 4; s++) {
+                Transfer1D &t = L.tr[d][s];
+                cudaFree(t.a); cudaFree(t.w0); cudaFree(t.w1); cudaFree(t.gptr); cudaFree(t.gf); cudaFree(t.gw);
+            }
+    }
+    cudaFree(c->dred);
+    if (c->hred) cudaFreeHost(c->hred);
+    c->hred = nullptr;
+}
+
+#define LAUNCH(kern, grid, block, ...)                                                     \
+    do {                                                                                   \
+        kern<<<(grid), (block), 0, c->st>>>(__VA_ARGS__);                                  \
+        c->launches++;                                                                     \
+    } while (0)
+
+int stokes_setup(i3g_ctx *c)
+{
+    Level &L0 = c->lev[0];
+    // restricted viscosity of coarse levels
+    for (int l = 1; l < c->nlev; l++) {
+        Level &F = c->lev[l - 1], &Cc = c->lev[l];
+        const float *nuf = l == 1 ? c->lev[0].nu : F.nu;
+        LAUNCH(k_nu_restrict, nblk(Cc.n), 256, nuf, F.nx, F.ny, F.nz, Cc.nu, Cc.nx, Cc.ny, Cc.nz,
+               trview(F.tr[0][kStagAbs]), trview(F.tr[1][kStagAbs]), trview(F.tr[2][kStagAbs]), c->p.viscmod);
+    }
+    double emin = c->p.nubeg, emax = c->p.nuend;
+    c->eta_ref = std::sqrt(emin * emax);
+    for (int l = 0; l < c->nlev; l++) {
+        Level &L = c->lev[l];
+        EtaArgs a;
+        a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.lev0 = l == 0; a.viscmod = c->p.viscmod;
+        a.nu = L.nu; a.nxx = c->nxx; a.nxy = c->nxy; a.nxz = c->nxz; a.nyz = c->nyz;
+        a.nubeg = c->p.nubeg; a.nuend = c->p.nuend;
+        a.etac = L.d.etac; a.etaxy = L.d.etaxy; a.etaxz = L.d.etaxz; a.etayz = L.d.etayz;
+        a.nd = L.d.nd;
+        LAUNCH(k_eta, nblk(L.n), 256, a);
+        LAUNCH(k_eta_f32, nblk(L.n), 256, L.n, L.d.etac, L.d.etaxy, L.d.etaxz, L.d.etayz, (const float *)a.nd,
+               L.s.etac, L.s.etaxy, L.s.etaxz, L.s.etayz, L.s.nd, 1.0 / c->eta_ref);
+        for (int v = 0; v < 4; v++) {
+            I3G_CUDA(cudaMemsetAsync(L.d.u[v], 0, L.n * 8, c->st));
+            I3G_CUDA(cudaMemsetAsync(L.d.f[v], 0, L.n * 8, c->st));
+            I3G_CUDA(cudaMemsetAsync(L.d.r[v], 0, L.n * 8, c->st));
+        }
+    }
+    View<double> V0 = view<double>(L0, L0.d);
+    LAUNCH(k_rhs0, nblk(L0.n), 256, V0, (const float *)c->ro, c->m.gxkoef, c->m.gykoef, c->m.gzkoef);
+    for (int v = 0; v < 4; v++) {
+        BcList &B = L0.bcl[v];
+        if (B.n) LAUNCH(k_bc_rhs, nblk(B.n), 256, L0.d.f[v], B.n, (const int *)B.node, (const double *)B.oc);
+    }
+    LAUNCH(k_load_sol, nblk(L0.n), 256, V0, (const double *)c->pr, (const float *)c->vx, (const float *)c->vy, (const float *)c->vz);
+    I3G_CUDA(cudaGetLastError());
+    c->stokes_ready = true;
+    return 0;
+}
+
+// ------------------------------------------------------------------------------------
+// solver drivers
+// ------------------------------------------------------------------------------------
+template <typename T>
+static Fields<T> &fields(Level &L);
+template <>
+Fields<double> &fields<double>(Level &L) { return L.d; }
+template <>
+Fields<float> &fields<float>(Level &L) { return L.s; }
+
+template <typename T>
+static void bc_apply(i3g_ctx *c, int l, int v, bool use_c)
+{
+    Level &L = c->lev[l];
+    BcList &B = L.bcl[v];
+    if (!B.n) return;
+    LAUNCH(k_bc_apply<T>, nblk(B.n), 256, fields<T>(L).u[v], B.n, (const int *)B.node, (const int *)B.pnode,
+           (const int *)B.depth, (const double *)B.c, (const double *)B.k, (int)use_c);
+}
+
+template <typename T>
+static void residual_t(i3g_ctx *c, int l)
+{
+    Level &L = c->lev[l];
+    View<T> V = view<T>(L, fields<T>(L));
+    LAUNCH(k_residual<T>, nblk(L.n), 256, V);
+    for (int v = 0; v < 4; v++) {
+        BcList &B = L.bcl[v];
+        if (B.n) LAUNCH(k_bc_residual<T>, nblk(B.n), 256, V, v, B.n, (const int *)B.node, (const int *)B.onode,
+                        (const int *)B.ocomp, (const double *)B.ok);
+    }
+}
+
+// nsweeps multicolour sweeps (gausmat4 update formula, move3mg.c:3087-3131)
+template <typename T>
+static void smooth_t(i3g_ctx *c, int l, int nsweeps, bool homogeneous, bool with_residual)
+{
+    Level &L = c->lev[l];
+    View<T> V = view<T>(L, fields<T>(L));
+    const long total = (long)((L.ny + 1) / 2) * L.nx * L.nz;
+    const T v0 = (T)c->p.v0koef, p0 = (T)c->p.p0koef;
+    const bool use_c = l == 0 && !homogeneous;
+    for (int s = 0; s < nsweeps; s++) {
+        LAUNCH((k_relax_vel<T, 1>), nblk(total), 256, V, 0, v0);
+        LAUNCH((k_relax_vel<T, 1>), nblk(total), 256, V, 1, v0);
+        bc_apply<T>(c, l, 1, use_c);
+        LAUNCH((k_relax_vel<T, 2>), nblk(total), 256, V, 0, v0);
+        LAUNCH((k_relax_vel<T, 2>), nblk(total), 256, V, 1, v0);
+        bc_apply<T>(c, l, 2, use_c);
+        LAUNCH((k_relax_vel<T, 3>), nblk(total), 256, V, 0, v0);
+        LAUNCH((k_relax_vel<T, 3>), nblk(total), 256, V, 1, v0);
+        bc_apply<T>(c, l, 3, use_c);
+        LAUNCH(k_relax_p<T>, nblk(L.n), 256, V, p0);
+        bc_apply<T>(c, l, 0, use_c);
+    }
+    if (with_residual) residual_t<T>(c, l);
+}
+
+template <typename T>
+static void restrict_t(i3g_ctx *c, int l)
+{
+    Level &F = c->lev[l - 1], &Cc = c->lev[l];
+    View<T> VF = view<T>(F, fields<T>(F)), VC = view<T>(Cc, fields<T>(Cc));
+#define RST(V_) LAUNCH((k_restrict<T, V_>), nblk(Cc.n), 256, VF, VC, trview(F.tr[0][kStag[V_][0]]), \
+                       trview(F.tr[1][kStag[V_][1]]), trview(F.tr[2][kStag[V_][2]]))
+    RST(1); RST(2); RST(3); RST(0);
+#undef RST
+}
+
+template <typename T>
+static void prolong_t(i3g_ctx *c, int l)
+{
+    Level &F = c->lev[l - 1], &Cc = c->lev[l];
+    View<T> VF = view<T>(F, fields<T>(F)), VC = view<T>(Cc, fields<T>(Cc));
+    const T kv = (T)c->p.v1koef, kp = (T)c->p.p1koef;
+#define PRL(V_, K_) LAUNCH((k_prolong<T, V_>), nblk(F.n), 256, VF, VC, trview(F.tr[0][kStag[V_][0]]), \
+                           trview(F.tr[1][kStag[V_][1]]), trview(F.tr[2][kStag[V_][2]]), K_)
+    PRL(1, kv); PRL(2, kv); PRL(3, kv); PRL(0, kp);
+#undef PRL
+}
+
+// V-cycle with the schedule of move3mg.c:2173-2213
+template <typename T>
+static void vcycle_t(i3g_ctx *c, int multinum, bool homogeneous)
+{
+    for (int l = 0; l < multinum; l++) {
+        const int n = c->p.multinnn[0][l];
+        if (n > 0) smooth_t<T>(c, l, n, homogeneous, true);
+        else residual_t<T>(c, l);
+        restrict_t<T>(c, l + 1);
+    }
+    for (int l = multinum; l > 0; l--) {
+        const int n = c->p.multinnn[1][l];
+        if (n > 0) smooth_t<T>(c, l, n, homogeneous, false);
+        prolong_t<T>(c, l);
+    }
+    if (c->p.multinnn[1][0] > 0) smooth_t<T>(c, 0, c->p.multinnn[1][0], homogeneous, false);
+}
+
+int stokes_residual(i3g_ctx *c, int level) { residual_t<double>(c, level); I3G_CUDA(cudaGetLastError()); return 0; }
+int stokes_smooth(i3g_ctx *c, int level, int nsweeps) { smooth_t<double>(c, level, nsweeps, false, true); I3G_CUDA(cudaGetLastError()); return 0; }
+int stokes_restrict(i3g_ctx *c, int level) { restrict_t<double>(c, level); I3G_CUDA(cudaGetLastError()); return 0; }
+int stokes_prolong(i3g_ctx *c, int level) { prolong_t<double>(c, level); I3G_CUDA(cudaGetLastError()); return 0; }
+int stokes_vcycle(i3g_ctx *c, int multinum) { vcycle_t<double>(c, multinum, false); I3G_CUDA(cudaGetLastError()); return 0; }
+
+// relative residuals of the level-0 system (same definition as the oracle)
+int stokes_relres(i3g_ctx *c, double *mom, double *cont)
+{
+    Level &L = c->lev[0];
+    View<double> V = view<double>(L, L.d);
+    LAUNCH(k_relres_part<double>, c->red_blocks, kRedThreads, V, c->dred);
+    LAUNCH(k_red_final, 1, 32 * kRedQ, (const double *)c->dred, c->red_blocks, kRedQ, c->dred + (long)c->red_blocks * kRedQ);
+    I3G_CUDA(cudaMemcpyAsync(c->hred, c->dred + (long)c->red_blocks * kRedQ, kRedQ * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    const double *q = c->hred;
+    *mom = q[1] > 0 ? std::sqrt(q[0] / q[1]) : std::sqrt(q[0]);
+    const double nc = (double)L.bcl[0].n, ncont = c->ncont, nvel = c->nvel;
+    (void)nc;
+    *cont = (ncont > 0 && q[3] > 0) ? std::sqrt(q[2] / ncont) * c->h_ref / std::sqrt(q[3] / nvel) : std::sqrt(q[2]);
+    return 0;
+}
+
+// ------------------------------------------------------------------------------------
+// mixed precision: FP32 multigrid on the correction inside FP64 defect correction
+// ------------------------------------------------------------------------------------
+__global__ void k_max_abs(const double *a, long n, double *part)
+{
+    __shared__ double sh[8];
+    double m = 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) m = fmax(m, fabs(a[t]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sh[w]);
+        part[blockIdx.x] = m;
+    }
+}
+
+// FP32 scaled right-hand side from the FP64 residual; boundary rows get 0
+__global__ void k_to_f32(long n, const double *r0, const double *r1, const double *r2, const double *r3,
+                         float *f0, float *f1, float *f2, float *f3, float *u0, float *u1, float *u2, float *u3,
+                         const uint8_t *bc, double sm, double sc)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint8_t b = bc[t];
+    f0[t] = (b & 1) ? 0.f : (float)(r0[t] * sc);
+    f1[t] = (b & 2) ? 0.f : (float)(r1[t] * sm);
+    f2[t] = (b & 4) ? 0.f : (float)(r2[t] * sm);
+    f3[t] = (b & 8) ? 0.f : (float)(r3[t] * sm);
+    u0[t] = 0.f; u1[t] = 0.f; u2[t] = 0.f; u3[t] = 0.f;
+}
+
+__global__ void k_add_correction(long n, double *x0, double *x1, double *x2, double *x3, const float *e0,
+                                 const float *e1, const float *e2, const float *e3, double sp, double sv)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    x0[t] += sp * (double)e0[t];
+    x1[t] += sv * (double)e1[t];
+    x2[t] += sv * (double)e2[t];
+    x3[t] += sv * (double)e3[t];
+}
+
+// ------------------------------------------------------------------------------------
+// after the solve: FP32 fields, pressure pinning, stresses, CFL (move3mg.c:2248-2632)
+// ------------------------------------------------------------------------------------
+__global__ void k_copy_back(View<double> L, long pin, double pinit, double *pr, float *vx, float *vy, float *vz, double *part)
+{
+    __shared__ double sh[4][8];
+    double m[4] = {0, 0, 0, -1e300};
+    const long N = L.nxy * L.nz;
+    const double shift = pinit - L.u0[pin];
+    for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % L.ny);
+        const long rest = n / L.ny;
+        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        if (row_exists(0, i, j, k, L.nx, L.ny, L.nz)) { pr[n] = L.u0[n] + shift; m[3] = fmax(m[3], pr[n]); }
+        if (row_exists(1, i, j, k, L.nx, L.ny, L.nz)) { vx[n] = (float)L.u1[n]; m[0] = fmax(m[0], fabs((double)vx[n])); }
+        if (row_exists(2, i, j, k, L.nx, L.ny, L.nz)) { vy[n] = (float)L.u2[n]; m[1] = fmax(m[1], fabs((double)vy[n])); }
+        if (row_exists(3, i, j, k, L.nx, L.ny, L.nz)) { vz[n] = (float)L.u3[n]; m[2] = fmax(m[2], fabs((double)vz[n])); }
+    }
+    for (int a = 0; a < 4; a++) {
+        double v = m[a];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0) sh[a][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = sh[threadIdx.x][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sh[threadIdx.x][w]);
+        part[(long)blockIdx.x * 4 + threadIdx.x] = v;
+    }
+}
+
+// strain rates and stresses from the FP32 velocities (sxxcalc..syzcalc with ynval = 0)
+__global__ void k_eps_sig(int nx, int ny, int nz, const float *vx, const float *vy, const float *vz,
+                          const double *etac, const double *etaxy, const double *etaxz, const double *etayz,
+                          const double *icx, const double *isx, const double *icy, const double *isy,
+                          const double *icz, const double *isz, float **eps, float **sig)
+{
+    const long NY = ny, NXY = (long)nx * ny, N = NXY * nz;
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int m2 = (int)(n % NY);
+    const long rest = n / NY;
+    const int m1 = (int)(rest % nx), m3 = (int)(rest / nx);
+    if (m1 > 0 && m2 > 0 && m3 > 0) {
+        const long v0 = n - NXY - NY - 1;
+        const double ne = etac[n];
+        double e;
+        e = __dmul_rn((double)__fsub_rn(vx[v0 + NY], vx[v0]), icx[m1]); eps[0][n] = (float)e; sig[0][n] = (float)__dmul_rn(__dmul_rn(2.0, ne), e);
+        e = __dmul_rn((double)__fsub_rn(vy[v0 + 1], vy[v0]), icy[m2]); eps[1][n] = (float)e; sig[1][n] = (float)__dmul_rn(__dmul_rn(2.0, ne), e);
+        e = __dmul_rn((double)__fsub_rn(vz[v0 + NXY], vz[v0]), icz[m3]); eps[2][n] = (float)e; sig[2][n] = (float)__dmul_rn(__dmul_rn(2.0, ne), e);
+    }
+    if (m1 > 0 && m1 < nx - 1 && m2 > 0 && m2 < ny - 1 && m3 < nz - 1) {
+        double e = __dadd_rn(__dmul_rn((double)__fsub_rn(vx[n], vx[n - 1]), isy[m2]),
+                             __dmul_rn((double)__fsub_rn(vy[n], vy[n - NY]), isx[m1]));
+        eps[3][n] = (float)e; sig[3][n] = (float)__dmul_rn(__dmul_rn(2.0, etaxy[n]), e);
+    }
+    if (m1 > 0 && m1 < nx - 1 && m2 < ny - 1 && m3 > 0 && m3 < nz - 1) {
+        double e = __dadd_rn(__dmul_rn((double)__fsub_rn(vx[n], vx[n - NXY]), isz[m3]),
+                             __dmul_rn((double)__fsub_rn(vz[n], vz[n - NY]), isx[m1]));
+        eps[4][n] = (float)e; sig[4][n] = (float)__dmul_rn(__dmul_rn(2.0, etaxz[n]), e);
+    }
+    if (m1 < nx - 1 && m2 > 0 && m2 < ny - 1 && m3 > 0 && m3 < nz - 1) {
+        double e = __dadd_rn(__dmul_rn((double)__fsub_rn(vy[n], vy[n - NXY]), isz[m3]),
+                             __dmul_rn((double)__fsub_rn(vz[n], vz[n - 1]), isy[m2]));
+        eps[5][n] = (float)e; sig[5][n] = (float)__dmul_rn(__dmul_rn(2.0, etayz[n]), e);
+    }
+}
+
+static int finish_solve(i3g_ctx *c, double *timestep)
+{
+    Level &L = c->lev[0];
+    View<double> V = view<double>(L, L.d);
+    const long pin = (long)c->m.pzinit * L.nx * L.ny + (long)c->m.pxinit * L.ny + c->m.pyinit;
+    const int nb = c->red_blocks;
+    LAUNCH(k_copy_back, nb, 256, V, pin, c->m.pinit, c->pr, c->vx, c->vy, c->vz, c->dred);
+    I3G_CUDA(cudaMemcpyAsync(c->hstage, c->dred, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, c->st));
+    LAUNCH(k_eps_sig, nblk(L.n), 256, L.nx, L.ny, L.nz, (const float *)c->vx, (const float *)c->vy, (const float *)c->vz,
+           (const double *)L.d.etac, (const double *)L.d.etaxy, (const double *)L.d.etaxz, (const double *)L.d.etayz,
+           (const double *)L.d.ix[0], (const double *)L.d.ix[1], (const double *)L.d.iy[0], (const double *)L.d.iy[1],
+           (const double *)L.d.iz[0], (const double *)L.d.iz[1], c->deps, c->dsig);
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    double vm[4] = {0, 0, 0, -1e300};
+    for (int b = 0; b < nb; b++)
+        for (int a = 0; a < 4; a++) vm[a] = std::max(vm[a], c->hstage[b * 4 + a]);
+    if (vm[3] > 1e12) return set_error(c, I3G_E_PRESSURE, "pressure is too big %e", vm[3]);
+    if (!(vm[0] == vm[0]) || !(vm[1] == vm[1]) || !(vm[2] == vm[2])) return set_error(c, I3G_E_NAN, "NaN velocity after the Stokes solve");
+    for (int a = 0; a < 3; a++)
+        if (vm[a] > 0) {
+            const double t = c->f.maxxystep / vm[a];
+            if (*timestep > t) *timestep = t;
+        }
+    return 0;
+}
+
+int stokes_solve(i3g_ctx *c, double *timestep)
+{
+    if (c->p.p2koef != 0 || c->f.p2koef != 0 || c->f.p2koef2 != 0)
+        return set_error(c, I3G_E_UNSUPPORTED, "p2koef != 0 (grad div terms, move3mg.c:860-889) is not supported");
+    cudaEvent_t e0, e1;
+    I3G_CUDA(cudaEventCreate(&e0));
+    I3G_CUDA(cudaEventCreate(&e1));
+    I3G_CUDA(cudaEventRecord(e0, c->st));
+    int rc = stokes_setup(c);
+    if (rc) return rc;
+    Level &L0 = c->lev[0];
+    if (!c->p.warm_start)
+        for (int v = 0; v < 4; v++) I3G_CUDA(cudaMemsetAsync(L0.d.u[v], 0, L0.n * 8, c->st));
+    // boundary rows of the initial guess consistent with their partners
+    for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
+    const int maxc = c->p.stokes_maxcyc > 0 ? c->p.stokes_maxcyc : 2000;
+    const double rtol = c->p.stokes_rtol > 0 ? c->p.stokes_rtol : 1e-8;
+    int multinum = c->f.multinum > 0 ? std::min(c->f.multinum, c->nlev - 1) : std::min(c->p.multimax, c->nlev - 1);
+    double mom, cont;
+    if ((rc = stokes_relres(c, &mom, &cont))) return rc;
+    c->st_.stokes_rel0 = std::max(mom, cont);
+    int cycles = 0, outer = 0;
+    bool conv = mom <= rtol && cont <= rtol;
+    const double p0_save = c->p.p0koef, p1_save = c->p.p1koef;
+    const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;
+    while (!conv && cycles < maxc) {
+        for (int i = 0; i < ncyc && cycles < maxc && !conv; i++) {
+            if (c->p.precision == 1) {
+                // defect correction: r = b - A x (FP64), solve A e = r with one FP32 V-cycle
+                residual_t<double>(c, 0);
+                const int nb = c->red_blocks;
+                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], L0.n, c->dred);
+                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], L0.n, c->dred + nb);
+                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], L0.n, c->dred + 2 * nb);
+                I3G_CUDA(cudaMemcpyAsync(c->hstage, c->dred, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->st));
+                I3G_CUDA(cudaStreamSynchronize(c->st));
+                double rmax = 0;
+                for (int b = 0; b < 3 * nb; b++) rmax = std::max(rmax, c->hstage[b]);
+                if (!(rmax > 0)) rmax = 1.0;
+                const double h = c->h_ref, er = c->eta_ref;
+                const double sv = rmax * h * h / er, sp = er * sv / h;
+                LAUNCH(k_to_f32, nblk(L0.n), 256, L0.n, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+                       (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
+                       L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, h * h / (er * sv), h / sv);
+                vcycle_t<float>(c, multinum, true);
+                LAUNCH(k_add_correction, nblk(L0.n), 256, L0.n, L0.d.u[0], L0.d.u[1], L0.d.u[2], L0.d.u[3],
+                       (const float *)L0.s.u[0], (const float *)L0.s.u[1], (const float *)L0.s.u[2], (const float *)L0.s.u[3], sp, sv);
+            } else {
+                vcycle_t<double>(c, multinum, false);
+            }
+            cycles++;
+            I3G_CUDA(cudaGetLastError());
+            if ((rc = stokes_relres(c, &mom, &cont))) return rc;
+            if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
+            conv = mom <= rtol && cont <= rtol;
+        }
+        outer++;
+        if (outer >= c->f.multstp && c->f.multstp > 0) {   // move3mg.c:2585-2593
+            multinum = std::min(c->f.multinum2 > 0 ? c->f.multinum2 : multinum, c->nlev - 1);
+            c->p.p0koef = c->f.p0koef2;
+            c->p.p1koef = c->f.p1koef2;
+        }
+    }
+    c->p.p0koef = p0_save;
+    c->p.p1koef = p1_save;
+    c->st_.stokes_cycles = cycles;
+    c->st_.stokes_outer = outer;
+    c->st_.stokes_rel = std::max(mom, cont);
+    c->st_.stokes_mom_rel = mom;
+    c->st_.stokes_cont_rel = cont;
+    if ((rc = finish_solve(c, timestep))) return rc;
+    I3G_CUDA(cudaEventRecord(e1, c->st));
+    I3G_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    c->st_.ms_stokes = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!conv) return set_error(c, I3G_E_NOCONV, "Stokes: %d V-cycles without reaching relative residual %g (mom %.3e cont %.3e)", cycles, rtol, mom, cont);
+    return 0;
+}
+
+// Timing of single kernel classes on level 0 with CUDA events on the context stream.
+int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes)
+{
+    if (!c->stokes_ready) {
+        int rc = stokes_setup(c);
+        if (rc) return rc;
+    }
+    Level &L = c->lev[0];
+    const double N = (double)L.n;
+    cudaEvent_t e0, e1;
+    I3G_CUDA(cudaEventCreate(&e0));
+    I3G_CUDA(cudaEventCreate(&e1));
+    View<double> V = view<double>(L, L.d);
+    View<float> Vf = view<float>(L, L.s);
+    const long total = (long)((L.ny + 1) / 2) * L.nx * L.nz;
+    // warm-up
+    for (int w = 0; w < 3; w++) {
+        if (kind == 0) LAUNCH((k_relax_vel<double, 1>), nblk(total), 256, V, 0, c->p.v0koef);
+        else if (kind == 7) LAUNCH((k_relax_vel<float, 1>), nblk(total), 256, Vf, 0, (float)c->p.v0koef);
+        else if (kind == 1) LAUNCH(k_residual<double>, nblk(L.n), 256, V);
+        else if (kind == 2 && c->nlev > 1) restrict_t<double>(c, 1);
+        else if (kind == 3 && c->nlev > 1) prolong_t<double>(c, 1);
+    }
+    I3G_CUDA(cudaEventRecord(e0, c->st));
+    for (int r = 0; r < reps; r++) {
+        if (kind == 0) LAUNCH((k_relax_vel<double, 1>), nblk(total), 256, V, r & 1, c->p.v0koef);
+        else if (kind == 7) LAUNCH((k_relax_vel<float, 1>), nblk(total), 256, Vf, r & 1, (float)c->p.v0koef);
+        else if (kind == 1) LAUNCH(k_residual<double>, nblk(L.n), 256, V);
+        else if (kind == 2 && c->nlev > 1) restrict_t<double>(c, 1);
+        else if (kind == 3 && c->nlev > 1) prolong_t<double>(c, 1);
+    }
+    I3G_CUDA(cudaEventRecord(e1, c->st));
+    I3G_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    // compulsory bytes of one launch (each datum read or written once)
+    switch (kind) {
+    case 0:   // one colour of Vx: vx, vy, vz, P, eta c/xy/xz read; rhs and writes of half the rows; bc mask
+        *bytes = N * (8.0 * 7 + 8.0 * 0.5 + 8.0 * 0.5 + 1.0); break;
+    case 7:
+        *bytes = N * (4.0 * 7 + 4.0 * 0.5 + 4.0 * 0.5 + 1.0); break;
+    case 1:   // residual: 4 unknowns, 4 rhs, 4 eta read, 4 residuals written, nd unused, bc mask
+        *bytes = N * (8.0 * 4 + 8.0 * 4 + 8.0 * 4 + 8.0 * 4 + 1.0); break;
+    case 2: { // restriction: fine residuals + bc mask + nd read, coarse rhs + sol written
+        const double Nc = (double)c->lev[1].n;
+        *bytes = N * (8.0 * 4 + 1.0 + 4.0) + Nc * (8.0 * 8 + 4.0); break;
+    }
+    case 3: { // prolongation: fine sol read+write, coarse sol read
+        const double Nc = (double)c->lev[1].n;
+        *bytes = N * 8.0 * 4 * 2 + Nc * 8.0 * 4; break;
+    }
+    default: *bytes = 0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    I3G_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace i3g

@@ -1,0 +1,146 @@
+"""ctypes binding of ``libi3g.so`` (the C ABI in ``include/i3g.h``).
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is visible, the
+constructor raises.  Every call goes through the extern "C" entry points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libi3g.so")
+
+
+class I3gError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"i3g error {abi.E_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load ``libi3g.so``; raise if it is absent (build it with ``python -m i3elvis_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise I3gError(-2, f"{LIBPATH} not built; run python -m i3elvis_b200.build")
+    L = C.CDLL(LIBPATH)
+    P = C.c_void_p
+    L.i3g_create.argtypes = [C.POINTER(abi.Model), C.POINTER(abi.Params), C.POINTER(P)]
+    L.i3g_destroy.argtypes = [P]
+    L.i3g_last_error.argtypes = [P]
+    L.i3g_last_error.restype = C.c_char_p
+    L.i3g_set_file_params.argtypes = [P, C.POINTER(abi.FileParams)]
+    L.i3g_stokes.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
+    L.i3g_heat.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
+    L.i3g_move_markers.argtypes = [P, C.c_double]
+    L.i3g_markers_to_nodes.argtypes = [P, C.c_double]
+    L.i3g_add_time.argtypes = [P, C.c_double]
+    L.i3g_download.argtypes = [P, C.POINTER(abi.Model), C.c_uint]
+    L.i3g_upload.argtypes = [P, C.POINTER(abi.Model), C.c_uint]
+    L.i3g_get_stats.argtypes = [P, C.POINTER(abi.Stats)]
+    L.i3g_get_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
+    L.i3g_set_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
+    L.i3g_stokes_setup.argtypes = [P]
+    for name in ("i3g_stokes_residual", "i3g_stokes_restrict", "i3g_stokes_prolong", "i3g_stokes_vcycles"):
+        getattr(L, name).argtypes = [P, C.c_int]
+    L.i3g_stokes_smooth.argtypes = [P, C.c_int, C.c_int]
+    L.i3g_stokes_relres.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.i3g_time_kernel.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    _lib = L
+    return L
+
+
+class Context:
+    """One model resident on the current GPU (owns an ``i3g_ctx``)."""
+
+    def __init__(self, buffers: abi.ModelBuffers, params: abi.Params, fparams: abi.FileParams = None):
+        L = load()
+        self.buf = buffers
+        self.params = params
+        self.h = C.c_void_p()
+        rc = L.i3g_create(C.byref(buffers.model), C.byref(params), C.byref(self.h))
+        if rc != 0:
+            raise I3gError(rc, L.i3g_last_error(None).decode())
+        if fparams is not None:
+            self.set_file_params(fparams)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise I3gError(rc, load().i3g_last_error(self.h).decode())
+        return rc
+
+    def call(self, name, *args):
+        return self._check(getattr(load(), name)(self.h, *args))
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().i3g_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_file_params(self, fp: abi.FileParams):
+        self.call("i3g_set_file_params", C.byref(fp))
+
+    # the four time-step calls of the host loop (i3mg.c:98-137)
+    def stokes(self, n0: int, timestep: float) -> float:
+        t = C.c_double(timestep)
+        self.call("i3g_stokes", n0, C.byref(t))
+        return t.value
+
+    def heat(self, n0: int, timestep: float) -> float:
+        t = C.c_double(timestep)
+        self.call("i3g_heat", n0, C.byref(t))
+        return t.value
+
+    def move_markers(self, timestep: float):
+        self.call("i3g_move_markers", timestep)
+
+    def markers_to_nodes(self, timestep: float):
+        self.call("i3g_markers_to_nodes", timestep)
+
+    def add_time(self, timestep: float):
+        self.call("i3g_add_time", timestep)
+
+    def download(self, mask=abi.SYNC_ALL):
+        self.call("i3g_download", C.byref(self.buf.model), mask)
+
+    def upload(self, mask=abi.SYNC_ALL):
+        self.call("i3g_upload", C.byref(self.buf.model), mask)
+
+    def stats(self) -> dict:
+        s = abi.Stats()
+        self.call("i3g_get_stats", C.byref(s))
+        return s.as_dict()
+
+    def get(self, which, level, count, dtype=np.float64):
+        out = np.zeros(count, dtype)
+        self.call("i3g_get_array", which, level, out.ctypes.data, out.nbytes)
+        return out
+
+    def set(self, which, level, arr):
+        arr = np.ascontiguousarray(arr)
+        self.call("i3g_set_array", which, level, arr.ctypes.data, arr.nbytes)
+
+    def relres(self):
+        a, b = C.c_double(), C.c_double()
+        self.call("i3g_stokes_relres", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def time_kernel(self, kind: int, reps: int):
+        ms, by = C.c_double(), C.c_double()
+        self.call("i3g_time_kernel", kind, reps, C.byref(ms), C.byref(by))
+        return ms.value, by.value

@@ -47,6 +47,8 @@ def lib():
             getattr(L, name).argtypes = [P, C.c_int, C.c_int]
         for name in ("orc_stokes_residual", "orc_stokes_restrict", "orc_stokes_prolong"):
             getattr(L, name).argtypes = [P, C.c_int]
+        L.orc_stokes_vcycles_mc.argtypes = [P, C.c_int]
+        L.orc_get_csr.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_stokes_relres.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_get_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
         L.orc_set_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
@@ -103,6 +105,16 @@ class Oracle:
     def set(self, which, level, arr):
         arr = np.ascontiguousarray(arr)
         self.call("orc_set_array", which, level, arr.ctypes.data, arr.nbytes)
+
+    def csr(self, level, nrows):
+        """Assembled rows of one level: (counts, cols, vals)."""
+        cnt = np.zeros(nrows, np.int64)
+        lib().orc_get_csr(self.h, level, cnt.ctypes.data, None, None)
+        nnz = int(cnt.sum())
+        cols = np.zeros(nnz, np.int64)
+        vals = np.zeros(nnz, np.float64)
+        lib().orc_get_csr(self.h, level, None, cols.ctypes.data, vals.ctypes.data)
+        return cnt, cols, vals
 
     def relres(self):
         a, b = C.c_double(), C.c_double()

@@ -371,3 +371,23 @@ int orc_upload(orc_ctx *o, const i3g_model *m, unsigned mask)
     }
     return 0;
 }
+
+/* V-cycles with the multicolour relaxation of the CUDA library (same schedule as
+ * move3mg.c:2173-2213; a level with zero down-leg sweeps still forms its residual). */
+int orc_stokes_vcycles_mc(orc_ctx *o, int n)
+{
+    int mn = o->f.multinum < o->nlev - 1 ? o->f.multinum : o->nlev - 1;
+    for (int i = 0; i < n; i++) {
+        for (int l = 0; l < mn; l++) {
+            if (o->p.multinnn[0][l] > 0) orc_smooth_mc(o, l, o->p.multinnn[0][l]);
+            else orc_residual(o, l);
+            orc_restrict(o, l + 1);
+        }
+        for (int l = mn; l > 0; l--) {
+            if (o->p.multinnn[1][l] > 0) orc_smooth_mc(o, l, o->p.multinnn[1][l]);
+            orc_prolong(o, l);
+        }
+        if (o->p.multinnn[1][0] > 0) orc_smooth_mc(o, 0, o->p.multinnn[1][0]);
+    }
+    return 0;
+}

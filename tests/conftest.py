@@ -1,0 +1,36 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests", "golden")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libi3g.so")
+
+
+def golden(name):
+    """Prepared (Prn, Mode, fixture dict) of a golden case: the seeded model with the nodal
+    fields and marker viscosities the reference's marker->node pass produced."""
+    import json
+    import cases
+    from i3elvis_b200 import prn as P
+    p, mode = cases.build(name)
+    fx = dict(np.load(os.path.join(ROOT, "tests", "golden", f"{name}.npz")))
+    for i, f in enumerate(P.NODE_FIELDS):
+        p.nodes[f] = fx["nodes"][i].copy()
+    p.marks["v"] = fx["markv"].copy()
+    with open(os.path.join(ROOT, "tests", "golden", f"{name}.json")) as fh:
+        fx["meta"] = json.load(fh)
+    mode.infile = "prep.prn"
+    return p, mode, fx
+
+
+@pytest.fixture(params=["sphere13", "sphere17"])
+def golden_case(request):
+    return (request.param,) + golden(request.param)

@@ -1,0 +1,117 @@
+"""CUDA Stokes multigrid against the CPU oracle (bit for bit) and the reference (converged)."""
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+from conftest import golden
+from i3elvis_b200 import abi, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(name, **solver):
+    p, mode, fx = golden(name)
+    par = abi.make_params(mode, **solver)
+    fp = abi.make_file_params(mode.files[0])
+    g = lib.Context(abi.ModelBuffers(p), par, fp)
+    o = O.Oracle(abi.ModelBuffers(p), par, fp)
+    return p, mode, fx, g, o
+
+
+def bc_rows(p, mode, level):
+    """Boolean mask [4*N_l] of boundary rows on one level."""
+    sizes = cases.level_sizes(p, mode.multinum)
+    off = int(np.sum(sizes[:level])) * 4
+    rows = p.bond["row"]
+    rows = rows[(rows >= off) & (rows < off + 4 * sizes[level])] - off
+    m = np.zeros(4 * sizes[level], bool)
+    m[rows] = True
+    return m
+
+
+@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+def test_setup_bit_exact(name):
+    p, mode, fx, g, o = pair(name)
+    g.call("i3g_stokes_setup")
+    o.call("orc_stokes_setup")
+    for l, n in enumerate(cases.level_sizes(p, mode.multinum)):
+        assert np.array_equal(g.get(abi.A_NU, l, n, np.float32), o.get(abi.A_NU, l, n, np.float32)), l
+        assert np.array_equal(g.get(abi.A_ETA, l, 4 * n), o.get(abi.A_ETA, l, 4 * n)), l
+    n0 = cases.level_sizes(p, mode.multinum)[0]
+    assert np.array_equal(g.get(abi.A_RHS, 0, 4 * n0), o.get(abi.A_RHS, 0, 4 * n0))
+    assert np.array_equal(g.get(abi.A_SOL, 0, 4 * n0), o.get(abi.A_SOL, 0, 4 * n0))
+
+
+@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+def test_residual_smooth_transfer_bit_exact(name):
+    p, mode, fx, g, o = pair(name)
+    g.call("i3g_stokes_setup")
+    o.call("orc_stokes_setup")
+    rng = np.random.default_rng(11)
+    sizes = cases.level_sizes(p, mode.multinum)
+    for l, n in enumerate(sizes):
+        x = rng.standard_normal(4 * n) * 1e-9
+        x[0::4] *= 1e9
+        g.set(abi.A_SOL, l, x); o.set(abi.A_SOL, l, x)
+        if l > 0:
+            f = rng.standard_normal(4 * n) * 1e4
+            f[bc_rows(p, mode, l)] = 0.0
+            g.set(abi.A_RHS, l, f); o.set(abi.A_RHS, l, f)
+        g.call("i3g_stokes_residual", l); o.call("orc_stokes_residual", l)
+        assert np.array_equal(g.get(abi.A_RES, l, 4 * n), o.get(abi.A_RES, l, 4 * n)), ("residual", l)
+        g.call("i3g_stokes_smooth", l, 3); o.call("orc_stokes_smooth", l, 3)
+        assert np.array_equal(g.get(abi.A_SOL, l, 4 * n), o.get(abi.A_SOL, l, 4 * n)), ("smooth", l)
+        assert np.array_equal(g.get(abi.A_RES, l, 4 * n), o.get(abi.A_RES, l, 4 * n)), ("smooth res", l)
+    for l in range(1, len(sizes)):
+        g.call("i3g_stokes_restrict", l); o.call("orc_stokes_restrict", l)
+        assert np.array_equal(g.get(abi.A_RHS, l, 4 * sizes[l]), o.get(abi.A_RHS, l, 4 * sizes[l])), ("restrict", l)
+        xc = rng.standard_normal(4 * sizes[l])
+        g.set(abi.A_SOL, l, xc); o.set(abi.A_SOL, l, xc)
+        g.call("i3g_stokes_prolong", l); o.call("orc_stokes_prolong", l)
+        assert np.array_equal(g.get(abi.A_SOL, l - 1, 4 * sizes[l - 1]), o.get(abi.A_SOL, l - 1, 4 * sizes[l - 1])), ("prolong", l)
+
+
+@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+def test_vcycles_bit_exact(name):
+    p, mode, fx, g, o = pair(name)
+    g.call("i3g_stokes_setup")
+    o.call("orc_stokes_setup")
+    g.call("i3g_stokes_vcycles", 3)
+    o.call("orc_stokes_vcycles_mc", 3)
+    for l, n in enumerate(cases.level_sizes(p, mode.multinum)):
+        assert np.array_equal(g.get(abi.A_SOL, l, 4 * n), o.get(abi.A_SOL, l, 4 * n)), l
+    gm, gc = g.relres()
+    om, oc = o.relres()
+    assert np.isclose(gm, om, rtol=1e-12) and np.isclose(gc, oc, rtol=1e-12)
+
+
+def _compare_to_reference(p, sol, ref, tol):
+    got = sol.reshape(-1, 4)
+    ref = ref.reshape(-1, 4)
+    x, y, z = p.shape
+    kk, ii, jj = np.meshgrid(np.arange(z), np.arange(x), np.arange(y), indexing="ij")
+    has_p = ((ii > 0) & (jj > 0) & (kk > 0)).reshape(-1)
+    pin = (p.head["pzinit"] * x + p.head["pxinit"]) * y + p.head["pyinit"]
+    errs = [np.linalg.norm(got[:, k] - ref[:, k]) / np.linalg.norm(ref[:, k]) for k in (1, 2, 3)]
+    gp = (got[:, 0] - got[pin, 0])[has_p]
+    rp = (ref[:, 0] - ref[pin, 0])[has_p]
+    errs.append(np.linalg.norm(gp - rp) / np.linalg.norm(rp))
+    assert max(errs) < tol, errs
+    return errs
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+def test_solve_matches_reference(name, precision):
+    """Converged velocity and pressure equal the reference's converged FP64 solution to
+    relative L2 1e-8 (FP64 multigrid and FP32 multigrid inside FP64 defect correction)."""
+    p, mode, fx = golden(name)
+    par = abi.make_params(mode, stokes_rtol=1e-11, stokes_maxcyc=3000, precision=precision)
+    g = lib.Context(abi.ModelBuffers(p), par, abi.make_file_params(mode.files[0]))
+    dt = g.stokes(0, 1e30)
+    st = g.stats()
+    assert st["stokes_rel"] <= 1e-11
+    n0 = cases.level_sizes(p, mode.multinum)[0]
+    _compare_to_reference(p, g.get(abi.A_SOL, 0, 4 * n0), fx["solve_sol"], 1e-8)
+    assert 0 < dt < 1e30
