@@ -1,13 +1,992 @@
-// markers.cu -- marker advection (movemark, mark3mg.c:2-397) and marker->node averaging
-// (ronurecalc, mark3mg.c:404-1015).
+// markers.cu -- marker advection (movemark, mark3mg.c:2-397) and marker -> node averaging
+// (ronurecalc, mark3mg.c:404-1015) for sm_100a.
+//
+// Markers live on the device as structure-of-arrays and are kept ordered by cell tile
+// (4 x 32 x 4 cells): after every advection a counting sort by tile regroups them, so the
+// marker -> node pass can give each CTA one tile, stage the tile's node sums in shared
+// memory (FP64) and touch global memory only once per node instead of once per marker.
+// The reference's scatter (mark3mg.c:848-924) adds into shared node arrays from many
+// threads without atomics; here the only global atomics are for nodes on tile faces,
+// after the marker loop.  An original-index array lets downloads return markers in the
+// reference's order.
+//
+// This file is compiled with -fmad=false so that the interpolation arithmetic rounds like
+// the CPU restatement (transcendentals may still differ in the last unit).
+#include <algorithm>
+#include <cmath>
+#include <vector>
 #include "heat_markers.cuh"
 
 namespace i3g {
-int markers_alloc(i3g_ctx *) { return 0; }
-void markers_free(i3g_ctx *) {}
-int markers_upload(i3g_ctx *, const i3g_model *) { return 0; }
-int markers_download(i3g_ctx *, i3g_model *) { return 0; }
-int markers_move(i3g_ctx *c, double) { return set_error(c, I3G_E_UNSUPPORTED, "markers not built yet"); }
-int markers_to_nodes(i3g_ctx *c, double) { return set_error(c, I3G_E_UNSUPPORTED, "markers not built yet"); }
-int markers_time_kernel(i3g_ctx *c, int, int, double *, double *) { return set_error(c, I3G_E_UNSUPPORTED, "markers not built yet"); }
+
+constexpr int TX = 4, TY = 32, TZ = 4;                       // cells per tile
+constexpr int NBX = TX + 1, NBY = TY + 1, NBZ = TZ + 1;       // nodes per tile box
+constexpr int NBOX = NBX * NBY * NBZ;
+enum { A_NU, W_NU, A_XX, W_XX, A_XY, W_XY, A_XZ, W_XZ, A_YZ, W_YZ, A_RO, A_CP, A_KT, A_HT, A_ET, A_TK, A_RR, W_P, NACC };
+enum { R_N0, R_N1, R_S0, R_S1, R_NU, R_DH, R_DV, R_SS, R_MM, R_LL, R_A0, R_A1, R_B0, R_B1, R_E0, R_E1,
+       R_RO, R_BB, R_AA, R_CP, R_KT, R_KF, R_KP, R_HT };
+enum { ERR_TYPE = 1, ERR_GRAIN = 2, ERR_WATER = 4, ERR_MELT = 8, ERR_DENSI = 16 };
+
+struct Marks {
+    float *x, *y, *z, *k, *w, *d, *v, *e, *ex, *ft, *rr, *rn;
+    int8_t *t;
+    int *id;
+};
+
+struct MarkerState {
+    long n = 0;
+    Marks a{}, b{};                 // current arrays and the sort target
+    int *key = nullptr;             // tile per marker (ntiles = not scattered)
+    int *cnt = nullptr, *off = nullptr, *cur = nullptr;
+    int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
+    double *acc = nullptr;          // [NACC * nodenum] node sums
+    float *tk1 = nullptr;           // copy of T before boundary rows
+    double *rock = nullptr;         // [24 * rocknum]
+    int *err = nullptr, *herr = nullptr;
+    int tbc_n = 0;                  // temperature boundary rows (level 0)
+    int *tbc_node = nullptr, *tbc_p = nullptr;
+    double *tbc_c = nullptr, *tbc_k = nullptr;
+    bool sorted = false;
+};
+
+static MarkerState *ms(i3g_ctx *c) { return (MarkerState *)c->mk; }
+
+// ------------------------------------------------------------------------------------
+// device-side physics (same expressions as the CPU restatement)
+// ------------------------------------------------------------------------------------
+struct Grid {
+    int nx, ny, nz;
+    double xsize, ysize, zsize;
+    const double *gx, *gy, *gz;     // shared-memory copies inside kernels
+};
+
+__device__ __forceinline__ int bsearch_g(const double *g, int n, double x)
+{
+    int a = 0, b = n - 1, m;
+    do {
+        m = (a + b) / 2;
+        if (g[m] > x) b = m; else a = m;
+    } while ((b - a) > 1);
+    if (a > n - 2) a = n - 2;
+    return a;
+}
+
+__device__ __forceinline__ double clamp01(double d) { return d < 0 ? 0.0 : (d > 1.0 ? 1.0 : d); }
+
+struct NodeF {
+    const float *vx, *vy, *vz;
+    const float *e[6], *s[6];
+    const double *pr;
+    long NY, NXY;
+};
+
+// vxyzcalc1 (mark3mg.c:2347-2530)
+__device__ void vxyz(const Grid &G, const NodeF &F, double x, double y, double z, double *v, int *wn)
+{
+    const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
+    const int X = G.nx, Y = G.ny, Z = G.nz;
+    v[0] = v[1] = v[2] = 0;
+    if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
+    if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
+    const int m1 = wn[0] = bsearch_g(gx, X, x), m2 = wn[1] = bsearch_g(gy, Y, y), m3 = wn[2] = bsearch_g(gz, Z, z);
+    int a, b, c;
+    double dx, dy, dz, ddx, ddy, ddz;
+    a = m1; if (a < 0) a = 0; if (a > X - 2) a = X - 2;
+    b = m2; if (y < (gy[b] + gy[b + 1]) / 2.0) b -= 1; if (b < 0) b = 0; if (b > Y - 3) b = Y - 3;
+    c = m3; if (z < (gz[c] + gz[c + 1]) / 2.0) c -= 1; if (c < 0) c = 0; if (c > Z - 3) c = Z - 3;
+    dx = gx[a + 1] - gx[a]; dy = (gy[b + 2] - gy[b]) / 2.0; dz = (gz[c + 2] - gz[c]) / 2.0;
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = ((gz[k3] + gz[k3 + 1]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = (gx[k1] - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = ((gy[k2] + gy[k2 + 1]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
+                v[0] += (double)F.vx[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
+            }
+        }
+    }
+    a = m1; if (x < (gx[a] + gx[a + 1]) / 2.0) a -= 1; if (a < 0) a = 0; if (a > X - 3) a = X - 3;
+    b = m2; if (b < 0) b = 0; if (b > Y - 2) b = Y - 2;
+    c = m3; if (z < (gz[c] + gz[c + 1]) / 2.0) c -= 1; if (c < 0) c = 0; if (c > Z - 3) c = Z - 3;
+    dx = (gx[a + 2] - gx[a]) / 2.0; dy = gy[b + 1] - gy[b]; dz = (gz[c + 2] - gz[c]) / 2.0;
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = ((gz[k3] + gz[k3 + 1]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = ((gx[k1] + gx[k1 + 1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = (gy[k2] - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
+                v[1] += (double)F.vy[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
+            }
+        }
+    }
+    a = m1; if (x < (gx[a] + gx[a + 1]) / 2.0) a -= 1; if (a < 0) a = 0; if (a > X - 3) a = X - 3;
+    b = m2; if (y < (gy[b] + gy[b + 1]) / 2.0) b -= 1; if (b < 0) b = 0; if (b > Y - 3) b = Y - 3;
+    c = m3; if (c < 0) c = 0; if (c > Z - 2) c = Z - 2;
+    dx = (gx[a + 2] - gx[a]) / 2.0; dy = (gy[b + 2] - gy[b]) / 2.0; dz = gz[c + 1] - gz[c];
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = (gz[k3] - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = ((gx[k1] + gx[k1 + 1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = ((gy[k2] + gy[k2 + 1]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
+                v[2] += (double)F.vz[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
+            }
+        }
+    }
+}
+
+// epscalc1 with the cell given (mark3mg.c:2535-2838)
+__device__ void eps_at(const Grid &G, const NodeF &F, double x, double y, double z, const int *wn, double *e,
+                       double *s, double *dis)
+{
+    const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
+    const int X = G.nx, Y = G.ny, Z = G.nz;
+    for (int i = 0; i < 7; i++) e[i] = 0;
+    for (int i = 0; i < 6; i++) s[i] = 0;
+    *dis = 0;
+    if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
+    if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
+    const int m1 = wn[0], m2 = wn[1], m3 = wn[2];
+    int a, b, c;
+    double dx, dy, dz, ddx, ddy, ddz, w;
+    a = m1; if (x > (gx[a] + gx[a + 1]) / 2.0) a += 1; if (a < 1) a = 1; if (a > X - 2) a = X - 2;
+    b = m2; if (y > (gy[b] + gy[b + 1]) / 2.0) b += 1; if (b < 1) b = 1; if (b > Y - 2) b = Y - 2;
+    c = m3; if (z > (gz[c] + gz[c + 1]) / 2.0) c += 1; if (c < 1) c = 1; if (c > Z - 2) c = Z - 2;
+    dx = (gx[a + 1] - gx[a - 1]) / 2.0; dy = (gy[b + 1] - gy[b - 1]) / 2.0; dz = (gz[c + 1] - gz[c - 1]) / 2.0;
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = ((gz[k3 - 1] + gz[k3]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = clamp01(1.0 - ddz);
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = ((gx[k1 - 1] + gx[k1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = clamp01(1.0 - ddx);
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = ((gy[k2 - 1] + gy[k2]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = clamp01(1.0 - ddy);
+                const long n = k3 * F.NXY + (long)k1 * F.NY + k2;
+                w = ddx * ddy * ddz;
+                const float exx = F.e[0][n], eyy = F.e[1][n], ezz = F.e[2][n];
+                const float sxx = F.s[0][n], syy = F.s[1][n], szz = F.s[2][n];
+                e[0] += exx * w; e[1] += eyy * w; e[2] += ezz * w;
+                s[0] += sxx * w; s[1] += syy * w; s[2] += szz * w;
+                *dis += (double)(__fadd_rn(__fadd_rn(__fmul_rn(sxx, exx), __fmul_rn(syy, eyy)), __fmul_rn(szz, ezz))) * w;
+                e[6] += F.pr[n] * w;
+            }
+        }
+    }
+    a = m1; if (a < 1) a = 1; if (a > X - 3) a = X - 3;
+    b = m2; if (b < 1) b = 1; if (b > Y - 3) b = Y - 3;
+    c = m3; if (z < (gz[c] + gz[c + 1]) / 2.0) c -= 1; if (c < 0) c = 0; if (c > Z - 3) c = Z - 3;
+    dx = gx[a + 1] - gx[a]; dy = gy[b + 1] - gy[b]; dz = (gz[c + 2] - gz[c]) / 2.0;
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = ((gz[k3] + gz[k3 + 1]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = clamp01(1.0 - ddz);
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = (gx[k1] - x) / dx; if (k1 == a) ddx = -ddx; ddx = clamp01(1.0 - ddx);
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = (gy[k2] - y) / dy; if (k2 == b) ddy = -ddy; ddy = clamp01(1.0 - ddy);
+                const long n = k3 * F.NXY + (long)k1 * F.NY + k2;
+                w = ddx * ddy * ddz;
+                e[3] += F.e[3][n] * w; s[3] += F.s[3][n] * w;
+                *dis += 2.0 * F.s[3][n] * F.e[3][n] * w;
+            }
+        }
+    }
+    a = m1; if (a < 1) a = 1; if (a > X - 3) a = X - 3;
+    b = m2; if (y < (gy[b] + gy[b + 1]) / 2.0) b -= 1; if (b < 0) b = 0; if (b > Y - 3) b = Y - 3;
+    c = m3; if (c < 1) c = 1; if (c > Z - 3) c = Z - 3;
+    dx = gx[a + 1] - gx[a]; dy = (gy[b + 2] - gy[b]) / 2.0; dz = gz[c + 1] - gz[c];
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = (gz[k3] - z) / dz; if (k3 == c) ddz = -ddz; ddz = clamp01(1.0 - ddz);
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = (gx[k1] - x) / dx; if (k1 == a) ddx = -ddx; ddx = clamp01(1.0 - ddx);
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = ((gy[k2] + gy[k2 + 1]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = clamp01(1.0 - ddy);
+                const long n = k3 * F.NXY + (long)k1 * F.NY + k2;
+                w = ddx * ddy * ddz;
+                e[4] += F.e[4][n] * w; s[4] += F.s[4][n] * w;
+                *dis += 2.0 * F.s[4][n] * F.e[4][n] * w;
+            }
+        }
+    }
+    a = m1; if (x < (gx[a] + gx[a + 1]) / 2.0) a -= 1; if (a < 0) a = 0; if (a > X - 3) a = X - 3;
+    b = m2; if (b < 1) b = 1; if (b > Y - 3) b = Y - 3;
+    c = m3; if (c < 1) c = 1; if (c > Z - 3) c = Z - 3;
+    dx = (gx[a + 2] - gx[a]) / 2.0; dy = gy[b + 1] - gy[b]; dz = gz[c + 1] - gz[c];
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = (gz[k3] - z) / dz; if (k3 == c) ddz = -ddz; ddz = clamp01(1.0 - ddz);
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = ((gx[k1] + gx[k1 + 1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = clamp01(1.0 - ddx);
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = (gy[k2] - y) / dy; if (k2 == b) ddy = -ddy; ddy = clamp01(1.0 - ddy);
+                const long n = k3 * F.NXY + (long)k1 * F.NY + k2;
+                w = ddx * ddy * ddz;
+                e[5] += F.e[5][n] * w; s[5] += F.s[5][n] * w;
+                *dis += 2.0 * F.s[5][n] * F.e[5][n] * w;
+            }
+        }
+    }
+}
+
+// prcalc1 (mark3mg.c:2917-3001)
+__device__ double pr_at(const Grid &G, const double *pr, long NY, long NXY, double x, double y, double z, int *wn)
+{
+    const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
+    const int X = G.nx, Y = G.ny, Z = G.nz;
+    if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
+    if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
+    const int m1 = wn[0] = bsearch_g(gx, X, x), m2 = wn[1] = bsearch_g(gy, Y, y), m3 = wn[2] = bsearch_g(gz, Z, z);
+    int a = m1, b = m2, c = m3;
+    if (x > (gx[a] + gx[a + 1]) / 2.0) a += 1; if (a < 1) a = 1; if (a > X - 2) a = X - 2;
+    if (y > (gy[b] + gy[b + 1]) / 2.0) b += 1; if (b < 1) b = 1; if (b > Y - 2) b = Y - 2;
+    if (z > (gz[c] + gz[c + 1]) / 2.0) c += 1; if (c < 1) c = 1; if (c > Z - 2) c = Z - 2;
+    const double dx = (gx[a + 1] - gx[a - 1]) / 2.0, dy = (gy[b + 1] - gy[b - 1]) / 2.0, dz = (gz[c + 1] - gz[c - 1]) / 2.0;
+    double p = 0, ddx, ddy, ddz;
+    for (int k3 = c; k3 <= c + 1; k3++) {
+        ddz = ((gz[k3 - 1] + gz[k3]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
+        for (int k1 = a; k1 <= a + 1; k1++) {
+            ddx = ((gx[k1 - 1] + gx[k1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
+            for (int k2 = b; k2 <= b + 1; k2++) {
+                ddy = ((gy[k2 - 1] + gy[k2]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
+                p += pr[k3 * NXY + (long)k1 * NY + k2] * (ddx * ddy * ddz);
+            }
+        }
+    }
+    return p;
+}
+
+struct Phys {
+    const double *rock;   // [24 * rocknum]
+    int rocknum, densimod, viscmod, outgrid, markmod;
+    double nubeg, nuend, nukoef, healrate, timesum;
+    double zdeep, vdeep, tdeep, nudeep, teclmin, teclmax, eroslev, sedilev, waterlev;
+    int *err;
+};
+
+__device__ __forceinline__ double RK(const Phys &P, int f, int t) { return P.rock[f * P.rocknum + t]; }
+
+// viscalc (mark3mg.c:1114-1693): rheologies A-D, F + brittle; updates the strain sign and the
+// formation time like the reference.  Returns -1 for the grain-damage rheology.
+__device__ double visc(const Phys &P, double mtk, double mpb, int mm2, double epsin, double markrii1, float &me, float &mft)
+{
+    const double rt = 8.314 * mtk;
+    double e1, k1, sduct, sbrit;
+    const double strain = fabs((double)me);
+    const double lamb = 1.0;
+    double abrit = RK(P, R_A0, mm2), bbrit = RK(P, R_B0, mm2);
+    const double E0 = RK(P, R_E0, mm2), E1 = RK(P, R_E1, mm2);
+    if (strain > E1) { abrit = RK(P, R_A1, mm2); bbrit = RK(P, R_B1, mm2); }
+    else if (strain > E0 && E1 > E0) {
+        abrit = RK(P, R_A0, mm2) + (RK(P, R_A1, mm2) - RK(P, R_A0, mm2)) * (strain - E0) / (E1 - E0);
+        bbrit = RK(P, R_B0, mm2) + (RK(P, R_B1, mm2) - RK(P, R_B0, mm2)) * (strain - E0) / (E1 - E0);
+    }
+    const double mpf = mpb * 1e+5;
+    double nubrit = 0;
+    if (epsin > 0 && (bbrit > 0 || abrit * lamb > 0) && mm2 > 1) {
+        sbrit = abrit + bbrit * mpf * lamb;
+        if (mpf < 0) sbrit = abrit + mpf;
+        if (sbrit > 0) nubrit = 1.0 / (0.5 * sbrit / epsin / markrii1);
+        else nubrit = 1.0 / RK(P, R_N0, mm2);
+    }
+    double nunewt = 0, nupowl = 0;
+    const double nu = RK(P, R_NU, mm2), dh = RK(P, R_DH, mm2), dv = RK(P, R_DV, mm2), ss = RK(P, R_SS, mm2), mm = RK(P, R_MM, mm2);
+    if (nu != 0) {
+        if (dh == 0 && dv == 0 && (ss == 0 || mm == 1.0)) nunewt = 1.0 / nu;
+        if ((dh != 0 || dv != 0) && (ss == 0 || mm == 1.0)) {
+            e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            if (dh < 0 && dv > 0) { e1 = dh * (mtk - dv); if (e1 < -150.0) e1 = -150.0; }
+            if (dh < 0 && dv < 0) { e1 = (-dh) * (1.0 - (mtk - (-dv)) / (-dv)) / 8.314 / (-dv); if (e1 > 150.0) e1 = 150.0; }
+            nunewt = 1.0 / (nu * exp(e1));
+        }
+        if ((dh == 0 && dv == 0) && ss != 0 && mm != 1.0) {
+            k1 = nu / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1);
+            sduct = pow(nu * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+        if (nu > 0 && dh > 0 && (dh != 0 || dv != 0) && ss != 0 && mm != 1.0) {
+            e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            e1 = exp(e1);
+            k1 = nu / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1 * e1);
+            sduct = pow(nu * e1 * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+        if (nu < 0) {
+            e1 = (ss + mpb * RK(P, R_LL, mm2)) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            e1 = exp(e1);
+            nunewt = 1.0 / (0.5 * pow(1.0 * 1e-3 / 5e-10, 2.5) * 8e+10 / RK(P, R_S1, mm2) * e1);
+            nupowl = 0;
+            if (epsin > 0) {
+                e1 = (dh + dv * mpb) / rt / mm;
+                if (e1 > 150.0) e1 = 150.0;
+                e1 = exp(e1);
+                nupowl = 1.0 / (0.5 * pow(epsin, 1.0 / mm - 1.0) * 8e+10 / pow(-nu, 1.0 / mm) * e1);
+            }
+        }
+        if (dh < 0) return -1;
+    }
+    double nueff = nunewt + nupowl;
+    if (mm2 == 7 || mm2 == 8 || mm2 == 9 || mm2 == 10) {
+        if (mtk > 1300.0) mft = 0;
+        else if (mft <= 0) mft = (float)P.timesum;
+    }
+    if (nubrit > nueff) {
+        nueff = nubrit;
+        if (me == 0) me = 1e-20f;
+        me = fabsf(me);
+    } else {
+        me = -fabsf(me);
+    }
+    if (nueff <= 0) nueff = 1.0 / RK(P, R_N1, mm2);
+    nueff = 1.0 / nueff;
+    if (nueff < RK(P, R_N0, mm2)) nueff = RK(P, R_N0, mm2);
+    if (nueff > RK(P, R_N1, mm2)) nueff = RK(P, R_N1, mm2);
+    if (nueff < P.nubeg) nueff = P.nubeg;
+    if (nueff > P.nuend) nueff = P.nuend;
+    return nueff;
+}
+
+__device__ __forceinline__ void load_grid(const Grid &Gg, double *sh, Grid &G)
+{
+    const int n = Gg.nx + Gg.ny + Gg.nz;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        sh[i] = i < Gg.nx ? Gg.gx[i] : i < Gg.nx + Gg.ny ? Gg.gy[i - Gg.nx] : Gg.gz[i - Gg.nx - Gg.ny];
+    __syncthreads();
+    G = Gg;
+    G.gx = sh; G.gy = sh + Gg.nx; G.gz = sh + Gg.nx + Gg.ny;
+}
+
+__device__ __forceinline__ double inv2(const double *e)
+{
+    return pow(0.5 * (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]) + e[3] * e[3] + e[4] * e[4] + e[5] * e[5], 0.5);
+}
+
+// ------------------------------------------------------------------------------------
+// movemark: rheology update + RK4 (mark3mg.c:49-310)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
+{
+    extern __shared__ double shg[];
+    Grid G;
+    load_grid(Gg, shg, G);
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int t = M.t[i];
+    const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+    const bool inbox = fx >= 0 && fy >= 0 && fz >= 0 && (double)fx <= G.xsize && (double)fy <= G.ysize && (double)fz <= G.zsize;
+    if (!(inbox || (P.outgrid != 1 && (t < 50 || t >= 100)))) return;
+    if (t >= 50) { atomicOr(P.err, ERR_TYPE); return; }
+    const double yold = fy;
+    double v1[3], e[7], s[6], dis;
+    int wn[3];
+    vxyz(G, F, fx, fy, fz, v1, wn);
+    eps_at(G, F, fx, fy, fz, wn, e, s, &dis);
+    const double eii = inv2(e), sii = inv2(s);
+    const double mpb = e[6] * 1e-5;
+    float mk = M.k[i], mv = M.v[i], me = M.e[i], mft = M.ft[i], mw = M.w[i];
+    const double mtk = mk;
+    if (t < 50 && mtk > 0) {
+        double rii = 1.0;
+        if (mv > 0 && fx > G.gx[3] && fx < G.gx[G.nx - 4] && fy > G.gy[3] && fy < G.gy[G.ny - 4] && fz > G.gz[3] && fz < G.gz[G.nz - 4])
+            rii *= pow(0.5 * sii / eii / mv, 0.87);
+        const double mnu = visc(P, mtk, mpb, t, eii, rii, me, mft);
+        if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); return; }
+        mv = (float)mnu;
+        if (me > 0) me += timestep * eii;
+        if (me > 0) { me -= timestep * P.healrate; if (me < 0) me = 0; }
+        else { me += timestep * P.healrate; if (me > 0) me = 0; }
+    }
+    double v[3];
+    if (P.markmod == 1) { v[0] = v1[0]; v[1] = v1[1]; v[2] = v1[2]; }
+    else {
+        double v2[3], v3[3], v4[3];
+        vxyz(G, F, fx + v1[0] * timestep / 2.0, fy + v1[1] * timestep / 2.0, fz + v1[2] * timestep / 2.0, v2, wn);
+        vxyz(G, F, fx + v2[0] * timestep / 2.0, fy + v2[1] * timestep / 2.0, fz + v2[2] * timestep / 2.0, v3, wn);
+        vxyz(G, F, fx + v3[0] * timestep, fy + v3[1] * timestep, fz + v3[2] * timestep, v4, wn);
+        for (int k = 0; k < 3; k++) v[k] = (v1[k] + 2.0 * v2[k] + 2.0 * v3[k] + v4[k]) / 6.0;
+    }
+    if (P.outgrid == 2) {
+        if (fx < 0 || (double)fx > G.xsize) v[1] = v[2] = 0;
+        if (fy < 0 || (double)fy > G.ysize) v[0] = v[2] = 0;
+        if (fz < 0 || (double)fz > G.zsize) v[0] = v[1] = 0;
+    }
+    if (fy > P.zdeep && v[1] < 0 && mk < P.tdeep && t == 10) mk = (float)P.tdeep;
+    if (fy > P.zdeep && v[1] < 0 && t != 10) { t = 10; mw = 0; }
+    if (fy > P.zdeep && t != 10 && t != 9) { t = 9; mw = 0; }
+    const float nx_ = (float)(fx + (timestep * v[0] - 0.0));
+    const float ny_ = (float)(fy + timestep * v[1]);
+    const float nz_ = (float)(fz + timestep * v[2]);
+    if ((yold > P.vdeep && ny_ < P.vdeep) || (yold > P.zdeep && ny_ < P.zdeep)) {
+        if (mk < P.tdeep) mk = (float)P.tdeep;
+        t = 10;
+    }
+    if (nx_ < 0 || ny_ < 0 || nz_ < 0 || (double)nx_ > G.xsize || (double)ny_ > G.ysize || (double)nz_ > G.zsize) {
+        mk = 0;
+        mv = 0;
+    }
+    M.x[i] = nx_; M.y[i] = ny_; M.z[i] = nz_;
+    M.k[i] = mk; M.v[i] = mv; M.e[i] = me; M.ft[i] = mft; M.w[i] = mw; M.t[i] = (int8_t)t;
+}
+
+// ------------------------------------------------------------------------------------
+// tile sort
+// ------------------------------------------------------------------------------------
+struct TileGeo { int ntx, nty, ntz, ntiles; };
+
+__device__ __forceinline__ bool r2n_active(const Grid &G, float x, float y, float z, int t, float k)
+{
+    return x > 0 && y > 0 && z > 0 && x < G.xsize && y < G.ysize && z < G.zsize && t < 50 && k > 0;
+}
+
+__global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *cnt)
+{
+    extern __shared__ double shg[];
+    Grid G;
+    load_grid(Gg, shg, G);
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int kk = T.ntiles;
+    if (i < n) {
+        const float x = M.x[i], y = M.y[i], z = M.z[i];
+        if (r2n_active(G, x, y, z, M.t[i], M.k[i])) {
+            double xd = x, yd = y, zd = z;
+            if (xd > G.xsize) xd = G.xsize;
+            if (yd > G.ysize) yd = G.ysize;
+            if (zd > G.zsize) zd = G.zsize;
+            const int c1 = bsearch_g(G.gx, G.nx, xd), c2 = bsearch_g(G.gy, G.ny, yd), c3 = bsearch_g(G.gz, G.nz, zd);
+            kk = ((c3 / TZ) * T.ntx + (c1 / TX)) * T.nty + (c2 / TY);
+        }
+        key[i] = kk;
+    }
+    // warp-aggregated histogram
+    const unsigned act = __ballot_sync(0xffffffffu, i < n);
+    if (i < n) {
+        const unsigned peers = __match_any_sync(act, kk);
+        const int leader = __ffs(peers) - 1;
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&cnt[kk], __popc(peers));
+    }
+}
+
+__global__ void k_scan(const int *cnt, int *off, int *cur, int n)
+{
+    // single block exclusive scan over n+1 bins (n up to a few hundred thousand)
+    __shared__ int part[1024];
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(n, b + per);
+    int s = 0;
+    for (int q = b; q < e; q++) s += cnt[q];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int q = 0; q < (int)blockDim.x; q++) { int v = part[q]; part[q] = run; run += v; }
+    }
+    __syncthreads();
+    int run = part[threadIdx.x];
+    for (int q = b; q < e; q++) { off[q] = run; cur[q] = run; run += cnt[q]; }
+    if (threadIdx.x == blockDim.x - 1) off[n] = run;
+}
+
+__global__ void k_tile_scatter(Marks A, Marks B, long n, const int *key, int *cur)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned act = __ballot_sync(0xffffffffu, i < n);
+    if (i >= n) return;
+    const int kk = key[i];
+    const unsigned peers = __match_any_sync(act, kk);
+    const int leader = __ffs(peers) - 1;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&cur[kk], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    const long d = base + __popc(peers & ((1u << lane) - 1));
+    B.x[d] = A.x[i]; B.y[d] = A.y[i]; B.z[d] = A.z[i]; B.k[d] = A.k[i]; B.w[d] = A.w[i]; B.d[d] = A.d[i];
+    B.v[d] = A.v[i]; B.e[d] = A.e[i]; B.ex[d] = A.ex[i]; B.ft[d] = A.ft[i]; B.rr[d] = A.rr[i]; B.rn[d] = A.rn[i];
+    B.t[d] = A.t[i]; B.id[d] = A.id[i];
+}
+
+// ------------------------------------------------------------------------------------
+// ronurecalc: one CTA per tile, FP64 node sums staged in shared memory
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void phase_density(const Phys &P, int mm2, double mtk, double mpb, double &mro)
+{
+    if ((mm2 >= 7 && mm2 <= 8) || (mm2 >= 16 && mm2 <= 18)) {   // mark3mg.c:530-587
+        double rokf = 1.0;
+        double p_ga_in = -9222.0 + mtk * 14.0; if (p_ga_in < 2000.0) p_ga_in = 2000.0;
+        double p_pl_out = -1460.0 + mtk * 20.0; if (p_pl_out < 12000.0) p_pl_out = 12000.0;
+        if (mpb > p_ga_in) { if (mpb >= p_pl_out) rokf *= 1.16; else rokf *= 1.0 + 0.16 * (mpb - p_ga_in) / (p_pl_out - p_ga_in); }
+        const double p_st_in = 59100.0 + mtk * 22.6;
+        if (mpb > p_st_in) rokf *= 1.06;
+        const double p_sp_out = 354000.0 - mtk * 40.0, p_pv_in = 352000.0 - mtk * 40.0;
+        if (mpb > p_pv_in) { if (mpb >= p_sp_out) rokf *= 1.08; else rokf *= 1.0 + 0.08 * (mpb - p_pv_in) / (p_sp_out - p_pv_in); }
+        if (mtk < P.teclmax) { if (mtk < P.teclmin) rokf = 1.00; else rokf = 1.0 + (rokf - 1.0) * (mtk - P.teclmin) / (P.teclmax - P.teclmin); }
+        mro *= rokf;
+    }
+    if (mm2 >= 9 && mm2 <= 14) {   // mark3mg.c:589-641
+        double rokf = 1.0;
+        const double p_ol_out = 91000.0 + mtk * 27.0;
+        double p_sp_in = 66000.0 + mtk * 39.0;
+        if (p_sp_in > p_ol_out - 2000.0) p_sp_in = p_ol_out - 2000.0;
+        if (mpb > p_sp_in) { if (mpb >= p_ol_out) rokf *= 1.06; else rokf *= 1.0 + 0.06 * (mpb - p_sp_in) / (p_ol_out - p_sp_in); }
+        const double p_sp_out = 304000.0 - mtk * 40.0, p_pv_in = 302000.0 - mtk * 40.0;
+        if (mpb > p_pv_in) { if (mpb >= p_sp_out) rokf *= 1.11; else rokf *= 1.0 + 0.11 * (mpb - p_pv_in) / (p_sp_out - p_pv_in); }
+        if (mtk < P.teclmax) { if (mtk < P.teclmin) rokf = 1.00; else rokf = 1.0 + (rokf - 1.0) * (mtk - P.teclmin) / (P.teclmax - P.teclmin); }
+        mro *= rokf;
+    }
+}
+
+__global__ void __launch_bounds__(512) k_r2n_tile(Marks M, const int *off, Grid Gg, NodeF F, Phys P, TileGeo T,
+                                                  double timestep, double *acc, long N)
+{
+    extern __shared__ double sm[];
+    double *sacc = sm;                          // [NACC][NBOX]
+    double *shg = sm + NACC * NBOX;             // grid lines
+    for (int q = threadIdx.x; q < NACC * NBOX; q += blockDim.x) sacc[q] = 0;
+    Grid G;
+    load_grid(Gg, shg, G);   // contains __syncthreads
+    const int tile = blockIdx.x;
+    const int ty = tile % T.nty, rest = tile / T.nty, tx = rest % T.ntx, tz = rest / T.ntx;
+    const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
+    const int beg = off[tile], end = off[tile + 1];
+    const int vm = P.viscmod;
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        int mm2 = M.t[i];
+        const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+        if (mm2 > 1 && fy < P.eroslev) { mm2 = 0; M.t[i] = 0; }
+        if (mm2 < 2) { atomicOr(P.err, ERR_WATER); continue; }
+        if (mm2 > 20) { atomicOr(P.err, ERR_MELT); continue; }
+        if (P.densimod >= 2) { atomicOr(P.err, ERR_DENSI); continue; }
+        int wn[3];
+        const double mpb = pr_at(G, F.pr, F.NY, F.NXY, fx, fy, fz, wn) * 1e-5;
+        const double mtk = M.k[i];
+        double mnu = M.v[i];
+        if (mnu <= 0 || timestep <= 0) {
+            double e[7], s[6], dis;
+            eps_at(G, F, fx, fy, fz, wn, e, s, &dis);
+            float me = M.e[i], mft = M.ft[i];
+            mnu = visc(P, mtk, mpb, mm2, inv2(e), 1.0, me, mft);
+            if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); continue; }
+            M.v[i] = (float)mnu; M.e[i] = me; M.ft[i] = mft;
+        }
+        double mbb = 0, mro = RK(P, R_RO, mm2);
+        if (P.densimod != 0) {   // dencalc1 (mark3mg.c:3006-3024)
+            const double bb = RK(P, R_BB, mm2);
+            mbb = bb / (1.0 - bb * (mtk - 298.15));
+            mro = mro * (1.0 - bb * (mtk - 298.15)) * (1.0 + RK(P, R_AA, mm2) * (mpb - 1.0) * 1e-3);
+        }
+        phase_density(P, mm2, mtk, mpb, mro);
+        const double mcp = RK(P, R_CP, mm2);
+        const double mkt = (RK(P, R_KT, mm2) + RK(P, R_KF, mm2) / (mtk + 77.0)) * exp(RK(P, R_KP, mm2) * mpb);
+        const double mht = RK(P, R_HT, mm2);
+        if (fy > P.vdeep && mnu > P.nudeep) mnu = P.nudeep;
+        if (fy < 5e+4 && fx > G.xsize - 1e+4 && fz > 1.5e+5 && fz < 8.7e+5 && mnu > 1e+19) mnu = 1e+19;
+        const int m10 = wn[0], m20 = wn[1], m30 = wn[2];
+        const double dx = G.gx[m10 + 1] - G.gx[m10], dy = G.gy[m20 + 1] - G.gy[m20], dz = G.gz[m30 + 1] - G.gz[m30];
+        const double vnu = vm == 0 ? mnu : vm == 1 ? log(mnu) : 1.0 / mnu;
+        const double mrr = M.rr[i];
+        for (int m3 = m30; m3 <= m30 + 1; m3++) {
+            double ddz = (G.gz[m3] - fz) / dz; ddz = 1.0 - fabs(ddz);
+            for (int m1 = m10; m1 <= m10 + 1; m1++) {
+                double ddx = (G.gx[m1] - fx) / dx; ddx = 1.0 - fabs(ddx);
+                for (int m2 = m20; m2 <= m20 + 1; m2++) {
+                    double ddy = (G.gy[m2] - fy) / dy; ddy = 1.0 - fabs(ddy);
+                    const double swt = ddx * ddy * ddz;
+                    const int lb = ((m3 - cz0) * NBX + (m1 - cx0)) * NBY + (m2 - cy0);
+                    double *a = sacc + lb;
+                    if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { atomicAdd(a + A_NU * NBOX, vnu * swt); atomicAdd(a + W_NU * NBOX, swt); }
+                    if (m1 > m10 && m2 > m20 && m3 > m30) {
+                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
+                        atomicAdd(a + A_XX * NBOX, vnu * w1); atomicAdd(a + W_XX * NBOX, w1);
+                    }
+                    if (m3 == m30 && ddx > 0.5 && ddy > 0.5) {
+                        const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
+                        atomicAdd(a + A_XY * NBOX, vnu * w1); atomicAdd(a + W_XY * NBOX, w1);
+                    }
+                    if (m2 == m20 && ddx > 0.5 && ddz > 0.5) {
+                        const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
+                        atomicAdd(a + A_XZ * NBOX, vnu * w1); atomicAdd(a + W_XZ * NBOX, w1);
+                    }
+                    if (m1 == m10 && ddy > 0.5 && ddz > 0.5) {
+                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
+                        atomicAdd(a + A_YZ * NBOX, vnu * w1); atomicAdd(a + W_YZ * NBOX, w1);
+                    }
+                    if (swt > 0) {
+                        atomicAdd(a + A_RO * NBOX, mro * swt); atomicAdd(a + A_CP * NBOX, mcp * mro * swt);
+                        atomicAdd(a + A_KT * NBOX, mkt * swt); atomicAdd(a + A_HT * NBOX, mht * swt);
+                        atomicAdd(a + A_ET * NBOX, mbb * swt); atomicAdd(a + A_TK * NBOX, mtk * swt);
+                        atomicAdd(a + A_RR * NBOX, mrr * swt); atomicAdd(a + W_P * NBOX, swt);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // flush: nodes inside the tile box face belong to this tile only
+    for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
+        const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
+        const int gxn = cx0 + lx, gyn = cy0 + ly, gzn = cz0 + lz;
+        if (gxn >= G.nx || gyn >= G.ny || gzn >= G.nz) continue;
+        const long node = (long)gzn * F.NXY + (long)gxn * F.NY + gyn;
+        const bool shared_node = lx == 0 || lx == TX || ly == 0 || ly == TY || lz == 0 || lz == TZ;
+        for (int a = 0; a < NACC; a++) {
+            const double v = sacc[a * NBOX + q];
+            if (v == 0.0) continue;
+            if (shared_node) atomicAdd(acc + a * N + node, v);
+            else acc[a * N + node] = v;
+        }
+    }
+}
+
+struct NodeOut {
+    float *nu, *nxx, *nxy, *nxz, *nyz, *ro, *cp, *kt, *ht, *et, *tk, *rr, *tk1;
+};
+
+// normalisation (mark3mg.c:938-1002)
+__global__ void k_r2n_norm(const double *acc, long N, NodeOut O, int vm, double nubeg, double nuend)
+{
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+#define ACC(a) acc[(long)(a) * N + n]
+#define FIN(field, A, W) if (ACC(W) > 0.01) { double v_ = ACC(A) / ACC(W); if (vm == 1) v_ = exp(v_); if (vm == 2) v_ = 1.0 / v_; O.field[n] = (float)v_; }
+    FIN(nu, A_NU, W_NU);
+    FIN(nxx, A_XX, W_XX);
+    FIN(nxy, A_XY, W_XY);
+    FIN(nxz, A_XZ, W_XZ);
+    FIN(nyz, A_YZ, W_YZ);
+    if (ACC(W_P) > 0.01) {
+        const double w = ACC(W_P);
+        const float ro = (float)(ACC(A_RO) / w);
+        O.ro[n] = ro;
+        O.cp[n] = (float)(ACC(A_CP) / w / ro);
+        O.kt[n] = (float)(ACC(A_KT) / w);
+        O.ht[n] = (float)(ACC(A_HT) / w);
+        O.et[n] = (float)(ACC(A_ET) / w);
+        O.tk[n] = (float)(ACC(A_TK) / w);
+        O.rr[n] = (float)(ACC(A_RR) / w);
+    }
+#undef FIN
+#undef ACC
+    float nu = O.nu[n];
+    if (nu < nubeg) nu = (float)nubeg;
+    if (nu > nuend) nu = (float)nuend;
+    O.nu[n] = nu;
+    O.tk1[n] = O.tk[n];
+}
+
+// tkrecalc (heat3mg.c:849-899): T = c + k * T_before(partner)
+__global__ void k_tk_bc(float *tk, const float *tk1, int n, const int *node, const int *p, const double *c, const double *k)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    // the reference's bondv1 and tk arrays are FP32: tk = c; tk += k * tk1 in FP32
+    float v = (float)c[t];
+    if (p[t] >= 0) v = __fadd_rn(v, __fmul_rn((float)k[t], tk1[p[t]]));
+    tk[node[t]] = v;
+}
+
+__global__ void k_iota(int *id, long n)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) id[i] = (int)i;
+}
+
+// scatter the sorted markers back to their original positions for a download
+__global__ void k_unsort(Marks A, Marks B, long n)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long d = A.id[i];
+    B.x[d] = A.x[i]; B.y[d] = A.y[i]; B.z[d] = A.z[i]; B.k[d] = A.k[i]; B.w[d] = A.w[i]; B.d[d] = A.d[i];
+    B.v[d] = A.v[i]; B.e[d] = A.e[i]; B.ex[d] = A.ex[i]; B.ft[d] = A.ft[i]; B.rr[d] = A.rr[i]; B.rn[d] = A.rn[i];
+    B.t[d] = A.t[i];
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+static inline unsigned nb(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+#define LAUNCH(kern, grid, block, smem, ...)                                               \
+    do {                                                                                   \
+        kern<<<(grid), (block), (smem), c->st>>>(__VA_ARGS__);                             \
+        c->launches++;                                                                     \
+    } while (0)
+
+static int alloc_marks(i3g_ctx *c, Marks &M, long n)
+{
+    float **f[12] = {&M.x, &M.y, &M.z, &M.k, &M.w, &M.d, &M.v, &M.e, &M.ex, &M.ft, &M.rr, &M.rn};
+    for (auto p : f) I3G_CUDA(cudaMalloc((void **)p, sizeof(float) * (n > 0 ? n : 1)));
+    I3G_CUDA(cudaMalloc((void **)&M.t, n > 0 ? n : 1));
+    I3G_CUDA(cudaMalloc((void **)&M.id, sizeof(int) * (n > 0 ? n : 1)));
+    return 0;
+}
+
+static void free_marks(Marks &M)
+{
+    float *f[12] = {M.x, M.y, M.z, M.k, M.w, M.d, M.v, M.e, M.ex, M.ft, M.rr, M.rn};
+    for (auto p : f) cudaFree(p);
+    cudaFree(M.t);
+    cudaFree(M.id);
+}
+
+static Grid grid_of(i3g_ctx *c)
+{
+    Grid G;
+    G.nx = (int)c->m.xnumx; G.ny = (int)c->m.ynumy; G.nz = (int)c->m.znumz;
+    G.xsize = c->m.xsize; G.ysize = c->m.ysize; G.zsize = c->m.zsize;
+    G.gx = c->gx0; G.gy = c->gy0; G.gz = c->gz0;
+    return G;
+}
+
+static NodeF nodes_of(i3g_ctx *c)
+{
+    NodeF F;
+    F.vx = c->vx; F.vy = c->vy; F.vz = c->vz;
+    for (int a = 0; a < 6; a++) { F.e[a] = c->eps[a]; F.s[a] = c->sig[a]; }
+    F.pr = c->pr;
+    F.NY = c->m.ynumy;
+    F.NXY = c->m.xnumx * c->m.ynumy;
+    return F;
+}
+
+static Phys phys_of(i3g_ctx *c)
+{
+    MarkerState *S = ms(c);
+    Phys P;
+    P.rock = S->rock; P.rocknum = c->m.rocknum; P.densimod = c->p.densimod; P.viscmod = c->p.viscmod;
+    P.outgrid = c->p.outgrid; P.markmod = c->p.markmod;
+    P.nubeg = c->p.nubeg; P.nuend = c->p.nuend; P.nukoef = c->p.nukoef; P.healrate = c->p.healrate;
+    P.timesum = c->m.timesum;
+    P.zdeep = c->p.zdeep; P.vdeep = c->p.vdeep; P.tdeep = c->p.tdeep; P.nudeep = c->p.nudeep;
+    P.teclmin = c->p.teclmin; P.teclmax = c->p.teclmax;
+    P.eroslev = c->p.eroslev; P.sedilev = c->p.sedilev; P.waterlev = c->p.waterlev;
+    P.err = S->err;
+    return P;
+}
+
+static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
+
+int markers_alloc(i3g_ctx *c)
+{
+    MarkerState *S = new MarkerState();
+    c->mk = S;
+    const long n = c->marknum, N = c->nodenum;
+    S->n = n;
+    int rc;
+    if ((rc = alloc_marks(c, S->a, n)) || (rc = alloc_marks(c, S->b, n))) return rc;
+    S->ntx = (int)((c->m.xnumx - 1 + TX - 1) / TX);
+    S->nty = (int)((c->m.ynumy - 1 + TY - 1) / TY);
+    S->ntz = (int)((c->m.znumz - 1 + TZ - 1) / TZ);
+    S->ntiles = S->ntx * S->nty * S->ntz;
+    I3G_CUDA(cudaMalloc((void **)&S->key, sizeof(int) * (n > 0 ? n : 1)));
+    I3G_CUDA(cudaMalloc((void **)&S->cnt, sizeof(int) * (S->ntiles + 2)));
+    I3G_CUDA(cudaMalloc((void **)&S->off, sizeof(int) * (S->ntiles + 2)));
+    I3G_CUDA(cudaMalloc((void **)&S->cur, sizeof(int) * (S->ntiles + 2)));
+    I3G_CUDA(cudaMalloc((void **)&S->acc, sizeof(double) * NACC * N));
+    I3G_CUDA(cudaMalloc((void **)&S->tk1, sizeof(float) * N));
+    const int rn = c->m.rocknum;
+    std::vector<double> rk(24 * (size_t)std::max(rn, 1), 0.0);
+    for (int f = 0; f < 24; f++)
+        for (int t = 0; t < rn; t++) rk[(size_t)f * rn + t] = c->m.rock[f] ? c->m.rock[f][t] : 0.0;
+    I3G_CUDA(cudaMalloc((void **)&S->rock, sizeof(double) * rk.size()));
+    I3G_CUDA(cudaMemcpyAsync(S->rock, rk.data(), sizeof(double) * rk.size(), cudaMemcpyHostToDevice, c->st));
+    I3G_CUDA(cudaMalloc((void **)&S->err, sizeof(int)));
+    I3G_CUDA(cudaMallocHost((void **)&S->herr, sizeof(int)));
+    // temperature boundary rows of level 0 (bondm[8*nodenum + node], heat3mg.c:859-889)
+    std::vector<int> tn, tp;
+    std::vector<double> tc, tkk;
+    for (long b = 0; b < c->m.bondnum; b++) {
+        const long row = c->m.bond_row[b];
+        if (row < 8 * N || row >= 9 * N) continue;
+        tn.push_back((int)(row - 8 * N));
+        tp.push_back(c->m.bond_partner1[b] > 0 ? (int)(c->m.bond_partner1[b] - 1) : -1);
+        if (tp.back() >= N) return set_error(c, I3G_E_BC, "temperature boundary partner beyond level 0");
+        tc.push_back(c->m.bond_c[b]);
+        tkk.push_back(c->m.bond_k[b]);
+    }
+    S->tbc_n = (int)tn.size();
+    I3G_CUDA(cudaMalloc((void **)&S->tbc_node, sizeof(int) * (tn.size() + 1)));
+    I3G_CUDA(cudaMalloc((void **)&S->tbc_p, sizeof(int) * (tn.size() + 1)));
+    I3G_CUDA(cudaMalloc((void **)&S->tbc_c, sizeof(double) * (tn.size() + 1)));
+    I3G_CUDA(cudaMalloc((void **)&S->tbc_k, sizeof(double) * (tn.size() + 1)));
+    if (!tn.empty()) {
+        I3G_CUDA(cudaMemcpyAsync(S->tbc_node, tn.data(), sizeof(int) * tn.size(), cudaMemcpyHostToDevice, c->st));
+        I3G_CUDA(cudaMemcpyAsync(S->tbc_p, tp.data(), sizeof(int) * tp.size(), cudaMemcpyHostToDevice, c->st));
+        I3G_CUDA(cudaMemcpyAsync(S->tbc_c, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice, c->st));
+        I3G_CUDA(cudaMemcpyAsync(S->tbc_k, tkk.data(), sizeof(double) * tkk.size(), cudaMemcpyHostToDevice, c->st));
+    }
+    I3G_CUDA(cudaFuncSetAttribute(k_r2n_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * NACC * NBOX + grid_smem(c))));
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    // upload the host markers
+    return markers_upload(c, &c->m);
+}
+
+void markers_free(i3g_ctx *c)
+{
+    MarkerState *S = ms(c);
+    if (!S) return;
+    free_marks(S->a);
+    free_marks(S->b);
+    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->acc); cudaFree(S->tk1);
+    cudaFree(S->rock); cudaFree(S->err);
+    if (S->herr) cudaFreeHost(S->herr);
+    cudaFree(S->tbc_node); cudaFree(S->tbc_p); cudaFree(S->tbc_c); cudaFree(S->tbc_k);
+    delete S;
+    c->mk = nullptr;
+}
+
+int markers_upload(i3g_ctx *c, const i3g_model *m)
+{
+    MarkerState *S = ms(c);
+    if (!S) return 0;
+    const long n = S->n;
+    if (m->marknum != n) return set_error(c, I3G_E_ARG, "marker count changed (%lld != %ld)", (long long)m->marknum, n);
+    Marks &A = S->a;
+    const float *src[12] = {m->markx, m->marky, m->markz, m->markk, m->markw, m->markd, m->markv, m->marke,
+                            m->markex, m->markft, m->markrr, m->markrn};
+    float *dst[12] = {A.x, A.y, A.z, A.k, A.w, A.d, A.v, A.e, A.ex, A.ft, A.rr, A.rn};
+    for (int f = 0; f < 12; f++) {
+        if (src[f]) I3G_CUDA(cudaMemcpyAsync(dst[f], src[f], sizeof(float) * n, cudaMemcpyHostToDevice, c->st));
+        else I3G_CUDA(cudaMemsetAsync(dst[f], 0, sizeof(float) * n, c->st));
+    }
+    if (n) I3G_CUDA(cudaMemcpyAsync(A.t, m->markt, n, cudaMemcpyHostToDevice, c->st));
+    if (n) LAUNCH(k_iota, nb(n), 256, 0, A.id, n);
+    S->sorted = false;
+    return 0;
+}
+
+int markers_download(i3g_ctx *c, i3g_model *m)
+{
+    MarkerState *S = ms(c);
+    if (!S || !S->n) return 0;
+    const long n = S->n;
+    LAUNCH(k_unsort, nb(n), 256, 0, S->a, S->b, n);
+    Marks &B = S->b;
+    float *dst[12] = {m->markx, m->marky, m->markz, m->markk, m->markw, m->markd, m->markv, m->marke,
+                      m->markex, m->markft, m->markrr, m->markrn};
+    const float *src[12] = {B.x, B.y, B.z, B.k, B.w, B.d, B.v, B.e, B.ex, B.ft, B.rr, B.rn};
+    for (int f = 0; f < 12; f++)
+        if (dst[f]) I3G_CUDA(cudaMemcpyAsync(dst[f], src[f], sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
+    if (m->markt) I3G_CUDA(cudaMemcpyAsync(m->markt, B.t, n, cudaMemcpyDeviceToHost, c->st));
+    return 0;
+}
+
+static int check_err(i3g_ctx *c, const char *what)
+{
+    MarkerState *S = ms(c);
+    I3G_CUDA(cudaMemcpyAsync(S->herr, S->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    const int e = *S->herr;
+    if (!e) return 0;
+    if (e & ERR_TYPE) return set_error(c, I3G_E_UNSUPPORTED, "%s: fluid or immobile marker types (>= 50) are not supported", what);
+    if (e & ERR_GRAIN) return set_error(c, I3G_E_UNSUPPORTED, "%s: grain-damage rheology (markdh < 0) is not supported", what);
+    if (e & ERR_WATER) return set_error(c, I3G_E_UNSUPPORTED, "%s: air/water marker types 0-1 are not supported", what);
+    if (e & ERR_MELT) return set_error(c, I3G_E_UNSUPPORTED, "%s: molten rock types > 20 are not supported", what);
+    return set_error(c, I3G_E_UNSUPPORTED, "%s: densimod >= 2 (thermodynamic database) is not supported", what);
+}
+
+int markers_move(i3g_ctx *c, double timestep)
+{
+    MarkerState *S = ms(c);
+    if (!S->n || timestep == 0) return 0;
+    cudaEvent_t e0, e1;
+    I3G_CUDA(cudaEventCreate(&e0));
+    I3G_CUDA(cudaEventCreate(&e1));
+    I3G_CUDA(cudaEventRecord(e0, c->st));
+    I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
+    LAUNCH(k_move, nb(S->n), 256, grid_smem(c), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c), timestep);
+    I3G_CUDA(cudaGetLastError());
+    I3G_CUDA(cudaEventRecord(e1, c->st));
+    int rc = check_err(c, "movemark");
+    float ms_ = 0;
+    cudaEventElapsedTime(&ms_, e0, e1);
+    c->st_.ms_move = ms_;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S->sorted = false;
+    return rc;
+}
+
+static int sort_markers(i3g_ctx *c)
+{
+    MarkerState *S = ms(c);
+    const long n = S->n;
+    TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
+    I3G_CUDA(cudaMemsetAsync(S->cnt, 0, sizeof(int) * (S->ntiles + 1), c->st));
+    LAUNCH(k_tile_key, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), T, S->key, S->cnt);
+    LAUNCH(k_scan, 1, 1024, 0, (const int *)S->cnt, S->off, S->cur, S->ntiles + 1);
+    LAUNCH(k_tile_scatter, nb(n), 256, 0, S->a, S->b, n, (const int *)S->key, S->cur);
+    std::swap(S->a, S->b);
+    S->sorted = true;
+    return 0;
+}
+
+int markers_to_nodes(i3g_ctx *c, double timestep)
+{
+    MarkerState *S = ms(c);
+    const long N = c->nodenum;
+    cudaEvent_t e0, e1;
+    I3G_CUDA(cudaEventCreate(&e0));
+    I3G_CUDA(cudaEventCreate(&e1));
+    I3G_CUDA(cudaEventRecord(e0, c->st));
+    I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
+    int rc = 0;
+    if (S->n) rc = sort_markers(c);
+    if (rc) return rc;
+    I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
+    TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
+    if (S->n)
+        LAUNCH(k_r2n_tile, S->ntiles, 512, sizeof(double) * NACC * NBOX + grid_smem(c), S->a, (const int *)S->off, grid_of(c),
+               nodes_of(c), phys_of(c), T, timestep, S->acc, N);
+    NodeOut O{c->lev[0].nu, c->nxx, c->nxy, c->nxz, c->nyz, c->ro, c->cp, c->kt, c->ht, c->et, c->tk, c->rr, S->tk1};
+    LAUNCH(k_r2n_norm, nb(N), 256, 0, (const double *)S->acc, N, O, c->p.viscmod, c->p.nubeg, c->p.nuend);
+    if (S->tbc_n)
+        LAUNCH(k_tk_bc, nb(S->tbc_n), 256, 0, c->tk, (const float *)S->tk1, S->tbc_n, (const int *)S->tbc_node,
+               (const int *)S->tbc_p, (const double *)S->tbc_c, (const double *)S->tbc_k);
+    I3G_CUDA(cudaGetLastError());
+    I3G_CUDA(cudaEventRecord(e1, c->st));
+    rc = check_err(c, "ronurecalc");
+    float ms_ = 0;
+    cudaEventElapsedTime(&ms_, e0, e1);
+    c->st_.ms_r2n = ms_;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->stokes_ready = false;
+    return rc;
+}
+
+int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *bytes)
+{
+    MarkerState *S = ms(c);
+    const long n = S->n, N = c->nodenum;
+    cudaEvent_t e0, e1;
+    I3G_CUDA(cudaEventCreate(&e0));
+    I3G_CUDA(cudaEventCreate(&e1));
+    TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
+    if (!S->sorted) { int rc = sort_markers(c); if (rc) return rc; }
+    I3G_CUDA(cudaEventRecord(e0, c->st));
+    for (int r = 0; r < reps; r++) {
+        if (kind == 4) {
+            I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
+            LAUNCH(k_r2n_tile, S->ntiles, 512, sizeof(double) * NACC * NBOX + grid_smem(c), S->a, (const int *)S->off,
+                   grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->acc, N);
+        } else {
+            LAUNCH(k_move, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), nodes_of(c), phys_of(c), 0.0);
+        }
+    }
+    I3G_CUDA(cudaEventRecord(e1, c->st));
+    I3G_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms_out = t / reps;
+    // compulsory bytes: marker fields read/written once, node fields read/written once
+    if (kind == 4) *bytes = (double)n * (4.0 * 6 + 1 + 4) + (double)N * (8.0 + NACC * 8.0);
+    else *bytes = (double)n * (4.0 * 9 + 1 + 4.0 * 9) + (double)N * (4.0 * 15 + 8.0);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
 }  // namespace i3g

@@ -174,3 +174,32 @@ def read_sol(path):
         h = int(np.frombuffer(fh.read(8), np.int64)[0])
         hist = np.frombuffer(fh.read(8 * h), np.float64).copy()
     return sol, hist
+
+
+FIELD_NAMES = ("vx", "vy", "vz", "exx", "eyy", "ezz", "exy", "exz", "eyz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+MARK_NAMES = ("x", "y", "z", "k", "w", "d", "v", "e", "ex", "ft", "rr", "rn")
+NODE_NAMES = ("ro", "nu", "nxx", "nxy", "nxz", "nyz", "tk", "cp", "et", "kt", "ht", "rr", "vx", "vy", "vz")
+
+
+def read_fields(path):
+    with open(path, "rb") as fh:
+        n = int(np.frombuffer(fh.read(8), np.int64)[0])
+        out = {"pr": np.frombuffer(fh.read(8 * n), np.float64).copy()}
+        for f in FIELD_NAMES:
+            out[f] = np.frombuffer(fh.read(4 * n), np.float32).copy()
+        out["timestep"] = float(np.frombuffer(fh.read(8), np.float64)[0])
+    return out
+
+
+def read_marks(path):
+    with open(path, "rb") as fh:
+        n = int(np.frombuffer(fh.read(8), np.int64)[0])
+        out = {f: np.frombuffer(fh.read(4 * n), np.float32).copy() for f in MARK_NAMES}
+        out["t"] = np.frombuffer(fh.read(n), np.int8).copy()
+    return out
+
+
+def read_nodes(path):
+    with open(path, "rb") as fh:
+        n = int(np.frombuffer(fh.read(8), np.int64)[0])
+        return {f: np.frombuffer(fh.read(4 * n), np.float32).copy() for f in NODE_NAMES}

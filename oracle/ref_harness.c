@@ -16,6 +16,7 @@
  *   stokes PREFIX              vpiterate(0,0) as is; writes PREFIX.fields (v, P, stresses)
  *   move DT PREFIX             loads PREFIX.fields, movemark(); writes PREFIX.marks
  *   r2n PREFIX                 ronurecalc() on the loaded markers; writes PREFIX.nodes
+ *   mover2n DT PREFIX          loads PREFIX.fields, movemark(), ronurecalc(); marks + nodes
  *   step OUT.prn               one full i3mg time step (i3mg.c:80-147), wall time per phase
  */
 #include <stdio.h>
@@ -351,6 +352,15 @@ int main(int argc, char **argv)
         timestep = atof(argv[2]);
         movemark();
         dump_marks(argv[3]);
+        return 0;
+    }
+    if (!strcmp(cmd, "mover2n") && argc == 4) {
+        load_fields(argv[3]);
+        timestep = atof(argv[2]);
+        movemark();
+        dump_marks(argv[3]);
+        ronurecalc();
+        dump_nodes(argv[3]);
         return 0;
     }
     if (!strcmp(cmd, "r2n") && argc == 3) {

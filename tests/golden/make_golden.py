@@ -26,6 +26,9 @@ import oracle as O  # noqa: E402
 from i3elvis_b200 import config, prn as P  # noqa: E402
 
 
+MARKER_CASES = ("sphere13",)
+
+
 def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
@@ -46,6 +49,18 @@ def make(name):
         vsol, vhist = O.read_sol(os.path.join(d, "v.sol"))
         info = O.run_reference(d, "solve", 1e-12, 3000, "s")
         ssol, shist = O.read_sol(os.path.join(d, "s.sol"))
+        extra = {}
+        if name in MARKER_CASES:
+            # reference vpiterate at its own (absolute) tolerance, then movemark + ronurecalc
+            O.run_reference(d, "stokes", "m")
+            flds = O.read_fields(os.path.join(d, "m.fields"))
+            O.run_reference(d, "mover2n", repr(flds["timestep"]), "m")
+            mk = O.read_marks(os.path.join(d, "m.marks"))
+            nd = O.read_nodes(os.path.join(d, "m.nodes"))
+            extra = dict(fld_pr=flds["pr"], fld=np.stack([flds[f] for f in O.FIELD_NAMES]),
+                         fld_dt=np.array([flds["timestep"]]),
+                         mk=np.stack([mk[f] for f in O.MARK_NAMES]), mk_t=mk["t"],
+                         r2n=np.stack([nd[f] for f in O.NODE_NAMES]))
     sizes = cases.level_sizes(p0, mode.multinum)
     offs = np.concatenate([[0], np.cumsum(sizes)]) * 4
     digests = {}
@@ -56,7 +71,7 @@ def make(name):
                                 cols=sha(csr["col"][a:b].astype(np.int64)), vals=sha(csr["val"][a:b]))
     digests["rhs0"] = sha(csr["rhs"][:offs[1]])
     out = dict(nodes=np.stack([prep.nodes[f] for f in P.NODE_FIELDS]), markv=prep.marks["v"],
-               vcyc_sol=vsol, vcyc_hist=vhist, solve_sol=ssol, solve_hist=shist)
+               vcyc_sol=vsol, vcyc_hist=vhist, solve_sol=ssol, solve_hist=shist, **extra)
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
     with open(os.path.join(HERE, f"{name}.json"), "w") as fh:
         json.dump(dict(case=cases.CASES[name], csr_sha256=digests, solve=info), fh, indent=1)

@@ -1,0 +1,46 @@
+"""The CPU oracle's marker operations against the reference (movemark + ronurecalc)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden
+from i3elvis_b200 import abi
+
+
+def marker_setup(name="sphere13"):
+    """Buffers holding the reference's post-Stokes fields (v, P, strain rates, stresses)."""
+    p, mode, fx = golden(name)
+    if "fld" not in fx:
+        pytest.skip("no marker fixture for this case")
+    buf = abi.ModelBuffers(p)
+    buf.pr[:] = fx["fld_pr"]
+    for i, f in enumerate(O.FIELD_NAMES):
+        buf.f32[f][:] = fx["fld"][i]
+    return p, mode, fx, buf
+
+
+def test_oracle_move_markers_matches_reference():
+    p, mode, fx, buf = marker_setup()
+    dt = float(fx["fld_dt"][0])
+    o = O.Oracle(buf, abi.make_params(mode), abi.make_file_params(mode.files[0]))
+    o.call("orc_move_markers", dt)
+    o.download(abi.SYNC_MARKERS)
+    ref = dict(zip(O.MARK_NAMES, fx["mk"]))
+    for f, bf in (("x", "markx"), ("y", "marky"), ("z", "markz")):
+        np.testing.assert_array_equal(buf.f32[bf], ref[f], err_msg=f)
+    np.testing.assert_allclose(buf.f32["markv"], ref["v"], rtol=2e-7)
+    np.testing.assert_array_equal(buf.f32["marke"], ref["e"])
+    np.testing.assert_array_equal(buf.markt, fx["mk_t"])
+
+
+def test_oracle_markers_to_nodes_matches_reference():
+    p, mode, fx, buf = marker_setup()
+    dt = float(fx["fld_dt"][0])
+    o = O.Oracle(buf, abi.make_params(mode), abi.make_file_params(mode.files[0]))
+    o.call("orc_move_markers", dt)
+    o.call("orc_markers_to_nodes", dt)
+    o.download(abi.SYNC_NODES)
+    ref = dict(zip(O.NODE_NAMES, fx["r2n"]))
+    # the reference sums most node fields in FP32 (in marker order); the oracle in FP64
+    for f in ("ro", "nu", "nxx", "nxy", "nxz", "nyz", "tk", "cp", "kt", "et", "ht", "rr"):
+        np.testing.assert_allclose(buf.f32[f], ref[f], rtol=2e-6, atol=0, err_msg=f)
