@@ -16,4 +16,6 @@ int markers_download(i3g_ctx *c, i3g_model *m);
 int markers_move(i3g_ctx *c, double timestep);
 int markers_to_nodes(i3g_ctx *c, double timestep);
 int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes);
+// marker temperature update after the heat solve (heat3mg.c:592-782)
+int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const float *tk1, const float *tk2);
 }  // namespace i3g

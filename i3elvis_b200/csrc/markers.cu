@@ -435,9 +435,12 @@ __global__ void __launch_bounds__(256) k_move(Marks M, long n, Grid Gg, NodeF F,
 // ------------------------------------------------------------------------------------
 struct TileGeo { int ntx, nty, ntz, ntiles; };
 
+// markers grouped into tiles: rock markers strictly inside the box (the set both ronurecalc,
+// mark3mg.c:459, and the marker temperature update, heat3mg.c:623, visit)
 __device__ __forceinline__ bool r2n_active(const Grid &G, float x, float y, float z, int t, float k)
 {
-    return x > 0 && y > 0 && z > 0 && x < G.xsize && y < G.ysize && z < G.zsize && t < 50 && k > 0;
+    (void)k;
+    return x > 0 && y > 0 && z > 0 && x < G.xsize && y < G.ysize && z < G.zsize && t < 50;
 }
 
 __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *cnt)
@@ -553,6 +556,7 @@ __global__ void __launch_bounds__(512) k_r2n_tile(Marks M, const int *off, Grid 
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
         int mm2 = M.t[i];
         const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+        if (!(M.k[i] > 0)) continue;
         if (mm2 > 1 && fy < P.eroslev) { mm2 = 0; M.t[i] = 0; }
         if (mm2 < 2) { atomicOr(P.err, ERR_WATER); continue; }
         if (mm2 > 20) { atomicOr(P.err, ERR_MELT); continue; }
@@ -636,6 +640,122 @@ __global__ void __launch_bounds__(512) k_r2n_tile(Marks M, const int *off, Grid 
             else acc[a * N + node] = v;
         }
     }
+}
+
+// ------------------------------------------------------------------------------------
+// marker temperatures after the heat solve (heat3mg.c:592-782)
+// ------------------------------------------------------------------------------------
+struct TkF { const float *tk0, *tk1, *tk, *tk2, *kt, *ro, *cp; long NY, NXY; };
+
+// tkcalc1 (mark3mg.c:2844-2910): cell, spacings, 8 weights and the 4 interpolated T arrays
+__device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, double y, double z, double *e, int *wn,
+                                      long *nodes, double *wi)
+{
+    const int m10 = wn[0] = bsearch_g(G.gx, G.nx, x), m20 = wn[1] = bsearch_g(G.gy, G.ny, y), m30 = wn[2] = bsearch_g(G.gz, G.nz, z);
+    const double dx = wi[8] = G.gx[m10 + 1] - G.gx[m10];
+    const double dy = wi[9] = G.gy[m20 + 1] - G.gy[m20];
+    const double dz = wi[10] = G.gz[m30 + 1] - G.gz[m30];
+    e[0] = e[1] = e[2] = e[3] = 0;
+    int q = 0;
+    for (int m3 = m30; m3 <= m30 + 1; m3++) {
+        double ddz = (G.gz[m3] - z) / dz; ddz = 1.0 - fabs(ddz);
+        for (int m1 = m10; m1 <= m10 + 1; m1++) {
+            double ddx = (G.gx[m1] - x) / dx; ddx = 1.0 - fabs(ddx);
+            for (int m2 = m20; m2 <= m20 + 1; m2++) {
+                double ddy = (G.gy[m2] - y) / dy; ddy = 1.0 - fabs(ddy);
+                const double swt = wi[q] = ddx * ddy * ddz;
+                const long m4 = nodes[q] = m3 * T.NXY + (long)m1 * T.NY + m2;
+                e[0] += swt * T.tk0[m4]; e[1] += swt * T.tk1[m4]; e[2] += swt * T.tk[m4]; e[3] += swt * T.tk2[m4];
+                q++;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(512) k_heat_mark_tile(Marks M, const int *off, Grid Gg, TkF T, TileGeo TG, double timestep,
+                                                        double heatdif, double zdeep, double tdeep, double *acc, long N)
+{
+    extern __shared__ double sm[];
+    double *sw0 = sm, *sw1 = sm + NBOX, *shg = sm + 2 * NBOX;
+    for (int q = threadIdx.x; q < 2 * NBOX; q += blockDim.x) sm[q] = 0;
+    Grid G;
+    load_grid(Gg, shg, G);
+    const int tile = blockIdx.x;
+    const int ty = tile % TG.nty, rest = tile / TG.nty, tx = rest % TG.ntx, tz = rest / TG.ntx;
+    const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
+    for (int i = off[tile] + threadIdx.x; i < off[tile + 1]; i += blockDim.x) {
+        const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+        double e[4], wi[11];
+        int wn[3];
+        long nodes[8];
+        tk_at(G, T, fx, fy, fz, e, wn, nodes, wi);
+        float mk = M.k[i];
+        if (mk <= 0) {
+            mk = (float)e[3];
+            if (fy > zdeep && mk < tdeep) mk = (float)tdeep;
+        }
+        if (heatdif != 0) {
+            double mkt = 0, rocp = 0, mtk = T.tk[nodes[0]];
+            for (int q = 0; q < 8; q++) {
+                mkt += T.kt[nodes[q]] * wi[q];
+                rocp += (double)__fmul_rn(T.ro[nodes[q]], T.cp[nodes[q]]) * wi[q];
+                mtk = fmax(mtk, (double)T.tk[nodes[q]]);
+            }
+            if ((wn[0] <= 0 || wn[0] >= G.nx - 2 || wn[1] <= 0 || wn[1] >= G.ny - 2 || wn[2] <= 0 || wn[2] >= G.nz - 2) &&
+                (mk + e[2] - e[3]) > mtk)
+                mk = (float)(mtk - e[2] + e[3]);
+            const double dtk = e[3] - (double)mk;
+            double dtk1 = -heatdif * mkt / rocp * 2.0 * (1.0 / wi[8] / wi[8] + 1.0 / wi[9] / wi[9] + 1.0 / wi[10] / wi[10]) * timestep;
+            if (dtk1 < -150.0) dtk1 = -150.0;
+            dtk1 = dtk * (1.0 - exp(dtk1));
+            mk = __fadd_rn(mk, (float)dtk1);
+            int q = 0;
+            for (int m3 = wn[2]; m3 <= wn[2] + 1; m3++)
+                for (int m1 = wn[0]; m1 <= wn[0] + 1; m1++)
+                    for (int m2 = wn[1]; m2 <= wn[1] + 1; m2++, q++) {
+                        const int lb = ((m3 - cz0) * NBX + (m1 - cx0)) * NBY + (m2 - cy0);
+                        atomicAdd(sw1 + lb, dtk1 * wi[q]);
+                        atomicAdd(sw0 + lb, wi[q]);
+                    }
+        }
+        mk = __fadd_rn(mk, (float)(e[2] - e[3]));
+        M.k[i] = mk;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
+        const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
+        const int gxn = cx0 + lx, gyn = cy0 + ly, gzn = cz0 + lz;
+        if (gxn >= G.nx || gyn >= G.ny || gzn >= G.nz) continue;
+        const long node = (long)gzn * T.NXY + (long)gxn * T.NY + gyn;
+        const bool shared_node = lx == 0 || lx == TX || ly == 0 || ly == TY || lz == 0 || lz == TZ;
+        const double a0 = sw0[q], a1 = sw1[q];
+        if (a0 == 0.0 && a1 == 0.0) continue;
+        if (shared_node) { atomicAdd(acc + node, a0); atomicAdd(acc + N + node, a1); }
+        else { acc[node] = a0; acc[N + node] = a1; }
+    }
+}
+
+__global__ void k_heat_mark_norm(double *acc, long N)
+{
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < N && acc[n] != 0.0) acc[N + n] /= acc[n];
+}
+
+// antidiffusion: marker T -= interpolated mean node change (heat3mg.c:722-779)
+__global__ void k_heat_mark_anti(Marks M, const int *off, int ntiles, Grid Gg, TkF T, const double *acc, long N)
+{
+    extern __shared__ double shg[];
+    Grid G;
+    load_grid(Gg, shg, G);
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= off[ntiles]) return;
+    double e[4], wi[11];
+    int wn[3];
+    long nodes[8];
+    tk_at(G, T, M.x[i], M.y[i], M.z[i], e, wn, nodes, wi);
+    double iv = 0;
+    for (int q = 0; q < 8; q++) iv -= acc[N + nodes[q]] * wi[q];
+    M.k[i] = __fadd_rn(M.k[i], (float)iv);
 }
 
 struct NodeOut {
@@ -955,6 +1075,29 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
     cudaEventDestroy(e1);
     c->stokes_ready = false;
     return rc;
+}
+
+int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const float *tk1, const float *tk2)
+{
+    MarkerState *S = ms(c);
+    if (!S->n) return 0;
+    const long N = c->nodenum;
+    if (!S->sorted) {
+        int rc = sort_markers(c);
+        if (rc) return rc;
+    }
+    I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * 2 * N, c->st));
+    TkF T{tk0, tk1, c->tk, tk2, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
+    TileGeo TG{S->ntx, S->nty, S->ntz, S->ntiles};
+    LAUNCH(k_heat_mark_tile, S->ntiles, 512, sizeof(double) * 2 * NBOX + grid_smem(c), S->a, (const int *)S->off, grid_of(c),
+           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->acc, N);
+    if (c->p.heatdif != 0) {
+        LAUNCH(k_heat_mark_norm, nb(N), 256, 0, S->acc, N);
+        LAUNCH(k_heat_mark_anti, nb(S->n), 256, grid_smem(c), S->a, (const int *)S->off, S->ntiles, grid_of(c), T,
+               (const double *)S->acc, N);
+    }
+    I3G_CUDA(cudaGetLastError());
+    return 0;
 }
 
 int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *bytes)

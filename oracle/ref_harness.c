@@ -17,6 +17,7 @@
  *   move DT PREFIX             loads PREFIX.fields, movemark(); writes PREFIX.marks
  *   r2n PREFIX                 ronurecalc() on the loaded markers; writes PREFIX.nodes
  *   mover2n DT PREFIX          loads PREFIX.fields, movemark(), ronurecalc(); marks + nodes
+ *   titerate DT PREFIX         loads PREFIX.fields, titerate(0); marks + nodes
  *   step OUT.prn               one full i3mg time step (i3mg.c:80-147), wall time per phase
  */
 #include <stdio.h>
@@ -360,6 +361,14 @@ int main(int argc, char **argv)
         movemark();
         dump_marks(argv[3]);
         ronurecalc();
+        dump_nodes(argv[3]);
+        return 0;
+    }
+    if (!strcmp(cmd, "titerate") && argc == 4) {
+        load_fields(argv[3]);
+        timestep = atof(argv[2]);
+        titerate(0);
+        dump_marks(argv[3]);
         dump_nodes(argv[3]);
         return 0;
     }

@@ -50,6 +50,7 @@ def make(name):
         info = O.run_reference(d, "solve", 1e-12, 3000, "s")
         ssol, shist = O.read_sol(os.path.join(d, "s.sol"))
         extra = {}
+        digests = {}
         if name in MARKER_CASES:
             # reference vpiterate at its own (absolute) tolerance, then movemark + ronurecalc
             O.run_reference(d, "stokes", "m")
@@ -61,9 +62,19 @@ def make(name):
                          fld_dt=np.array([flds["timestep"]]),
                          mk=np.stack([mk[f] for f in O.MARK_NAMES]), mk_t=mk["t"],
                          r2n=np.stack([nd[f] for f in O.NODE_NAMES]))
+            # the reference's own titerate (absolute HEATMIN, evaluated on FP32 temperatures)
+            O.run_reference(d, "titerate", repr(flds["timestep"]), "m", timeout=600)
+            # and its heat rows solved tightly in FP64 (relative residual 1e-13)
+            hinfo = O.run_reference(d, "heat", repr(flds["timestep"]), 1e-13, 5000, "h", timeout=600)
+            hc = O.read_csr(os.path.join(d, "h.csr"))
+            hsol, _ = O.read_sol(os.path.join(d, "h.sol"))
+            digests["heat"] = dict(counts=sha(np.diff(hc["indptr"]).astype(np.int64)), cols=sha(hc["col"].astype(np.int64)),
+                                   vals=sha(hc["val"]), rhs=sha(hc["rhs"]), info=hinfo)
+            hm = O.read_marks(os.path.join(d, "m.marks"))
+            hn = O.read_nodes(os.path.join(d, "m.nodes"))
+            extra.update(heat_tk=hn["tk"], heat_mk=hm["k"], heat_sol=hsol)
     sizes = cases.level_sizes(p0, mode.multinum)
     offs = np.concatenate([[0], np.cumsum(sizes)]) * 4
-    digests = {}
     counts = np.diff(csr["indptr"])
     for l in range(len(sizes)):
         a, b = csr["indptr"][offs[l]], csr["indptr"][offs[l + 1]]

@@ -59,3 +59,25 @@ def test_prepare_matches_reference():
         np.testing.assert_allclose(buf.f32[f], ref[f], rtol=2e-6, atol=0, err_msg=f)
     np.testing.assert_allclose(buf.pr, ref["pr"].astype(np.float64), rtol=1e-6, atol=1e-3)
     np.testing.assert_allclose(buf.f32["markv"], fx["markv"], rtol=2e-7)
+
+
+def test_heat_matches_reference_and_oracle():
+    """titerate on the GPU: converged FP64 temperature equals the reference's heat rows solved
+    to 1e-13; marker temperatures match the oracle's restatement and the reference's run."""
+    p, mode, fx, buf = marker_setup()
+    dt = float(fx["fld_dt"][0])
+    g = lib.Context(buf, abi.make_params(mode, heat_rtol=1e-13), abi.make_file_params(mode.files[0]))
+    assert g.heat(0, dt) == dt
+    T = g.get(abi.A_TK, 0, p.nodenum)
+    ref = fx["heat_sol"]
+    assert np.linalg.norm(T - ref) / np.linalg.norm(ref) < 1e-12
+    g.download(abi.SYNC_ALL)
+    p2, mode2, fx2, buf2 = marker_setup()
+    o = O.Oracle(buf2, abi.make_params(mode2, heat_rtol=1e-13), abi.make_file_params(mode2.files[0]))
+    o.call("orc_heat", (O.C.c_double * 1)(dt))
+    o.download(abi.SYNC_ALL)
+    np.testing.assert_allclose(buf.f32["tk"], buf2.f32["tk"], rtol=2e-7, atol=0)
+    np.testing.assert_allclose(buf.f32["markk"], buf2.f32["markk"], rtol=1e-6, atol=1e-4)
+    np.testing.assert_allclose(buf.f32["markk"], fx["heat_mk"], rtol=1e-5, atol=1e-3)
+    st = g.stats()
+    assert st["heat_rel"] <= 1e-13 and st["heat_substeps"] == 1

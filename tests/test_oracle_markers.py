@@ -44,3 +44,20 @@ def test_oracle_markers_to_nodes_matches_reference():
     # the reference sums most node fields in FP32 (in marker order); the oracle in FP64
     for f in ("ro", "nu", "nxx", "nxy", "nxz", "nyz", "tk", "cp", "kt", "et", "ht", "rr"):
         np.testing.assert_allclose(buf.f32[f], ref[f], rtol=2e-6, atol=0, err_msg=f)
+
+
+def test_oracle_heat_matches_reference():
+    """titerate: converged FP64 temperature equals the reference's tightly solved heat rows;
+    marker temperatures (subgrid diffusion) equal the reference's titerate to its tolerance."""
+    p, mode, fx, buf = marker_setup()
+    dt = float(fx["fld_dt"][0])
+    o = O.Oracle(buf, abi.make_params(mode, heat_rtol=1e-13), abi.make_file_params(mode.files[0]))
+    t = (O.C.c_double * 1)(dt)
+    o.call("orc_heat", t)
+    T = o.get(abi.A_TK, 0, p.nodenum)
+    ref = fx["heat_sol"]
+    assert np.linalg.norm(T - ref) / np.linalg.norm(ref) < 1e-12
+    o.download(abi.SYNC_ALL)
+    # the reference stops on HEATMIN = 1e-3 K evaluated on FP32 temperatures
+    np.testing.assert_allclose(buf.f32["tk"], fx["heat_tk"], rtol=1e-5, atol=1e-3)
+    np.testing.assert_allclose(buf.f32["markk"], fx["heat_mk"], rtol=1e-5, atol=1e-3)
