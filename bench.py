@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per marker-in-cell time step at 129^3 nodes, Stokes to relative residual
+1e-8 (plus heat solve, RK4 marker advection and marker->node averaging), on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--workload incl129|sphere33|incl65] [--impl ours|reference]
+
+One step is one reference time step (i3mg.c:80-147) on a synthetic model of the named shape:
+129^3 nodes in a 200 km cube, 27 jittered markers per cell (56.6 M markers), 100 seeded
+spherical inclusions (radius 2-8 km, density 3250-3450), Arrhenius matrix viscosity clipped to
+1e18-1e24 Pa s.  Inputs are resident in HBM when the timed region starts; the model is far
+larger than L2, so no flush is needed.  Under torchrun (N > 1) every rank advances its own
+model (replicas; the path has no cross-rank exchange), and the reported value is the
+aggregate seconds per step: max-over-ranks time / (steps * N).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from i3elvis_b200 import abi, config, model  # noqa: E402
+from i3elvis_b200.prn import write_prn  # noqa: E402
+
+METRIC = "s/time-step at 129^3, Stokes residual 1e-8"
+
+WORKLOADS = {
+    "incl129": dict(n=129, mnum=3, multinum=4, seed=7, count=100,
+                    desc="129^3 nodes, 200 km cube, 27 markers/cell (56.6M), 100 inclusions, Arrhenius 1e18-1e24"),
+    "incl65": dict(n=65, mnum=3, multinum=3, seed=7, count=100,
+                   desc="65^3 nodes, 200 km cube, 27 markers/cell, 100 inclusions, Arrhenius 1e18-1e24"),
+    "sphere33": dict(n=33, mnum=3, multinum=2, seed=1,
+                     desc="33^3 nodes, 100 km cube, 27 markers/cell, sinking sphere 1e23/1e21"),
+}
+
+
+def build_case(name, seed_offset=0):
+    w = WORKLOADS[name]
+    if name.startswith("sphere"):
+        prn, spec = model.sinking_sphere(n=w["n"], mnum=w["mnum"], multinum=w["multinum"], seed=w["seed"] + seed_offset)
+        size = 100e3
+    else:
+        prn, spec = model.random_inclusions(n=w["n"], mnum=w["mnum"], multinum=w["multinum"],
+                                            seed=w["seed"] + seed_offset, count=w["count"])
+        size = 200e3
+    mn = w["multinum"]
+    down = (8, 16, 16, 32, 32, 32)[:mn] + (0,)
+    up = (8, 16, 16, 32, 32, 32)[:mn] + (64,)
+    dx = size / (w["n"] - 1)
+    mode = config.Mode(
+        infile="in0.prn", multinum=mn, multicyc=1, multinnn=(down, up),
+        p0koef=0.71, p1koef=1.0, v0koef=0.7, v1koef=0.7, nubeg=1e18, nuend=1e24,
+        files=[config.OutFile("out1.prn", maxxystep=0.5 * dx, maxtmstep_yr=1e9, nubeg=1e18, nuend=1e24,
+                              p0koef=0.71, p1koef=1.0, multinum=mn, multinum2=mn)])
+    return prn, mode
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.file = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=self.file, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 7:
+                    try:
+                        rows.append((float(f[0]), float(f[1]), float(f[2]), f[3:7]))
+                    except ValueError:
+                        pass
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def reference_sample(prn, mode, ncyc_for_1e8, threads):
+    """Time the reference's own functions on this workload (bounded sample, all host threads):
+    vpiterate set-up + one V-cycle, titerate, movemark, ronurecalc.  The step estimate scales
+    the V-cycle by the number of V-cycles this multigrid needs for relative residual 1e-8."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.have_reference():
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        write_prn(os.path.join(d, "in0.prn"), prn)
+        config.write_mode(os.path.join(d, "mode.t3c"), mode)
+        config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
+        r = O.run_reference(d, "sample", 1, threads=threads, timeout=1200)
+    if not r:
+        return None
+    est = r["assemble_s"] + ncyc_for_1e8 * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
+    return est, r
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's CPU implementation of the step on this box's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    prn, mode = build_case(args.workload)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built (reference sources absent at build time)"}))
+        return 0
+    ncyc = args.ref_cycles
+    times = []
+    detail = None
+    with tempfile.TemporaryDirectory() as d:
+        write_prn(os.path.join(d, "in0.prn"), prn)
+        config.write_mode(os.path.join(d, "mode.t3c"), mode)
+        config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
+        # the reference's own initial-condition passes (in3mg.c:990-1031)
+        O.run_reference(d, "prepare", "prep.prn", threads=threads, timeout=1800)
+        mode.infile = "prep.prn"
+        config.write_mode(os.path.join(d, "mode.t3c"), mode)
+        for i in range(args.warmup + args.steps):
+            r = O.run_reference(d, "sample", 1, threads=threads, timeout=1800)
+            est = r["assemble_s"] + ncyc * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
+            if i >= args.warmup:
+                times.append(est)
+                detail = r
+    v = float(np.mean(times))
+    sample = (f"per step: reference vpiterate set-up + 1 V-cycle (x {ncyc} V-cycles to relative residual 1e-8), "
+              f"titerate, movemark, ronurecalc on the full {args.workload} model, {threads} OpenMP threads; "
+              f"phases {json.dumps(detail)}")
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s/step", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"]},
+                      "cpu_baseline": {"value": v, "unit": "s/step", "cores": threads, "kind": "reference", "sample": sample},
+                      "e2e": {"value": v, "unit": "s/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--precision", default="mixed", choices=("fp64", "mixed"))
+    ap.add_argument("--workload", default="incl129", choices=tuple(WORKLOADS))
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("I3G_REF_CYCLES", "40")))
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from i3elvis_b200 import lib, runtime
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    prn, mode = build_case(args.workload, seed_offset=rank)
+    prec = 1 if args.precision == "mixed" else 0
+    par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec)
+    buf = abi.ModelBuffers(prn, pinned=True)
+    ctx = lib.Context(buf, par, abi.make_file_params(mode.files[0]))
+    f = mode.files[0]
+    runtime.prepare(ctx)
+    cycles = []
+    for i in range(args.warmup):
+        runtime.time_step(ctx, mode, f, i)
+        cycles.append(ctx.stats()["stokes_cycles"])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    l0 = ctx.stats()["kernel_launches"]
+    barrier()
+    clocks.start()
+    ctx.timer_start()
+    logs = []
+    for i in range(args.steps):
+        logs.append(runtime.time_step(ctx, mode, f, args.warmup + i))
+        st = ctx.stats()
+        cycles.append(st["stokes_cycles"])
+        logs[-1].update({k: st[k] for k in ("stokes_cycles", "stokes_rel", "ms_stokes", "ms_heat", "ms_move", "ms_r2n")})
+    ms = ctx.timer_stop()
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.stats()["kernel_launches"] - l0
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = ms_max / 1e3 / (args.steps * world)
+
+    # end to end through the C ABI with host buffers: full state up, step, full state down
+    e2e_steps = max(1, min(args.steps, 2))
+    n, m = prn.nodenum, prn.marknum
+    h2d = n * (8 + 4 * 15) + m * (4 * 12 + 1)
+    d2h = h2d + n * 4 * 12
+    ctx.download(abi.SYNC_ALL)   # host buffers hold the current state, so each upload resumes it
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        ctx.upload(abi.SYNC_NODES | abi.SYNC_MARKERS)
+        runtime.time_step(ctx, mode, f, 100 + i)
+        ctx.download(abi.SYNC_ALL)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = float(tt.item()) / world
+
+    # roofline of the dominant kernel: the multicolour Stokes relaxation of this precision
+    kind = 7 if prec == 1 else 0
+    kms, kbytes = ctx.time_kernel(kind, 20)
+    peak, peak_src = peaks()
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as fh:
+                traffic = json.load(fh).get(args.workload, {}).get("relax_vel_" + args.precision)
+        except Exception:
+            traffic = None
+    out = {
+        "metric": METRIC, "value": value, "unit": "s/step", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32-in-f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "precision": args.precision,
+                   "stokes_rtol": args.rtol, "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "stokes_cycles": cycles[args.warmup:], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in
+                                                           ("ms_stokes", "ms_heat", "ms_move", "ms_r2n")},
+        "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "s/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "kernel": "k_relax_vel<%s>" % ("float" if prec else "double"),
+                     "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "bytes_per_launch": kbytes, "ms_per_launch": kms},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ncyc = int(np.median(cycles)) if cycles else 40
+        ctx.download(abi.SYNC_ALL)
+        try:
+            r = reference_sample(buf.to_prn(), mode, ncyc, os.cpu_count() or 1)
+        except Exception as e:  # the CPU baseline is reported, never required
+            r = None
+            out["cpu_baseline_error"] = str(e)[:300]
+        if r:
+            est, detail = r
+            out["cpu_baseline"] = {"value": est, "unit": "s/step", "cores": detail["threads"], "kind": "reference",
+                                   "sample": f"reference set-up + 1 V-cycle x {ncyc} V-cycles (this run's count to 1e-8), "
+                                             f"titerate, movemark, ronurecalc on the same model; phases {json.dumps(detail)}"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -99,10 +99,21 @@ def _ptr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
-class ModelBuffers:
-    """Numpy storage behind one ``Model`` struct."""
+def _pinned_like(a, keep):
+    """Page-locked copy of ``a`` (through torch) so host<->device copies run at full speed;
+    the owning tensor is appended to ``keep``."""
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    keep.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
 
-    def __init__(self, prn: Prn):
+
+class ModelBuffers:
+    """Numpy storage behind one ``Model`` struct (page-locked when ``pinned``)."""
+
+    def __init__(self, prn: Prn, pinned: bool = False):
         self.prn = prn
         n = prn.nodenum
         self.gx = np.ascontiguousarray(prn.gx, np.float32)
@@ -115,6 +126,11 @@ class ModelBuffers:
         for f in MARK_F32:
             self.f32[f] = np.ascontiguousarray(prn.marks[_MARK_SRC[f]], np.float32).copy()
         self.markt = np.ascontiguousarray(prn.marks["t"], np.int8).copy()
+        self._pinned = []
+        if pinned:
+            self.pr = _pinned_like(self.pr, self._pinned)
+            self.f32 = {k: _pinned_like(v, self._pinned) for k, v in self.f32.items()}
+            self.markt = _pinned_like(self.markt, self._pinned)
         b = prn.bond
         self.bond_row = np.ascontiguousarray(b["row"], np.int64)
         self.bond_c = np.ascontiguousarray(b["c"], np.float32)

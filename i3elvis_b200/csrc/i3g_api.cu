@@ -54,6 +54,7 @@ void i3g_destroy(i3g_ctx *c)
     for (void *p : f) cudaFree(p);
     for (int a = 0; a < 6; a++) { cudaFree(c->eps[a]); cudaFree(c->sig[a]); }
     if (c->hstage) cudaFreeHost(c->hstage);
+    if (c->tev[0]) { cudaEventDestroy(c->tev[0]); cudaEventDestroy(c->tev[1]); }
     delete[] c->hgx; delete[] c->hgy; delete[] c->hgz;
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -360,6 +361,26 @@ int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, doubl
     if (kind == 4 || kind == 5) return i3g::markers_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
     if (kind == 6) return i3g::heat_time_kernel(c, reps, ms_per_launch, bytes_per_launch);
     return i3g::stokes_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
+}
+
+int i3g_timer(i3g_ctx *c, int op, double *ms)
+{
+    if (!c) return I3G_E_ARG;
+    if (!c->tev[0]) {
+        I3G_CUDA(cudaEventCreate(&c->tev[0]));
+        I3G_CUDA(cudaEventCreate(&c->tev[1]));
+    }
+    if (op == 0) {
+        I3G_CUDA(cudaEventRecord(c->tev[0], c->st));
+        return 0;
+    }
+    if (op != 1 || !ms) return I3G_E_ARG;
+    I3G_CUDA(cudaEventRecord(c->tev[1], c->st));
+    I3G_CUDA(cudaEventSynchronize(c->tev[1]));
+    float t = 0;
+    I3G_CUDA(cudaEventElapsedTime(&t, c->tev[0], c->tev[1]));
+    *ms = t;
+    return 0;
 }
 
 }  // extern "C"

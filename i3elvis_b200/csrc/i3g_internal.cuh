@@ -111,6 +111,13 @@ struct i3g_ctx {
     i3g_stats st_;
     char err[512] = {0};
     int64_t launches = 0;
+    cudaEvent_t tev[2] = {nullptr, nullptr};   // i3g_timer
+    // captured Stokes iteration (one V-cycle + norms) and the parameters it was built with
+    cudaGraphExec_t sgraph = nullptr;
+    int sg_multinum = -1, sg_prec = -1;
+    double sg_p0 = 0, sg_p1 = 0, sg_v0 = 0, sg_v1 = 0;
+    long sg_nodes = 0;
+    double *dscale = nullptr;                   // device scale factors of the FP32 correction solve
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state
 };
@@ -122,6 +129,7 @@ namespace i3g {
 // stokes.cu
 int stokes_alloc(i3g_ctx *c);
 void stokes_free(i3g_ctx *c);
+void stokes_graph_free(i3g_ctx *c);
 int stokes_setup(i3g_ctx *c);
 int stokes_residual(i3g_ctx *c, int level);
 int stokes_smooth(i3g_ctx *c, int level, int nsweeps);

@@ -938,6 +938,7 @@ int stokes_alloc(i3g_ctx *c)
 
 void stokes_free(i3g_ctx *c)
 {
+    stokes_graph_free(c);
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
         delete[] L.gx; delete[] L.gy; delete[] L.gz;
@@ -1121,19 +1122,31 @@ int stokes_prolong(i3g_ctx *c, int level) { prolong_t<double>(c, level); I3G_CUD
 int stokes_vcycle(i3g_ctx *c, int multinum) { vcycle_t<double>(c, multinum, false); I3G_CUDA(cudaGetLastError()); return 0; }
 
 // relative residuals of the level-0 system (same definition as the oracle)
-int stokes_relres(i3g_ctx *c, double *mom, double *cont)
+// norms into the pinned host mirror (enqueued; read after the stream has passed them)
+static int relres_enqueue(i3g_ctx *c)
 {
     Level &L = c->lev[0];
     View<double> V = view<double>(L, L.d);
     LAUNCH(k_relres_part<double>, c->red_blocks, kRedThreads, V, c->dred);
     LAUNCH(k_red_final, 1, 32 * kRedQ, (const double *)c->dred, c->red_blocks, kRedQ, c->dred + (long)c->red_blocks * kRedQ);
     I3G_CUDA(cudaMemcpyAsync(c->hred, c->dred + (long)c->red_blocks * kRedQ, kRedQ * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    I3G_CUDA(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+static void relres_read(i3g_ctx *c, double *mom, double *cont)
+{
     const double *q = c->hred;
     *mom = q[1] > 0 ? std::sqrt(q[0] / q[1]) : std::sqrt(q[0]);
-    const double nc = (double)L.bcl[0].n, ncont = c->ncont, nvel = c->nvel;
-    (void)nc;
+    const double ncont = c->ncont, nvel = c->nvel;
     *cont = (ncont > 0 && q[3] > 0) ? std::sqrt(q[2] / ncont) * c->h_ref / std::sqrt(q[3] / nvel) : std::sqrt(q[2]);
+}
+
+int stokes_relres(i3g_ctx *c, double *mom, double *cont)
+{
+    int rc = relres_enqueue(c);
+    if (rc) return rc;
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    relres_read(c, mom, cont);
     return 0;
 }
 
@@ -1154,13 +1167,37 @@ __global__ void k_max_abs(const double *a, long n, double *part)
     }
 }
 
+// Scale factors of the FP32 correction solve from the largest momentum residual r:
+// e_v = sv * e_v', e_p = sp * e_p' with sv = r h^2 / eta_ref and sp = eta_ref sv / h, so that
+// the scaled rows (viscosity / eta_ref, lengths / h) have right-hand sides of order one.
+// scale = {momentum rhs factor, continuity rhs factor, sp, sv}
+__global__ void k_scale(const double *part, int nparts, double h, double er, double *scale)
+{
+    __shared__ double sh[32];
+    double m = 0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) m = fmax(m, part[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sh[w]);
+        if (!(m > 0)) m = 1.0;
+        const double sv = m * h * h / er, sp = er * sv / h;
+        scale[0] = h * h / (er * sv);
+        scale[1] = h / sv;
+        scale[2] = sp;
+        scale[3] = sv;
+    }
+}
+
 // FP32 scaled right-hand side from the FP64 residual; boundary rows get 0
 __global__ void k_to_f32(long n, const double *r0, const double *r1, const double *r2, const double *r3,
                          float *f0, float *f1, float *f2, float *f3, float *u0, float *u1, float *u2, float *u3,
-                         const uint8_t *bc, double sm, double sc)
+                         const uint8_t *bc, const double *scale)
 {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    const double sm = scale[0], sc = scale[1];
     const uint8_t b = bc[t];
     f0[t] = (b & 1) ? 0.f : (float)(r0[t] * sc);
     f1[t] = (b & 2) ? 0.f : (float)(r1[t] * sm);
@@ -1170,10 +1207,11 @@ __global__ void k_to_f32(long n, const double *r0, const double *r1, const doubl
 }
 
 __global__ void k_add_correction(long n, double *x0, double *x1, double *x2, double *x3, const float *e0,
-                                 const float *e1, const float *e2, const float *e3, double sp, double sv)
+                                 const float *e1, const float *e2, const float *e3, const double *scale)
 {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    const double sp = scale[2], sv = scale[3];
     x0[t] += sp * (double)e0[t];
     x1[t] += sv * (double)e1[t];
     x2[t] += sv * (double)e2[t];
@@ -1274,6 +1312,64 @@ static int finish_solve(i3g_ctx *c, double *timestep)
     return 0;
 }
 
+// One solver iteration: an FP64 V-cycle, or (mixed precision) r = b - A x in FP64, one FP32
+// V-cycle on the scaled correction system and x += e; then the level-0 norms to the host.
+static int enqueue_iteration(i3g_ctx *c, int multinum)
+{
+    Level &L0 = c->lev[0];
+    if (c->p.precision == 1) {
+        residual_t<double>(c, 0);
+        const int nb = c->red_blocks;
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], L0.n, c->dred);
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], L0.n, c->dred + nb);
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], L0.n, c->dred + 2 * nb);
+        LAUNCH(k_scale, 1, 1024, (const double *)c->dred, 3 * nb, c->h_ref, c->eta_ref, c->dscale);
+        LAUNCH(k_to_f32, nblk(L0.n), 256, L0.n, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+               (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
+               L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, (const double *)c->dscale);
+        vcycle_t<float>(c, multinum, true);
+        LAUNCH(k_add_correction, nblk(L0.n), 256, L0.n, L0.d.u[0], L0.d.u[1], L0.d.u[2], L0.d.u[3],
+               (const float *)L0.s.u[0], (const float *)L0.s.u[1], (const float *)L0.s.u[2], (const float *)L0.s.u[3],
+               (const double *)c->dscale);
+    } else {
+        vcycle_t<double>(c, multinum, false);
+    }
+    return relres_enqueue(c);
+}
+
+// Capture the iteration into a CUDA graph, re-capturing when its parameters change.
+static int iteration_graph(i3g_ctx *c, int multinum)
+{
+    if (c->sgraph && c->sg_multinum == multinum && c->sg_prec == c->p.precision && c->sg_p0 == c->p.p0koef &&
+        c->sg_p1 == c->p.p1koef && c->sg_v0 == c->p.v0koef && c->sg_v1 == c->p.v1koef)
+        return 0;
+    if (c->sgraph) { cudaGraphExecDestroy(c->sgraph); c->sgraph = nullptr; }
+    if (!c->dscale) I3G_CUDA(cudaMalloc((void **)&c->dscale, 16 * sizeof(double)));
+    const int64_t l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    I3G_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_iteration(c, multinum);
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&c->sgraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    c->sg_nodes = c->launches - l0;
+    c->launches = l0;
+    c->sg_multinum = multinum; c->sg_prec = c->p.precision;
+    c->sg_p0 = c->p.p0koef; c->sg_p1 = c->p.p1koef; c->sg_v0 = c->p.v0koef; c->sg_v1 = c->p.v1koef;
+    return 0;
+}
+
+void stokes_graph_free(i3g_ctx *c)
+{
+    if (c->sgraph) cudaGraphExecDestroy(c->sgraph);
+    c->sgraph = nullptr;
+    cudaFree(c->dscale);
+    c->dscale = nullptr;
+}
+
 int stokes_solve(i3g_ctx *c, double *timestep)
 {
     if (c->p.p2koef != 0 || c->f.p2koef != 0 || c->f.p2koef2 != 0)
@@ -1301,32 +1397,12 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;
     while (!conv && cycles < maxc) {
         for (int i = 0; i < ncyc && cycles < maxc && !conv; i++) {
-            if (c->p.precision == 1) {
-                // defect correction: r = b - A x (FP64), solve A e = r with one FP32 V-cycle
-                residual_t<double>(c, 0);
-                const int nb = c->red_blocks;
-                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], L0.n, c->dred);
-                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], L0.n, c->dred + nb);
-                LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], L0.n, c->dred + 2 * nb);
-                I3G_CUDA(cudaMemcpyAsync(c->hstage, c->dred, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->st));
-                I3G_CUDA(cudaStreamSynchronize(c->st));
-                double rmax = 0;
-                for (int b = 0; b < 3 * nb; b++) rmax = std::max(rmax, c->hstage[b]);
-                if (!(rmax > 0)) rmax = 1.0;
-                const double h = c->h_ref, er = c->eta_ref;
-                const double sv = rmax * h * h / er, sp = er * sv / h;
-                LAUNCH(k_to_f32, nblk(L0.n), 256, L0.n, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
-                       (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
-                       L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, h * h / (er * sv), h / sv);
-                vcycle_t<float>(c, multinum, true);
-                LAUNCH(k_add_correction, nblk(L0.n), 256, L0.n, L0.d.u[0], L0.d.u[1], L0.d.u[2], L0.d.u[3],
-                       (const float *)L0.s.u[0], (const float *)L0.s.u[1], (const float *)L0.s.u[2], (const float *)L0.s.u[3], sp, sv);
-            } else {
-                vcycle_t<double>(c, multinum, false);
-            }
+            if ((rc = iteration_graph(c, multinum))) return rc;
+            I3G_CUDA(cudaGraphLaunch(c->sgraph, c->st));
+            c->launches += c->sg_nodes;
+            I3G_CUDA(cudaStreamSynchronize(c->st));
             cycles++;
-            I3G_CUDA(cudaGetLastError());
-            if ((rc = stokes_relres(c, &mom, &cont))) return rc;
+            relres_read(c, &mom, &cont);
             if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
             conv = mom <= rtol && cont <= rtol;
         }

@@ -54,6 +54,7 @@ def load():
         getattr(L, name).argtypes = [P, C.c_int]
     L.i3g_stokes_smooth.argtypes = [P, C.c_int, C.c_int]
     L.i3g_stokes_relres.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.i3g_timer.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
     L.i3g_time_kernel.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _lib = L
     return L
@@ -139,6 +140,14 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self.call("i3g_stokes_relres", C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def timer_start(self):
+        self.call("i3g_timer", 0, None)
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        self.call("i3g_timer", 1, C.byref(ms))
+        return ms.value
 
     def time_kernel(self, kind: int, reps: int):
         ms, by = C.c_double(), C.c_double()

@@ -224,26 +224,47 @@ def _uniform_grid(n, size):
 
 
 def build_markers(spec: ModelSpec, seed: int):
+    """Markers on a regular sub-grid per cell in cell-major order (cell (z, x, y), inside a
+    cell (z, x, y)) as in in3mg.c:141-175, jittered as in in3mg.c:177-186."""
     nx, ny, nz = spec.shape
     xs, ys, zs = spec.size
     mx, my, mz = spec.mnum
     stp = (xs / (nx - 1), ys / (ny - 1), zs / (nz - 1))
     d = (stp[0] / mx, stp[1] / my, stp[2] / mz)
-    # cell-major order: cell (z, x, y), inside a cell (z, x, y) as in in3mg.c:141-175
-    c3, c1, c2, s5, s6, s7 = np.meshgrid(np.arange(nz - 1), np.arange(nx - 1), np.arange(ny - 1),
-                                         np.arange(mz), np.arange(mx), np.arange(my), indexing="ij")
-    x = c1 * stp[0] + d[0] / 2.0 + s6 * d[0]
-    y = c2 * stp[1] + d[1] / 2.0 + s7 * d[1]
-    z = c3 * stp[2] + d[2] / 2.0 + s5 * d[2]
-    x, y, z = (np.ascontiguousarray(a.reshape(-1)).astype(np.float32) for a in (x, y, z))
+    shape = (nz - 1, nx - 1, ny - 1, mz, mx, my)
+    cz = (np.arange(nz - 1) * stp[2])[:, None, None, None, None, None]
+    cx = (np.arange(nx - 1) * stp[0])[None, :, None, None, None, None]
+    cy = (np.arange(ny - 1) * stp[1])[None, None, :, None, None, None]
+    sz = (d[2] / 2.0 + np.arange(mz) * d[2])[None, None, None, :, None, None]
+    sx = (d[0] / 2.0 + np.arange(mx) * d[0])[None, None, None, None, :, None]
+    sy = (d[1] / 2.0 + np.arange(my) * d[1])[None, None, None, None, None, :]
+    x = np.broadcast_to((cx + sx).astype(np.float32), shape).reshape(-1).copy()
+    y = np.broadcast_to((cy + sy).astype(np.float32), shape).reshape(-1).copy()
+    z = np.broadcast_to((cz + sz).astype(np.float32), shape).reshape(-1).copy()
     if spec.nonstab:
         n = spec.nonstab
         rng = np.random.default_rng(seed)
         for arr, dd in ((x, d[0]), (y, d[1]), (z, d[2])):
-            r = rng.integers(0, 2 * n + 1, size=arr.size)
+            r = rng.integers(0, 2 * n + 1, size=arr.size, dtype=np.int32)
             jit = ((r - n).astype(np.float32) / np.float32(n)) * np.float32(spec.jitter * dd)
-            arr += jit.astype(np.float32)
+            arr += jit
     return x, y, z
+
+
+def markers_in_box(spec: ModelSpec, lo, hi):
+    """Indices of the markers of all cells overlapping the box [lo, hi] (cell-major order)."""
+    nx, ny, nz = spec.shape
+    mpc = int(np.prod(spec.mnum))
+    stp = [s / (n - 1) for s, n in zip(spec.size, spec.shape)]
+    rng_ = []
+    for a in range(3):
+        n1 = spec.shape[a] - 1
+        c0 = max(0, int(np.floor(lo[a] / stp[a])) - 1)
+        c1 = min(n1 - 1, int(np.floor(hi[a] / stp[a])) + 1)
+        rng_.append(np.arange(c0, c1 + 1))
+    cx, cy, cz = rng_
+    cells = (cz[:, None, None] * ((nx - 1) * (ny - 1)) + cx[None, :, None] * (ny - 1) + cy[None, None, :]).reshape(-1)
+    return (cells[:, None] * mpc + np.arange(mpc)[None, :]).reshape(-1)
 
 
 def make_prn(spec: ModelSpec, rocks: dict, types: np.ndarray, marks_xyz, seed: int = 0) -> Prn:
@@ -333,14 +354,11 @@ def random_inclusions(n=129, size_km=200.0, mnum=3, multinum=4, seed=7, count=10
             10 ** ((b % nc + 0.5) * np.log10(contrast) / nc) if contrast else 1.0)
         rocks[INCLUSION_TYPES[b]] = dataclasses.replace(mat, nu=A * c_mean, ro=float(d_mean))
     xyz = build_markers(spec, seed)
-    x, y, z = (a.astype(np.float64) for a in xyz)
-    types = np.full(x.size, MATRIX, np.int64)
+    x, y, z = xyz
+    types = np.full(x.size, MATRIX, np.int8)
     for i in range(count):
-        # cheap bounding-box prefilter before the distance test
         r = rad[i]
-        sel = ((np.abs(x - cen[i, 0]) <= r) & (np.abs(y - cen[i, 1]) <= r) & (np.abs(z - cen[i, 2]) <= r))
-        idx = np.nonzero(sel)[0]
-        if idx.size:
-            d2 = (x[idx] - cen[i, 0]) ** 2 + (y[idx] - cen[i, 1]) ** 2 + (z[idx] - cen[i, 2]) ** 2
-            types[idx[d2 <= r * r]] = INCLUSION_TYPES[tbin[i]]
+        idx = markers_in_box(spec, cen[i] - r, cen[i] + r)
+        d2 = ((x[idx] - cen[i, 0]) ** 2 + (y[idx] - cen[i, 1]) ** 2 + (z[idx] - cen[i, 2]) ** 2)
+        types[idx[d2 <= r * r]] = INCLUSION_TYPES[tbin[i]]
     return make_prn(spec, rocks, types, xyz, seed), spec

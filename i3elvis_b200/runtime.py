@@ -25,17 +25,13 @@ def hydrostatic_pressure(buf: abi.ModelBuffers) -> None:
     if g <= 0:
         return
     gy = buf.gy.astype(np.float64)
-    ro = buf.f32["ro"].reshape(nz, nx, ny).astype(np.float64)
+    ro = buf.f32["ro"].reshape(nz, nx, ny)
     pr = buf.pr.reshape(nz, nx, ny)
-    pinit = float(h["pinit"])
-    for m3 in range(1, nz):
-        for m1 in range(1, nx):
-            p = pinit
-            pr[m3, m1, 1] = p
-            for m2 in range(2, ny):
-                rav = (ro[m3, m1, m2 - 1] + ro[m3, m1 - 1, m2 - 1] + ro[m3 - 1, m1, m2 - 1] + ro[m3 - 1, m1 - 1, m2 - 1]) / 4.0
-                p = p + (gy[m2] - gy[m2 - 2]) / 2.0 * g * rav
-                pr[m3, m1, m2] = p
+    # mean density of the 4 nodes around each vertical cell edge, FP32 sum as in C
+    rs = ((ro[1:, 1:, 1:-1] + ro[1:, :-1, 1:-1]) + ro[:-1, 1:, 1:-1]) + ro[:-1, :-1, 1:-1]
+    inc = (gy[2:] - gy[:-2])[None, None, :] / 2.0 * g * (rs.astype(np.float64) / 4.0)
+    pr[1:, 1:, 1] = float(h["pinit"])
+    pr[1:, 1:, 2:] = float(h["pinit"]) + np.cumsum(inc, axis=2)
 
 
 def prepare(ctx: lib.Context) -> None:

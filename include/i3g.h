@@ -201,6 +201,11 @@ int i3g_stokes_relres(i3g_ctx *c, double *mom_rel, double *cont_rel);
  * 4 marker->node, 5 RK4 advection, 6 heat sweep. */
 int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, double *bytes_per_launch);
 
+/* Device-side stopwatch on the context stream (no reference counterpart: the reference
+ * times phases with clock(), i3mg.c:96-139).  op 0 records the start event; op 1 records
+ * the stop event, waits for it and returns the elapsed milliseconds in *ms. */
+int i3g_timer(i3g_ctx *c, int op, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

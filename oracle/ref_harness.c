@@ -377,6 +377,26 @@ int main(int argc, char **argv)
         dump_nodes(argv[2]);
         return 0;
     }
+    if (!strcmp(cmd, "sample") && argc == 3) {
+        /* bounded timing sample of one time step: the reference's set-up and one V-cycle of
+         * vpiterate (move3mg.c:1948-2223), titerate, movemark and ronurecalc, wall clock */
+        int ncyc = atoi(argv[2]);
+        double t0 = omp_get_wtime();
+        stokes_assemble();
+        double t1 = omp_get_wtime();
+        for (int i = 0; i < ncyc; i++) vcycle();
+        double t2 = omp_get_wtime();
+        if (tempmod) titerate(0);
+        double t3 = omp_get_wtime();
+        if (markmod) movemark();
+        double t4 = omp_get_wtime();
+        if (gridmod) ronurecalc();
+        double t5 = omp_get_wtime();
+        printf("{\"assemble_s\": %.4f, \"vcycle_s\": %.4f, \"ncyc\": %d, \"heat_s\": %.4f, \"move_s\": %.4f, "
+               "\"r2n_s\": %.4f, \"threads\": %d}\n", t1 - t0, (t2 - t1) / (ncyc > 0 ? ncyc : 1), ncyc, t3 - t2,
+               t4 - t3, t5 - t4, omp_get_max_threads());
+        return 0;
+    }
     if (!strcmp(cmd, "step") && argc == 3) {
         double t[5];
         t[0] = omp_get_wtime();
