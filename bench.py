@@ -62,7 +62,7 @@ def build_case(name, seed_offset=0):
         infile="in0.prn", multinum=mn, multicyc=1, multinnn=(down, up),
         p0koef=0.71, p1koef=1.0, v0koef=0.7, v1koef=0.7, nubeg=1e18, nuend=1e24,
         files=[config.OutFile("out1.prn", maxxystep=0.5 * dx, maxtmstep_yr=1e9, nubeg=1e18, nuend=1e24,
-                              p0koef=0.71, p1koef=1.0, multinum=mn, multinum2=mn)])
+                              p0koef=0.71, p1koef=1.0, p0koef2=0.71, p1koef2=0.0, multinum=mn, multinum2=mn)])
     return prn, mode
 
 

@@ -1395,6 +1395,9 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     bool conv = mom <= rtol && cont <= rtol;
     const double p0_save = c->p.p0koef, p1_save = c->p.p1koef;
     const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;
+    double prev = std::max(mom, cont);
+    int rises = 0;
+    bool switched = false;
     while (!conv && cycles < maxc) {
         for (int i = 0; i < ncyc && cycles < maxc && !conv; i++) {
             if ((rc = iteration_graph(c, multinum))) return rc;
@@ -1405,12 +1408,26 @@ int stokes_solve(i3g_ctx *c, double *timestep)
             relres_read(c, &mom, &cont);
             if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
             conv = mom <= rtol && cont <= rtol;
+            // Safeguard: a residual that grows three cycles running switches to the file row's
+            // second relaxation set early (the reference switches after multstp iterations,
+            // move3mg.c:2585-2593).
+            const double cur = std::max(mom, cont);
+            rises = cur > prev ? rises + 1 : 0;
+            prev = cur;
+            if (rises >= 3 && !switched && (c->p.p0koef != c->f.p0koef2 || c->p.p1koef != c->f.p1koef2)) {
+                c->p.p0koef = c->f.p0koef2;
+                c->p.p1koef = c->f.p1koef2;
+                multinum = std::min(c->f.multinum2 > 0 ? c->f.multinum2 : multinum, c->nlev - 1);
+                switched = true;
+                rises = 0;
+            }
         }
         outer++;
-        if (outer >= c->f.multstp && c->f.multstp > 0) {   // move3mg.c:2585-2593
+        if (outer >= c->f.multstp && c->f.multstp > 0 && !switched) {   // move3mg.c:2585-2593
             multinum = std::min(c->f.multinum2 > 0 ? c->f.multinum2 : multinum, c->nlev - 1);
             c->p.p0koef = c->f.p0koef2;
             c->p.p1koef = c->f.p1koef2;
+            switched = true;
         }
     }
     c->p.p0koef = p0_save;
