@@ -82,6 +82,13 @@ def run(workdir: str, max_files: int | None = None, **solver) -> list:
     prn = read_prn(os.path.join(workdir, infile))
     buf = abi.ModelBuffers(prn)
     ctx = lib.Context(buf, abi.make_params(mode, **solver))
+    if mode.cyc1max < 0:
+        # reset v, P, strain rates and stresses, then nodes from markers (i3mg.c:40-52)
+        buf.pr[:] = 0.0
+        for f in ("vx", "vy", "vz") + abi.STRESS_F32:
+            buf.f32[f][:] = 0.0
+        ctx.upload(abi.SYNC_NODES | abi.SYNC_STRESS)
+        ctx.markers_to_nodes(0.0)
     log = []
     first = fln3 + 1
     last = min(first + mode.filesjob, len(mode.files))
