@@ -28,6 +28,16 @@ int cuda_fail(i3g_ctx *c, cudaError_t e, const char *what, const char *file, int
 
 static thread_local char g_err[512];
 
+// failures of entry points that have no context (reported by i3g_last_error(NULL))
+int set_global_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
 template <typename T>
 static int dup_to_device(i3g_ctx *c, T *&dst, const T *src, long n)
 {

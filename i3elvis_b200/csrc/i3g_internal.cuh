@@ -124,6 +124,7 @@ struct i3g_ctx {
 
 int cuda_fail(i3g_ctx *c, cudaError_t e, const char *what, const char *file, int line);
 int set_error(i3g_ctx *c, int code, const char *fmt, ...);
+int set_global_error(int code, const char *fmt, ...);
 
 namespace i3g {
 // stokes.cu

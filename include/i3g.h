@@ -206,6 +206,31 @@ int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, doubl
  * the stop event, waits for it and returns the elapsed milliseconds in *ms. */
 int i3g_timer(i3g_ctx *c, int op, double *ms);
 
+/* ---- allocation-free stopping test (no counterpart in the reference) --------------- */
+/* For host codes that may not allocate device memory after start-up (they give all of it
+ * to their own pool allocator, or cannot let a cudaMalloc synchronise the device under work
+ * they have queued) and so cannot create a context.  Computes the two numbers of
+ * i3g_stokes_relres() -- momentum ||b - Ax|| / ||b|| and continuity RMS(div v) * h / RMS(v)
+ * over the non-boundary rows -- from a level-0 system in the caller's device memory, in
+ * the library's layout (node = z*nx*ny + x*ny + y; one array per component):
+ *   res[4]  device residuals of the P, Vx, Vy, Vz rows (b - Ax)
+ *   rhs[4], sol[4]  device right-hand sides and solution (index 0, pressure, is not read)
+ *   bc      device byte per node, bit v set when row v of that node is a boundary row
+ *   h       mean grid spacing, (xsize/(nx-1) + ysize/(ny-1) + zsize/(nz-1)) / 3
+ *   out     device, 2 doubles: momentum, continuity
+ *   stream  cudaStream_t the two kernels are queued on (NULL: the legacy default stream);
+ *           the call returns without waiting for them.
+ * It allocates nothing: its scratch is a static device array of I3G_NOALLOC_MAX_COLUMNS x 6
+ * doubles (3 MiB, held by every GPU that loads the library until the process exits), one
+ * slot per x-z grid column, so grids with nx*nz > I3G_NOALLOC_MAX_COLUMNS are rejected with
+ * I3G_E_ARG.  The first call on each device looks up the array's device address (make it
+ * before any stream capture on that device).  All calls share the array: calls whose kernels
+ * may overlap on the GPU race.  Errors are read with i3g_last_error(NULL). */
+#define I3G_NOALLOC_MAX_COLUMNS 65536
+int i3g_stokes_relres_noalloc(int nx, int ny, int nz, double h, const uint8_t *bc,
+                              const double *const res[4], const double *const rhs[4],
+                              const double *const sol[4], double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
