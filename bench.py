@@ -45,7 +45,9 @@ WORKLOADS = {
 }
 
 
-def build_case(name, seed_offset=0):
+def build_case(name, seed_offset=0, sweeps=None):
+    """Seeded model and mode of a named workload.  ``sweeps`` = "d0,d1,../u0,u1,..,uc" replaces
+    the relaxation sweeps per level (down leg / up leg, the coarsest level last on the up leg)."""
     w = WORKLOADS[name]
     if name.startswith("sphere"):
         prn, spec = model.sinking_sphere(n=w["n"], mnum=w["mnum"], multinum=w["multinum"], seed=w["seed"] + seed_offset)
@@ -57,6 +59,12 @@ def build_case(name, seed_offset=0):
     mn = w["multinum"]
     down = (8, 16, 16, 32, 32, 32)[:mn] + (0,)
     up = (8, 16, 16, 32, 32, 32)[:mn] + (64,)
+    if sweeps:
+        d, u = sweeps.split("/")
+        down = tuple(int(v) for v in d.split(",")) + (0,)
+        up = tuple(int(v) for v in u.split(","))
+        if len(down) != mn + 1 or len(up) != mn + 1:
+            raise SystemExit(f"--sweeps needs {mn} down and {mn + 1} up counts")
     dx = size / (w["n"] - 1)
     mode = config.Mode(
         infile="in0.prn", multinum=mn, multicyc=1, multinnn=(down, up),
@@ -118,10 +126,16 @@ class Clocks:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
 
 
+def _est(r, ncyc):
+    """Step estimate from one sample: set-up + ncyc V-cycles + heat + advection + marker->node."""
+    return r["assemble_s"] + ncyc * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
+
+
 def reference_sample(prn, mode, ncyc_for_1e8, threads):
     """Time the reference's own functions on this workload (bounded sample, all host threads):
-    vpiterate set-up + one V-cycle, titerate, movemark, ronurecalc.  The step estimate scales
-    the V-cycle by the number of V-cycles this multigrid needs for relative residual 1e-8."""
+    vpiterate set-up + one V-cycle, titerate, movemark, ronurecalc on the prepared model.  The
+    step estimate scales the V-cycle by the number of V-cycles this multigrid needs for
+    relative residual 1e-8."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.have_reference():
@@ -130,11 +144,10 @@ def reference_sample(prn, mode, ncyc_for_1e8, threads):
         write_prn(os.path.join(d, "in0.prn"), prn)
         config.write_mode(os.path.join(d, "mode.t3c"), mode)
         config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-        r = O.run_reference(d, "sample", 1, threads=threads, timeout=1200)
-    if not r:
+        rs = O.run_reference_lines(d, "sample", 1, 1, 0, threads=threads, timeout=1200)
+    if not rs:
         return None
-    est = r["assemble_s"] + ncyc_for_1e8 * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
-    return est, r
+    return _est(rs[-1], ncyc_for_1e8), rs[-1]
 
 
 def run_reference_arm(args):
@@ -143,33 +156,28 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    prn, mode = build_case(args.workload)
+    prn, mode = build_case(args.workload, sweeps=args.sweeps)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.have_reference():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built (reference sources absent at build time)"}))
         return 0
     ncyc = args.ref_cycles
-    times = []
-    detail = None
     with tempfile.TemporaryDirectory() as d:
         write_prn(os.path.join(d, "in0.prn"), prn)
         config.write_mode(os.path.join(d, "mode.t3c"), mode)
         config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-        # the reference's own initial-condition passes (in3mg.c:990-1031)
-        O.run_reference(d, "prepare", "prep.prn", threads=threads, timeout=1800)
-        mode.infile = "prep.prn"
-        config.write_mode(os.path.join(d, "mode.t3c"), mode)
-        for i in range(args.warmup + args.steps):
-            r = O.run_reference(d, "sample", 1, threads=threads, timeout=1800)
-            est = r["assemble_s"] + ncyc * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
-            if i >= args.warmup:
-                times.append(est)
-                detail = r
+        # one process: the reference's initial-condition passes (in3mg.c:990-1031), then
+        # warmup + timed steps, each a sample of the step (see the harness's sample command)
+        rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, threads=threads, timeout=3000)
+    timed = rs[args.warmup:]
+    times = [_est(r, ncyc) for r in timed]
+    detail = timed[-1] if timed else None
     v = float(np.mean(times))
-    sample = (f"per step: reference vpiterate set-up + 1 V-cycle (x {ncyc} V-cycles to relative residual 1e-8), "
-              f"titerate, movemark, ronurecalc on the full {args.workload} model, {threads} OpenMP threads; "
-              f"phases {json.dumps(detail)}")
+    sample = (f"per step: reference vpiterate set-up + 1 V-cycle (x {ncyc} V-cycles, the count this multigrid "
+              f"needs for relative residual 1e-8), velocities and CFL step from that iterate, titerate, movemark, "
+              f"ronurecalc on the full {args.workload} model, {threads} OpenMP threads, one process after the "
+              f"reference's initial-condition passes; last timed step {json.dumps(detail)}")
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s/step", "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -188,8 +196,11 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=("fp64", "mixed"))
     ap.add_argument("--workload", default="incl129", choices=tuple(WORKLOADS))
     ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--sweeps", default=None, help="relaxation sweeps per level, 'down,../up,..'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("I3G_REF_CYCLES", "40")))
+    # V-cycles per step that the reference-arm estimate charges: the count the FP64 multigrid
+    # takes to relative residual 1e-8 on incl129 on the GPU (21-22 per step after warm-up)
+    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("I3G_REF_CYCLES", "21")))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -204,7 +215,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
-    prn, mode = build_case(args.workload, seed_offset=rank)
+    prn, mode = build_case(args.workload, seed_offset=rank, sweeps=args.sweeps)
     prec = 1 if args.precision == "mixed" else 0
     par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec)
     buf = abi.ModelBuffers(prn, pinned=True)
@@ -279,7 +290,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32-in-f64", "data": "synthetic",
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "precision": args.precision,
-                   "stokes_rtol": args.rtol, "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+                   "stokes_rtol": args.rtol, "sweeps": [list(mode.multinnn[0]), list(mode.multinnn[1])],
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "stokes_cycles": cycles[args.warmup:], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in
                                                            ("ms_stokes", "ms_heat", "ms_move", "ms_r2n")},
         "gpu_launches": int(launches),

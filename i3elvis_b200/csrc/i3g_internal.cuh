@@ -118,6 +118,7 @@ struct i3g_ctx {
     double sg_p0 = 0, sg_p1 = 0, sg_v0 = 0, sg_v1 = 0;
     long sg_nodes = 0;
     double *dscale = nullptr;                   // device scale factors of the FP32 correction solve
+    long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state
 };

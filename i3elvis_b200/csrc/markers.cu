@@ -1,14 +1,15 @@
 // markers.cu -- marker advection (movemark, mark3mg.c:2-397) and marker -> node averaging
 // (ronurecalc, mark3mg.c:404-1015) for sm_100a.
 //
-// Markers live on the device as structure-of-arrays and are kept ordered by cell tile
-// (4 x 32 x 4 cells): after every advection a counting sort by tile regroups them, so the
-// marker -> node pass can give each CTA one tile, stage the tile's node sums in shared
-// memory (FP64) and touch global memory only once per node instead of once per marker.
-// The reference's scatter (mark3mg.c:848-924) adds into shared node arrays from many
-// threads without atomics; here the only global atomics are for nodes on tile faces,
-// after the marker loop.  An original-index array lets downloads return markers in the
-// reference's order.
+// Markers live on the device as structure-of-arrays, sorted by cell inside cell tiles
+// (4 x 32 x 4 cells): after every advection a counting sort by (tile, cell) regroups them.
+// The marker -> node pass gives each CTA one tile and each warp one cell: the warp computes
+// its markers' properties, then sums them per node of the cell in registers, and adds the
+// per-cell sums to the tile's FP64 node sums in shared memory in 8 parity classes of cells
+// that share no node -- no atomics inside the tile.  The reference's scatter
+// (mark3mg.c:848-924) adds into shared node arrays from many threads without atomics; here
+// the only atomics are the global ones for nodes on tile faces, once per tile.  An
+// original-index array lets downloads return markers in the reference's order.
 //
 // This file is compiled with -fmad=false so that the interpolation arithmetic rounds like
 // the CPU restatement (transcendentals may still differ in the last unit).
@@ -36,9 +37,12 @@ struct Marks {
 struct MarkerState {
     long n = 0;
     Marks a{}, b{};                 // current arrays and the sort target
-    int *key = nullptr;             // tile per marker (ntiles = not scattered)
-    int *cnt = nullptr, *off = nullptr, *cur = nullptr;
+    int *key = nullptr;             // sort key per marker: tile * cells per tile + cell in tile
+    int *cnt = nullptr, *coff = nullptr, *cur = nullptr;   // per cell (+ inactive bin)
+    int *off = nullptr;             // per tile: first marker (ntiles + 1 entries)
+    int *bsum = nullptr;            // scan chunk sums
     int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
+    long nbins = 0;                 // cells of all tiles + inactive bin + end
     double *acc = nullptr;          // [NACC * nodenum] node sums
     float *tk1 = nullptr;           // copy of T before boundary rows
     double *rock = nullptr;         // [24 * rocknum]
@@ -366,7 +370,7 @@ __device__ __forceinline__ double inv2(const double *e)
 // ------------------------------------------------------------------------------------
 // movemark: rheology update + RK4 (mark3mg.c:49-310)
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
+__global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
 {
     extern __shared__ double shg[];
     Grid G;
@@ -443,13 +447,22 @@ __device__ __forceinline__ bool r2n_active(const Grid &G, float x, float y, floa
     return x > 0 && y > 0 && z > 0 && x < G.xsize && y < G.ysize && z < G.zsize && t < 50;
 }
 
+constexpr int CPT = TX * TY * TZ;   // cells per tile
+
+// sort key: tile, then cell inside the tile (y fastest); inactive markers sort last
+__device__ __forceinline__ int cell_key(int c1, int c2, int c3, const TileGeo &T)
+{
+    const int tile = ((c3 / TZ) * T.ntx + (c1 / TX)) * T.nty + (c2 / TY);
+    return tile * CPT + ((c3 % TZ) * TX + (c1 % TX)) * TY + (c2 % TY);
+}
+
 __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *cnt)
 {
     extern __shared__ double shg[];
     Grid G;
     load_grid(Gg, shg, G);
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    int kk = T.ntiles;
+    int kk = T.ntiles * CPT;
     if (i < n) {
         const float x = M.x[i], y = M.y[i], z = M.z[i];
         if (r2n_active(G, x, y, z, M.t[i], M.k[i])) {
@@ -457,8 +470,7 @@ __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *c
             if (xd > G.xsize) xd = G.xsize;
             if (yd > G.ysize) yd = G.ysize;
             if (zd > G.zsize) zd = G.zsize;
-            const int c1 = bsearch_g(G.gx, G.nx, xd), c2 = bsearch_g(G.gy, G.ny, yd), c3 = bsearch_g(G.gz, G.nz, zd);
-            kk = ((c3 / TZ) * T.ntx + (c1 / TX)) * T.nty + (c2 / TY);
+            kk = cell_key(bsearch_g(G.gx, G.nx, xd), bsearch_g(G.gy, G.ny, yd), bsearch_g(G.gz, G.nz, zd), T);
         }
         key[i] = kk;
     }
@@ -471,24 +483,73 @@ __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *c
     }
 }
 
-__global__ void k_scan(const int *cnt, int *off, int *cur, int n)
+// exclusive scan of n counts in three passes: chunk sums, scan of the chunk sums, chunk scans
+constexpr int kScanT = 1024, kScanPer = 4, kScanChunk = kScanT * kScanPer;
+
+__device__ __forceinline__ int block_excl_scan(int v, int *total)
 {
-    // single block exclusive scan over n+1 bins (n up to a few hundred thousand)
-    __shared__ int part[1024];
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per, e = min(n, b + per);
-    int s = 0;
-    for (int q = b; q < e; q++) s += cnt[q];
-    part[threadIdx.x] = s;
+    __shared__ int wsum[kScanT / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int q = 0; q < (int)blockDim.x; q++) { int v = part[q]; part[q] = run; run += v; }
+    if (w == 0) {
+        int t = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        wsum[lane] = t;   // inclusive
     }
     __syncthreads();
-    int run = part[threadIdx.x];
-    for (int q = b; q < e; q++) { off[q] = run; cur[q] = run; run += cnt[q]; }
-    if (threadIdx.x == blockDim.x - 1) off[n] = run;
+    const int before = (w ? wsum[w - 1] : 0) + x - v;
+    *total = wsum[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanT) k_scan_part(const int *cnt, long n, int *bsum)
+{
+    const long b0 = (long)blockIdx.x * kScanChunk + (long)threadIdx.x * kScanPer;
+    int s = 0;
+    for (int q = 0; q < kScanPer; q++) s += b0 + q < n ? cnt[b0 + q] : 0;
+    int total;
+    block_excl_scan(s, &total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanT) k_scan_top(int *bsum, int nb)
+{
+    // one block: exclusive scan of nb chunk sums in place
+    const int per = (nb + kScanT - 1) / kScanT;
+    const int b = threadIdx.x * per;
+    int s = 0;
+    for (int q = b; q < b + per && q < nb; q++) s += bsum[q];
+    int total;
+    int run = block_excl_scan(s, &total);
+    for (int q = b; q < b + per && q < nb; q++) { const int v = bsum[q]; bsum[q] = run; run += v; }
+}
+
+__global__ void __launch_bounds__(kScanT) k_scan_apply(const int *cnt, long n, const int *bsum, int *off, int *cur)
+{
+    const long b0 = (long)blockIdx.x * kScanChunk + (long)threadIdx.x * kScanPer;
+    int v[kScanPer], s = 0;
+    for (int q = 0; q < kScanPer; q++) { v[q] = b0 + q < n ? cnt[b0 + q] : 0; s += v[q]; }
+    int total;
+    int run = bsum[blockIdx.x] + block_excl_scan(s, &total);
+    for (int q = 0; q < kScanPer; q++)
+        if (b0 + q < n) { off[b0 + q] = run; cur[b0 + q] = run; run += v[q]; }
+}
+
+// tile offsets from cell offsets
+__global__ void k_tile_off(const int *coff, int ntiles, int *toff)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= ntiles) toff[t] = coff[(long)t * CPT];
 }
 
 __global__ void k_tile_scatter(Marks A, Marks B, long n, const int *key, int *cur)
@@ -539,93 +600,146 @@ __device__ __forceinline__ void phase_density(const Phys &P, int mm2, double mtk
     }
 }
 
-__global__ void __launch_bounds__(512) k_r2n_tile(Marks M, const int *off, Grid Gg, NodeF F, Phys P, TileGeo T,
-                                                  double timestep, double *acc, long N)
+// Each CTA owns one tile; markers are sorted by cell inside the tile.  A warp takes one cell:
+// lanes first compute the properties of up to 32 of its markers (stage 1, one marker per
+// lane) into a shared staging area, then lane = 4 * node + group accumulates, for one of the
+// cell's 8 nodes, one group of the 18 node sums over all staged markers (stage 2).  Cells are
+// visited in 8 parity classes; cells of one class share no node, so the per-cell sums are
+// added to the shared node sums without atomics, in a fixed order.
+constexpr int kR2nWarps = 16;
+constexpr int kStage = 14;   // ddx0 ddx1 ddy0 ddy1 ddz0 ddz1 vnu mro mcp*mro mkt mht mbb mtk mrr
+
+__global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int *coff, Grid Gg, NodeF F, Phys P,
+                                                              TileGeo T, double timestep, double *acc, long N)
 {
     extern __shared__ double sm[];
-    double *sacc = sm;                          // [NACC][NBOX]
-    double *shg = sm + NACC * NBOX;             // grid lines
+    double *sacc = sm;                                   // [NACC][NBOX]
+    double *stg = sm + NACC * NBOX;                      // [kR2nWarps][32][kStage]
+    double *shg = stg + kR2nWarps * 32 * kStage;         // grid lines
     for (int q = threadIdx.x; q < NACC * NBOX; q += blockDim.x) sacc[q] = 0;
     Grid G;
     load_grid(Gg, shg, G);   // contains __syncthreads
     const int tile = blockIdx.x;
     const int ty = tile % T.nty, rest = tile / T.nty, tx = rest % T.ntx, tz = rest / T.ntx;
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
-    const int beg = off[tile], end = off[tile + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *my = stg + warp * 32 * kStage;
+    const int nd = lane >> 2, grp = lane & 3;
+    const int iz = nd >> 2, ix = (nd >> 1) & 1, iy = nd & 1;
     const int vm = P.viscmod;
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
-        int mm2 = M.t[i];
-        const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
-        if (!(M.k[i] > 0)) continue;
-        if (mm2 > 1 && fy < P.eroslev) { mm2 = 0; M.t[i] = 0; }
-        if (mm2 < 2) { atomicOr(P.err, ERR_WATER); continue; }
-        if (mm2 > 20) { atomicOr(P.err, ERR_MELT); continue; }
-        if (P.densimod >= 2) { atomicOr(P.err, ERR_DENSI); continue; }
-        int wn[3];
-        const double mpb = pr_at(G, F.pr, F.NY, F.NXY, fx, fy, fz, wn) * 1e-5;
-        const double mtk = M.k[i];
-        double mnu = M.v[i];
-        if (mnu <= 0 || timestep <= 0) {
-            double e[7], s[6], dis;
-            eps_at(G, F, fx, fy, fz, wn, e, s, &dis);
-            float me = M.e[i], mft = M.ft[i];
-            mnu = visc(P, mtk, mpb, mm2, inv2(e), 1.0, me, mft);
-            if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); continue; }
-            M.v[i] = (float)mnu; M.e[i] = me; M.ft[i] = mft;
-        }
-        double mbb = 0, mro = RK(P, R_RO, mm2);
-        if (P.densimod != 0) {   // dencalc1 (mark3mg.c:3006-3024)
-            const double bb = RK(P, R_BB, mm2);
-            mbb = bb / (1.0 - bb * (mtk - 298.15));
-            mro = mro * (1.0 - bb * (mtk - 298.15)) * (1.0 + RK(P, R_AA, mm2) * (mpb - 1.0) * 1e-3);
-        }
-        phase_density(P, mm2, mtk, mpb, mro);
-        const double mcp = RK(P, R_CP, mm2);
-        const double mkt = (RK(P, R_KT, mm2) + RK(P, R_KF, mm2) / (mtk + 77.0)) * exp(RK(P, R_KP, mm2) * mpb);
-        const double mht = RK(P, R_HT, mm2);
-        if (fy > P.vdeep && mnu > P.nudeep) mnu = P.nudeep;
-        if (fy < 5e+4 && fx > G.xsize - 1e+4 && fz > 1.5e+5 && fz < 8.7e+5 && mnu > 1e+19) mnu = 1e+19;
-        const int m10 = wn[0], m20 = wn[1], m30 = wn[2];
-        const double dx = G.gx[m10 + 1] - G.gx[m10], dy = G.gy[m20 + 1] - G.gy[m20], dz = G.gz[m30 + 1] - G.gz[m30];
-        const double vnu = vm == 0 ? mnu : vm == 1 ? log(mnu) : 1.0 / mnu;
-        const double mrr = M.rr[i];
-        for (int m3 = m30; m3 <= m30 + 1; m3++) {
-            double ddz = (G.gz[m3] - fz) / dz; ddz = 1.0 - fabs(ddz);
-            for (int m1 = m10; m1 <= m10 + 1; m1++) {
-                double ddx = (G.gx[m1] - fx) / dx; ddx = 1.0 - fabs(ddx);
-                for (int m2 = m20; m2 <= m20 + 1; m2++) {
-                    double ddy = (G.gy[m2] - fy) / dy; ddy = 1.0 - fabs(ddy);
-                    const double swt = ddx * ddy * ddz;
-                    const int lb = ((m3 - cz0) * NBX + (m1 - cx0)) * NBY + (m2 - cy0);
-                    double *a = sacc + lb;
-                    if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { atomicAdd(a + A_NU * NBOX, vnu * swt); atomicAdd(a + W_NU * NBOX, swt); }
-                    if (m1 > m10 && m2 > m20 && m3 > m30) {
-                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
-                        atomicAdd(a + A_XX * NBOX, vnu * w1); atomicAdd(a + W_XX * NBOX, w1);
-                    }
-                    if (m3 == m30 && ddx > 0.5 && ddy > 0.5) {
-                        const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
-                        atomicAdd(a + A_XY * NBOX, vnu * w1); atomicAdd(a + W_XY * NBOX, w1);
-                    }
-                    if (m2 == m20 && ddx > 0.5 && ddz > 0.5) {
-                        const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
-                        atomicAdd(a + A_XZ * NBOX, vnu * w1); atomicAdd(a + W_XZ * NBOX, w1);
-                    }
-                    if (m1 == m10 && ddy > 0.5 && ddz > 0.5) {
-                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
-                        atomicAdd(a + A_YZ * NBOX, vnu * w1); atomicAdd(a + W_YZ * NBOX, w1);
-                    }
-                    if (swt > 0) {
-                        atomicAdd(a + A_RO * NBOX, mro * swt); atomicAdd(a + A_CP * NBOX, mcp * mro * swt);
-                        atomicAdd(a + A_KT * NBOX, mkt * swt); atomicAdd(a + A_HT * NBOX, mht * swt);
-                        atomicAdd(a + A_ET * NBOX, mbb * swt); atomicAdd(a + A_TK * NBOX, mtk * swt);
-                        atomicAdd(a + A_RR * NBOX, mrr * swt); atomicAdd(a + W_P * NBOX, swt);
+    for (int colour = 0; colour < 8; colour++) {
+        const int pz = colour >> 2, px = (colour >> 1) & 1, py = colour & 1;
+        for (int q = warp; q < CPT / 8; q += kR2nWarps) {
+            const int ly = 2 * (q % (TY / 2)) + py, r2 = q / (TY / 2);
+            const int lx = 2 * (r2 % (TX / 2)) + px, lz = 2 * (r2 / (TX / 2)) + pz;
+            const long cell = (long)tile * CPT + (lz * TX + lx) * TY + ly;
+            const int beg = coff[cell], end = coff[cell + 1];
+            if (beg == end) continue;   // uniform over the warp
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+            for (int base = beg; base < end; base += 32) {
+                // stage 1: one marker per lane
+                bool ok = false;
+                if (base + lane < end) {
+                    const int i = base + lane;
+                    int mm2 = M.t[i];
+                    const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+                    ok = M.k[i] > 0;
+                    if (ok && mm2 > 1 && fy < P.eroslev) { mm2 = 0; M.t[i] = 0; }
+                    if (ok && mm2 < 2) { atomicOr(P.err, ERR_WATER); ok = false; }
+                    if (ok && mm2 > 20) { atomicOr(P.err, ERR_MELT); ok = false; }
+                    if (ok && P.densimod >= 2) { atomicOr(P.err, ERR_DENSI); ok = false; }
+                    if (ok) {
+                        int wn[3];
+                        const double mpb = pr_at(G, F.pr, F.NY, F.NXY, fx, fy, fz, wn) * 1e-5;
+                        const double mtk = M.k[i];
+                        double mnu = M.v[i];
+                        if (mnu <= 0 || timestep <= 0) {
+                            double e[7], sg[6], dis;
+                            eps_at(G, F, fx, fy, fz, wn, e, sg, &dis);
+                            float me = M.e[i], mft = M.ft[i];
+                            mnu = visc(P, mtk, mpb, mm2, inv2(e), 1.0, me, mft);
+                            if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); ok = false; }
+                            else { M.v[i] = (float)mnu; M.e[i] = me; M.ft[i] = mft; }
+                        }
+                        if (ok) {
+                            double mbb = 0, mro = RK(P, R_RO, mm2);
+                            if (P.densimod != 0) {   // dencalc1 (mark3mg.c:3006-3024)
+                                const double bb = RK(P, R_BB, mm2);
+                                mbb = bb / (1.0 - bb * (mtk - 298.15));
+                                mro = mro * (1.0 - bb * (mtk - 298.15)) * (1.0 + RK(P, R_AA, mm2) * (mpb - 1.0) * 1e-3);
+                            }
+                            phase_density(P, mm2, mtk, mpb, mro);
+                            const double mcp = RK(P, R_CP, mm2);
+                            const double mkt = (RK(P, R_KT, mm2) + RK(P, R_KF, mm2) / (mtk + 77.0)) * exp(RK(P, R_KP, mm2) * mpb);
+                            if (fy > P.vdeep && mnu > P.nudeep) mnu = P.nudeep;
+                            if (fy < 5e+4 && fx > G.xsize - 1e+4 && fz > 1.5e+5 && fz < 8.7e+5 && mnu > 1e+19) mnu = 1e+19;
+                            const int m10 = wn[0], m20 = wn[1], m30 = wn[2];
+                            const double dx = G.gx[m10 + 1] - G.gx[m10], dy = G.gy[m20 + 1] - G.gy[m20], dz = G.gz[m30 + 1] - G.gz[m30];
+                            double *st = my + lane * kStage;
+                            st[0] = 1.0 - fabs((G.gx[m10] - fx) / dx);
+                            st[1] = 1.0 - fabs((G.gx[m10 + 1] - fx) / dx);
+                            st[2] = 1.0 - fabs((G.gy[m20] - fy) / dy);
+                            st[3] = 1.0 - fabs((G.gy[m20 + 1] - fy) / dy);
+                            st[4] = 1.0 - fabs((G.gz[m30] - fz) / dz);
+                            st[5] = 1.0 - fabs((G.gz[m30 + 1] - fz) / dz);
+                            st[6] = vm == 0 ? mnu : vm == 1 ? log(mnu) : 1.0 / mnu;
+                            st[7] = mro;
+                            st[8] = mcp * mro;
+                            st[9] = mkt;
+                            st[10] = RK(P, R_HT, mm2);
+                            st[11] = mbb;
+                            st[12] = mtk;
+                            st[13] = M.rr[i];
+                        }
                     }
                 }
+                unsigned valid = __ballot_sync(0xffffffffu, ok);
+                __syncwarp();
+                // stage 2: lane (node, group) over the staged markers, in lane order
+                for (; valid; valid &= valid - 1) {
+                    const double *st = my + (__ffs(valid) - 1) * kStage;
+                    const double ddx = st[ix], ddy = st[2 + iy], ddz = st[4 + iz];
+                    const double swt = ddx * ddy * ddz;
+                    const double vnu = st[6];
+                    if (grp == 0) {
+                        if (swt > 0) { s0 += st[7] * swt; s1 += st[8] * swt; s2 += st[9] * swt; s3 += st[10] * swt; }
+                    } else if (grp == 1) {
+                        if (swt > 0) { s0 += st[11] * swt; s1 += st[12] * swt; s2 += st[13] * swt; s3 += swt; }
+                    } else if (grp == 2) {
+                        if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { s0 += vnu * swt; s1 += swt; }
+                        if (ix && iy && iz) {
+                            const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
+                            s2 += vnu * w1; s3 += w1;
+                        }
+                    } else {
+                        if (!iz && ddx > 0.5 && ddy > 0.5) {
+                            const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
+                            s0 += vnu * w1; s1 += w1;
+                        }
+                        if (!iy && ddx > 0.5 && ddz > 0.5) {
+                            const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
+                            s2 += vnu * w1; s3 += w1;
+                        }
+                        if (!ix && ddy > 0.5 && ddz > 0.5) {
+                            const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
+                            s4 += vnu * w1; s5 += w1;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            const int lb = ((lz + iz) * NBX + (lx + ix)) * NBY + (ly + iy);
+            double *a = sacc + lb;
+            if (grp == 0) { a[A_RO * NBOX] += s0; a[A_CP * NBOX] += s1; a[A_KT * NBOX] += s2; a[A_HT * NBOX] += s3; }
+            else if (grp == 1) { a[A_ET * NBOX] += s0; a[A_TK * NBOX] += s1; a[A_RR * NBOX] += s2; a[W_P * NBOX] += s3; }
+            else if (grp == 2) { a[A_NU * NBOX] += s0; a[W_NU * NBOX] += s1; a[A_XX * NBOX] += s2; a[W_XX * NBOX] += s3; }
+            else {
+                a[A_XY * NBOX] += s0; a[W_XY * NBOX] += s1; a[A_XZ * NBOX] += s2; a[W_XZ * NBOX] += s3;
+                a[A_YZ * NBOX] += s4; a[W_YZ * NBOX] += s5;
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
     // flush: nodes inside the tile box face belong to this tile only
     for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
         const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
@@ -672,56 +786,91 @@ __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, dou
     }
 }
 
-__global__ void __launch_bounds__(512) k_heat_mark_tile(Marks M, const int *off, Grid Gg, TkF T, TileGeo TG, double timestep,
-                                                        double heatdif, double zdeep, double tdeep, double *acc, long N)
+// One CTA per tile, one warp per cell (8 parity classes, as in k_r2n_cells): stage 1 updates
+// up to 32 markers of the cell (one per lane) and stages their node weights and subgrid
+// change; stage 2 sums them per node (lane = 2 * node + quantity) without atomics.
+constexpr int kHmStage = 9;   // wi[0..7], dtk1
+
+__global__ void __launch_bounds__(32 * kR2nWarps) k_heat_mark_cells(Marks M, const int *coff, Grid Gg, TkF T, TileGeo TG,
+                                                                    double timestep, double heatdif, double zdeep,
+                                                                    double tdeep, double *acc, long N)
 {
     extern __shared__ double sm[];
-    double *sw0 = sm, *sw1 = sm + NBOX, *shg = sm + 2 * NBOX;
+    double *sw0 = sm, *sw1 = sm + NBOX;
+    double *stg = sm + 2 * NBOX;
+    double *shg = stg + kR2nWarps * 32 * kHmStage;
     for (int q = threadIdx.x; q < 2 * NBOX; q += blockDim.x) sm[q] = 0;
     Grid G;
     load_grid(Gg, shg, G);
     const int tile = blockIdx.x;
     const int ty = tile % TG.nty, rest = tile / TG.nty, tx = rest % TG.ntx, tz = rest / TG.ntx;
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
-    for (int i = off[tile] + threadIdx.x; i < off[tile + 1]; i += blockDim.x) {
-        const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
-        double e[4], wi[11];
-        int wn[3];
-        long nodes[8];
-        tk_at(G, T, fx, fy, fz, e, wn, nodes, wi);
-        float mk = M.k[i];
-        if (mk <= 0) {
-            mk = (float)e[3];
-            if (fy > zdeep && mk < tdeep) mk = (float)tdeep;
-        }
-        if (heatdif != 0) {
-            double mkt = 0, rocp = 0, mtk = T.tk[nodes[0]];
-            for (int q = 0; q < 8; q++) {
-                mkt += T.kt[nodes[q]] * wi[q];
-                rocp += (double)__fmul_rn(T.ro[nodes[q]], T.cp[nodes[q]]) * wi[q];
-                mtk = fmax(mtk, (double)T.tk[nodes[q]]);
-            }
-            if ((wn[0] <= 0 || wn[0] >= G.nx - 2 || wn[1] <= 0 || wn[1] >= G.ny - 2 || wn[2] <= 0 || wn[2] >= G.nz - 2) &&
-                (mk + e[2] - e[3]) > mtk)
-                mk = (float)(mtk - e[2] + e[3]);
-            const double dtk = e[3] - (double)mk;
-            double dtk1 = -heatdif * mkt / rocp * 2.0 * (1.0 / wi[8] / wi[8] + 1.0 / wi[9] / wi[9] + 1.0 / wi[10] / wi[10]) * timestep;
-            if (dtk1 < -150.0) dtk1 = -150.0;
-            dtk1 = dtk * (1.0 - exp(dtk1));
-            mk = __fadd_rn(mk, (float)dtk1);
-            int q = 0;
-            for (int m3 = wn[2]; m3 <= wn[2] + 1; m3++)
-                for (int m1 = wn[0]; m1 <= wn[0] + 1; m1++)
-                    for (int m2 = wn[1]; m2 <= wn[1] + 1; m2++, q++) {
-                        const int lb = ((m3 - cz0) * NBX + (m1 - cx0)) * NBY + (m2 - cy0);
-                        atomicAdd(sw1 + lb, dtk1 * wi[q]);
-                        atomicAdd(sw0 + lb, wi[q]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *my = stg + warp * 32 * kHmStage;
+    const int nd = (lane >> 1) & 7, qty = lane & 1;
+    const int iz = nd >> 2, ix = (nd >> 1) & 1, iy = nd & 1;
+    for (int colour = 0; colour < 8; colour++) {
+        const int pz = colour >> 2, px = (colour >> 1) & 1, py = colour & 1;
+        for (int q = warp; q < CPT / 8; q += kR2nWarps) {
+            const int ly = 2 * (q % (TY / 2)) + py, r2 = q / (TY / 2);
+            const int lx = 2 * (r2 % (TX / 2)) + px, lz = 2 * (r2 / (TX / 2)) + pz;
+            const long cell = (long)tile * CPT + (lz * TX + lx) * TY + ly;
+            const int beg = coff[cell], end = coff[cell + 1];
+            if (beg == end) continue;   // uniform over the warp
+            double acc_w = 0;
+            for (int base = beg; base < end; base += 32) {
+                bool staged = false;
+                if (base + lane < end) {
+                    const int i = base + lane;
+                    const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
+                    double e[4], wi[11];
+                    int wn[3];
+                    long nodes[8];
+                    tk_at(G, T, fx, fy, fz, e, wn, nodes, wi);
+                    float mk = M.k[i];
+                    if (mk <= 0) {
+                        mk = (float)e[3];
+                        if (fy > zdeep && mk < tdeep) mk = (float)tdeep;
                     }
+                    if (heatdif != 0) {
+                        double mkt = 0, rocp = 0, mtk = T.tk[nodes[0]];
+                        for (int qq = 0; qq < 8; qq++) {
+                            mkt += T.kt[nodes[qq]] * wi[qq];
+                            rocp += (double)__fmul_rn(T.ro[nodes[qq]], T.cp[nodes[qq]]) * wi[qq];
+                            mtk = fmax(mtk, (double)T.tk[nodes[qq]]);
+                        }
+                        if ((wn[0] <= 0 || wn[0] >= G.nx - 2 || wn[1] <= 0 || wn[1] >= G.ny - 2 || wn[2] <= 0 || wn[2] >= G.nz - 2) &&
+                            (mk + e[2] - e[3]) > mtk)
+                            mk = (float)(mtk - e[2] + e[3]);
+                        const double dtk = e[3] - (double)mk;
+                        double dtk1 = -heatdif * mkt / rocp * 2.0 * (1.0 / wi[8] / wi[8] + 1.0 / wi[9] / wi[9] + 1.0 / wi[10] / wi[10]) * timestep;
+                        if (dtk1 < -150.0) dtk1 = -150.0;
+                        dtk1 = dtk * (1.0 - exp(dtk1));
+                        mk = __fadd_rn(mk, (float)dtk1);
+                        double *st = my + lane * kHmStage;
+                        for (int qq = 0; qq < 8; qq++) st[qq] = wi[qq];
+                        st[8] = dtk1;
+                        staged = true;
+                    }
+                    mk = __fadd_rn(mk, (float)(e[2] - e[3]));
+                    M.k[i] = mk;
+                }
+                unsigned valid = __ballot_sync(0xffffffffu, staged);
+                __syncwarp();
+                // wi[] is ordered z, x, y (tk_at loops m3, m1, m2): node index = (iz*2 + ix)*2 + iy = nd
+                for (; valid; valid &= valid - 1) {
+                    const double *st = my + (__ffs(valid) - 1) * kHmStage;
+                    acc_w += qty ? st[8] * st[nd] : st[nd];
+                }
+                __syncwarp();
+            }
+            if (lane < 16) {
+                const int lb = ((lz + iz) * NBX + (lx + ix)) * NBY + (ly + iy);
+                (qty ? sw1 : sw0)[lb] += acc_w;
+            }
         }
-        mk = __fadd_rn(mk, (float)(e[2] - e[3]));
-        M.k[i] = mk;
+        __syncthreads();
     }
-    __syncthreads();
     for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
         const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
         const int gxn = cx0 + lx, gyn = cy0 + ly, gzn = cz0 + lz;
@@ -886,6 +1035,8 @@ static Phys phys_of(i3g_ctx *c)
 }
 
 static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
+static size_t r2n_smem(i3g_ctx *c) { return sizeof(double) * (NACC * NBOX + kR2nWarps * 32 * kStage) + grid_smem(c); }
+static size_t heat_mark_smem(i3g_ctx *c) { return sizeof(double) * (2 * NBOX + kR2nWarps * 32 * kHmStage) + grid_smem(c); }
 
 int markers_alloc(i3g_ctx *c)
 {
@@ -900,9 +1051,13 @@ int markers_alloc(i3g_ctx *c)
     S->ntz = (int)((c->m.znumz - 1 + TZ - 1) / TZ);
     S->ntiles = S->ntx * S->nty * S->ntz;
     I3G_CUDA(cudaMalloc((void **)&S->key, sizeof(int) * (n > 0 ? n : 1)));
-    I3G_CUDA(cudaMalloc((void **)&S->cnt, sizeof(int) * (S->ntiles + 2)));
+    S->nbins = (long)S->ntiles * CPT + 2;
+    const long nchunks = (S->nbins + kScanChunk - 1) / kScanChunk;
+    I3G_CUDA(cudaMalloc((void **)&S->cnt, sizeof(int) * S->nbins));
+    I3G_CUDA(cudaMalloc((void **)&S->coff, sizeof(int) * S->nbins));
+    I3G_CUDA(cudaMalloc((void **)&S->cur, sizeof(int) * S->nbins));
     I3G_CUDA(cudaMalloc((void **)&S->off, sizeof(int) * (S->ntiles + 2)));
-    I3G_CUDA(cudaMalloc((void **)&S->cur, sizeof(int) * (S->ntiles + 2)));
+    I3G_CUDA(cudaMalloc((void **)&S->bsum, sizeof(int) * nchunks));
     I3G_CUDA(cudaMalloc((void **)&S->acc, sizeof(double) * NACC * N));
     I3G_CUDA(cudaMalloc((void **)&S->tk1, sizeof(float) * N));
     const int rn = c->m.rocknum;
@@ -936,8 +1091,8 @@ int markers_alloc(i3g_ctx *c)
         I3G_CUDA(cudaMemcpyAsync(S->tbc_c, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice, c->st));
         I3G_CUDA(cudaMemcpyAsync(S->tbc_k, tkk.data(), sizeof(double) * tkk.size(), cudaMemcpyHostToDevice, c->st));
     }
-    I3G_CUDA(cudaFuncSetAttribute(k_r2n_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * NACC * NBOX + grid_smem(c))));
+    I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
     I3G_CUDA(cudaStreamSynchronize(c->st));
     // upload the host markers
     return markers_upload(c, &c->m);
@@ -949,7 +1104,7 @@ void markers_free(i3g_ctx *c)
     if (!S) return;
     free_marks(S->a);
     free_marks(S->b);
-    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->acc); cudaFree(S->tk1);
+    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->coff); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->bsum); cudaFree(S->acc); cudaFree(S->tk1);
     cudaFree(S->rock); cudaFree(S->err);
     if (S->herr) cudaFreeHost(S->herr);
     cudaFree(S->tbc_node); cudaFree(S->tbc_p); cudaFree(S->tbc_c); cudaFree(S->tbc_k);
@@ -1034,9 +1189,14 @@ static int sort_markers(i3g_ctx *c)
     MarkerState *S = ms(c);
     const long n = S->n;
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
-    I3G_CUDA(cudaMemsetAsync(S->cnt, 0, sizeof(int) * (S->ntiles + 1), c->st));
+    const long nbins = S->nbins;
+    const unsigned nchunks = (unsigned)((nbins + kScanChunk - 1) / kScanChunk);
+    I3G_CUDA(cudaMemsetAsync(S->cnt, 0, sizeof(int) * nbins, c->st));
     LAUNCH(k_tile_key, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), T, S->key, S->cnt);
-    LAUNCH(k_scan, 1, 1024, 0, (const int *)S->cnt, S->off, S->cur, S->ntiles + 1);
+    LAUNCH(k_scan_part, nchunks, kScanT, 0, (const int *)S->cnt, nbins, S->bsum);
+    LAUNCH(k_scan_top, 1, kScanT, 0, S->bsum, (int)nchunks);
+    LAUNCH(k_scan_apply, nchunks, kScanT, 0, (const int *)S->cnt, nbins, (const int *)S->bsum, S->coff, S->cur);
+    LAUNCH(k_tile_off, nb(S->ntiles + 1), 256, 0, (const int *)S->coff, S->ntiles, S->off);
     LAUNCH(k_tile_scatter, nb(n), 256, 0, S->a, S->b, n, (const int *)S->key, S->cur);
     std::swap(S->a, S->b);
     S->sorted = true;
@@ -1058,7 +1218,7 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
     I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
     if (S->n)
-        LAUNCH(k_r2n_tile, S->ntiles, 512, sizeof(double) * NACC * NBOX + grid_smem(c), S->a, (const int *)S->off, grid_of(c),
+        LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff, grid_of(c),
                nodes_of(c), phys_of(c), T, timestep, S->acc, N);
     NodeOut O{c->lev[0].nu, c->nxx, c->nxy, c->nxz, c->nyz, c->ro, c->cp, c->kt, c->ht, c->et, c->tk, c->rr, S->tk1};
     LAUNCH(k_r2n_norm, nb(N), 256, 0, (const double *)S->acc, N, O, c->p.viscmod, c->p.nubeg, c->p.nuend);
@@ -1089,7 +1249,7 @@ int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const flo
     I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * 2 * N, c->st));
     TkF T{tk0, tk1, c->tk, tk2, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
     TileGeo TG{S->ntx, S->nty, S->ntz, S->ntiles};
-    LAUNCH(k_heat_mark_tile, S->ntiles, 512, sizeof(double) * 2 * NBOX + grid_smem(c), S->a, (const int *)S->off, grid_of(c),
+    LAUNCH(k_heat_mark_cells, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
            T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->acc, N);
     if (c->p.heatdif != 0) {
         LAUNCH(k_heat_mark_norm, nb(N), 256, 0, S->acc, N);
@@ -1113,7 +1273,7 @@ int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *
     for (int r = 0; r < reps; r++) {
         if (kind == 4) {
             I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
-            LAUNCH(k_r2n_tile, S->ntiles, 512, sizeof(double) * NACC * NBOX + grid_smem(c), S->a, (const int *)S->off,
+            LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff,
                    grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->acc, N);
         } else {
             LAUNCH(k_move, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), nodes_of(c), phys_of(c), 0.0);

@@ -229,13 +229,10 @@ __device__ __forceinline__ void crow(const View<T> &L, int i, int j, int k, long
 // One colour of one velocity component: thread t handles the row of colour `color` in the
 // y-pair (2*jh, 2*jh+1) of line (i,k), so a warp covers 64 consecutive y.
 template <typename T, int V>
-__global__ void __launch_bounds__(256) k_relax_vel(View<T> L, int color, T koef)
+__device__ __forceinline__ void relax_vel_at(const View<T> &L, long t, int color, T koef)
 {
     using A = Ar<T>;
     const int hy = (L.ny + 1) >> 1;
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long total = (long)hy * L.nx * L.nz;
-    if (t >= total) return;
     const int jh = (int)(t % hy);
     const long rest = t / hy;
     const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
@@ -249,14 +246,19 @@ __global__ void __launch_bounds__(256) k_relax_vel(View<T> L, int color, T koef)
     if (V == 3) { s = -L.f3[n]; d = zrow<T, false>(L, i, j, k, n, s); L.u3[n] = A::sub(L.u3[n], A::mul(A::div(s, d), koef)); }
 }
 
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_relax_vel(View<T> L, int color, T koef)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)((L.ny + 1) >> 1) * L.nx * L.nz) return;
+    relax_vel_at<T, V>(L, t, color, koef);
+}
+
 // All interior pressure rows: p -= (div v - f) * nd * p0koef (move3mg.c:3105-3116)
 template <typename T>
-__global__ void __launch_bounds__(256) k_relax_p(View<T> L, T koef)
+__device__ __forceinline__ void relax_p_at(const View<T> &L, long n, T koef)
 {
     using A = Ar<T>;
-    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long N = L.nxy * L.nz;
-    if (n >= N) return;
     const int j = (int)(n % L.ny);
     const long rest = n / L.ny;
     const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
@@ -266,15 +268,21 @@ __global__ void __launch_bounds__(256) k_relax_p(View<T> L, T koef)
     L.u0[n] = A::sub(L.u0[n], A::mul(A::mul(s, (T)L.nd[n]), koef));
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_relax_p(View<T> L, T koef)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.nxy * L.nz) return;
+    relax_p_at<T>(L, n, koef);
+}
+
 // Boundary rows of one component: x = c1 + k1*(c2 + k2*(... x_partner)) evaluated from the
 // innermost link outwards (the fixed point of bonderr rows, move3mg.c:1532-1579).
 template <typename T>
-__global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const int *depth,
-                           const double *cc, const double *kk, int use_c)
+__device__ __forceinline__ void bc_apply_at(T *u, int t, const int *node, const int *pnode, const int *depth,
+                                            const double *cc, const double *kk, int use_c)
 {
     using A = Ar<T>;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
     const int p = pnode[t];
     T val = p >= 0 ? u[p] : T(0);
     for (int d = depth[t] - 1; d >= 0; d--) {
@@ -284,15 +292,21 @@ __global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const
     u[node[t]] = val;
 }
 
+template <typename T>
+__global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const int *depth,
+                           const double *cc, const double *kk, int use_c)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    bc_apply_at<T>(u, t, node, pnode, depth, cc, kk, use_c);
+}
+
 // ------------------------------------------------------------------------------------
 // residual (gausmat4 residual pass, move3mg.c:3136-3157)
 // ------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual(View<T> L)
+__device__ __forceinline__ void residual_at(const View<T> &L, long n)
 {
-    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long N = L.nxy * L.nz;
-    if (n >= N) return;
     const int j = (int)(n % L.ny);
     const long rest = n / L.ny;
     const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
@@ -303,14 +317,20 @@ __global__ void __launch_bounds__(256) k_residual(View<T> L)
     if (row_exists(3, i, j, k, L.nx, L.ny, L.nz) && !(b & 8)) { T s = L.f3[n]; zrow<T, true>(L, i, j, k, n, s); L.r3[n] = s; }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual(View<T> L)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.nxy * L.nz) return;
+    residual_at<T>(L, n);
+}
+
 // residual of boundary rows with their original (unflattened) partner
 template <typename T>
-__global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const int *onode, const int *ocomp,
-                              const double *ok)
+__device__ __forceinline__ void bc_residual_at(const View<T> &L, int V, int t, const int *node, const int *onode,
+                                               const int *ocomp, const double *ok)
 {
     using A = Ar<T>;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
     T *u[4] = {L.u0, L.u1, L.u2, L.u3};
     T *f[4] = {L.f0, L.f1, L.f2, L.f3};
     T *r[4] = {L.r0, L.r1, L.r2, L.r3};
@@ -319,6 +339,15 @@ __global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const in
     s = A::sub(s, A::mul(T(1), u[V][nd]));
     if (onode[t] >= 0) s = A::sub(s, A::mul((T)(-ok[t]), u[ocomp[t]][onode[t]]));
     r[V][nd] = s;
+}
+
+template <typename T>
+__global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const int *onode, const int *ocomp,
+                              const double *ok)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    bc_residual_at<T>(L, V, t, node, onode, ocomp, ok);
 }
 
 // ------------------------------------------------------------------------------------
@@ -341,12 +370,10 @@ static TrView trview(const Transfer1D &t)
 // nd_fine/nd_coarse.  Contributions are summed in the fine lexicographic order of the
 // reference's scatter loop.  Coarse solution is zeroed.
 template <typename T, int V>
-__global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz)
+__device__ __forceinline__ void restrict_at(const View<T> &F, const View<T> &Cc, const TrView &tx, const TrView &ty,
+                                            const TrView &tz, long n)
 {
     using A = Ar<T>;
-    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long N = Cc.nxy * Cc.nz;
-    if (n >= N) return;
     const int j = (int)(n % Cc.ny);
     const long rest = n / Cc.ny;
     const int i = (int)(rest % Cc.nx), k = (int)(rest / Cc.nx);
@@ -380,14 +407,20 @@ __global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView 
     cf_[n] = ws != T(0) ? A::div(sum, ws) : sum;
 }
 
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Cc.nxy * Cc.nz) return;
+    restrict_at<T, V>(F, Cc, tx, ty, tz, n);
+}
+
 // vpprolong (move3mg.c:2748-3063): fine += sum_8 coarse * weight * koef
 template <typename T, int V>
-__global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz, T koef)
+__device__ __forceinline__ void prolong_at(const View<T> &F, const View<T> &Cc, const TrView &tx, const TrView &ty,
+                                           const TrView &tz, T koef, long n)
 {
     using A = Ar<T>;
-    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long N = F.nxy * F.nz;
-    if (n >= N) return;
     const int j = (int)(n % F.ny);
     const long rest = n / F.ny;
     const int i = (int)(rest % F.nx), k = (int)(rest / F.nx);
@@ -407,6 +440,148 @@ __global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView t
                 s = A::add(s, A::mul(A::mul(cu[m], swt), koef));
             }
     fu[n] = s;
+}
+
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz, T koef)
+{
+    long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= F.nxy * F.nz) return;
+    prolong_at<T, V>(F, Cc, tx, ty, tz, koef, n);
+}
+
+// ------------------------------------------------------------------------------------
+// coarse tail of a V-cycle in one thread block
+// ------------------------------------------------------------------------------------
+// On levels of a few thousand nodes every relaxation phase is a kernel of a few hundred
+// rows, so the V-cycle there is bound by kernel-to-kernel latency (11 dependent launches per
+// sweep, up to 64 sweeps per level).  The tail kernel runs the whole lower part of the
+// V-cycle -- down sweeps, residuals, restrictions, coarsest sweeps, prolongations and up
+// sweeps of the small levels -- in one block of 512 threads, with __syncthreads() where the
+// multi-kernel version has a kernel boundary.  Each phase applies the same per-row functions
+// to the same rows, and rows within a phase are independent, so results are bit-identical.
+// The small levels stay resident in L1/L2.
+constexpr int kTailMax = 6;
+constexpr int kTailThreads = 512;
+
+struct BcDev {
+    int n;
+    const int *node, *pnode, *depth, *onode, *ocomp;
+    const double *c, *k, *ok;
+};
+
+template <typename T>
+struct TailLevel {
+    View<T> v;
+    BcDev bc[4];
+    TrView tr[4][3];     // transfer to the next coarser level: [component][axis]
+    int down, up;        // sweeps on the way down (0: residual only) and on the way up
+};
+
+template <typename T>
+struct TailArgs {
+    int nl;
+    T v0, p0, kv, kp;
+    TailLevel<T> L[kTailMax];
+};
+
+template <typename T>
+__device__ __forceinline__ T *comp(const View<T> &L, int v)
+{
+    return v == 0 ? L.u0 : v == 1 ? L.u1 : v == 2 ? L.u2 : L.u3;
+}
+
+template <typename T>
+__device__ void tail_bc(const TailLevel<T> &TL, int v)
+{
+    const BcDev &B = TL.bc[v];
+    if (B.n == 0) return;   // uniform over the block
+    T *u = comp(TL.v, v);
+    for (int t = threadIdx.x; t < B.n; t += blockDim.x) bc_apply_at<T>(u, t, B.node, B.pnode, B.depth, B.c, B.k, 0);
+    __syncthreads();
+}
+
+template <typename T, int V>
+__device__ void tail_colours(const TailLevel<T> &TL, T v0)
+{
+    const View<T> &L = TL.v;
+    const long total = (long)((L.ny + 1) >> 1) * L.nx * L.nz;
+    for (int color = 0; color < 2; color++) {
+        for (long t = threadIdx.x; t < total; t += blockDim.x) relax_vel_at<T, V>(L, t, color, v0);
+        __syncthreads();
+    }
+    tail_bc<T>(TL, V);
+}
+
+template <typename T>
+__device__ void tail_smooth(const TailLevel<T> &TL, int nsweeps, T v0, T p0)
+{
+    const View<T> &L = TL.v;
+    const long N = L.nxy * L.nz;
+    for (int s = 0; s < nsweeps; s++) {
+        tail_colours<T, 1>(TL, v0);
+        tail_colours<T, 2>(TL, v0);
+        tail_colours<T, 3>(TL, v0);
+        for (long n = threadIdx.x; n < N; n += blockDim.x) relax_p_at<T>(L, n, p0);
+        __syncthreads();
+        tail_bc<T>(TL, 0);
+    }
+}
+
+template <typename T>
+__device__ void tail_residual(const TailLevel<T> &TL)
+{
+    const View<T> &L = TL.v;
+    const long N = L.nxy * L.nz;
+    for (long n = threadIdx.x; n < N; n += blockDim.x) residual_at<T>(L, n);
+    for (int v = 0; v < 4; v++) {
+        const BcDev &B = TL.bc[v];
+        for (int t = threadIdx.x; t < B.n; t += blockDim.x) bc_residual_at<T>(L, v, t, B.node, B.onode, B.ocomp, B.ok);
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void tail_restrict(const TailLevel<T> &F, const TailLevel<T> &C)
+{
+    const long N = C.v.nxy * C.v.nz;
+    for (long n = threadIdx.x; n < N; n += blockDim.x) {
+        restrict_at<T, 1>(F.v, C.v, F.tr[1][0], F.tr[1][1], F.tr[1][2], n);
+        restrict_at<T, 2>(F.v, C.v, F.tr[2][0], F.tr[2][1], F.tr[2][2], n);
+        restrict_at<T, 3>(F.v, C.v, F.tr[3][0], F.tr[3][1], F.tr[3][2], n);
+        restrict_at<T, 0>(F.v, C.v, F.tr[0][0], F.tr[0][1], F.tr[0][2], n);
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void tail_prolong(const TailLevel<T> &F, const TailLevel<T> &C, T kv, T kp)
+{
+    const long N = F.v.nxy * F.v.nz;
+    for (long n = threadIdx.x; n < N; n += blockDim.x) {
+        prolong_at<T, 1>(F.v, C.v, F.tr[1][0], F.tr[1][1], F.tr[1][2], kv, n);
+        prolong_at<T, 2>(F.v, C.v, F.tr[2][0], F.tr[2][1], F.tr[2][2], kv, n);
+        prolong_at<T, 3>(F.v, C.v, F.tr[3][0], F.tr[3][1], F.tr[3][2], kv, n);
+        prolong_at<T, 0>(F.v, C.v, F.tr[0][0], F.tr[0][1], F.tr[0][2], kp, n);
+    }
+    __syncthreads();
+}
+
+// Levels a.L[0..nl-1] (fine to coarse) of the V-cycle schedule of move3mg.c:2173-2213, from
+// the down sweeps of a.L[0] to its up sweeps.
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_constant__ TailArgs<T> a)
+{
+    for (int q = 0; q + 1 < a.nl; q++) {
+        if (a.L[q].down > 0) tail_smooth<T>(a.L[q], a.L[q].down, a.v0, a.p0);
+        tail_residual<T>(a.L[q]);
+        tail_restrict<T>(a.L[q], a.L[q + 1]);
+    }
+    for (int q = a.nl - 1; q > 0; q--) {
+        if (a.L[q].up > 0) tail_smooth<T>(a.L[q], a.L[q].up, a.v0, a.p0);
+        tail_prolong<T>(a.L[q - 1], a.L[q], a.kv, a.kp);
+    }
+    if (a.L[0].up > 0) tail_smooth<T>(a.L[0], a.L[0].up, a.v0, a.p0);
 }
 
 // ronurestrict (move3mg.c:2642-2741): FP32 accumulator as in nu[], FP64 weights
@@ -861,6 +1036,8 @@ static int build_bc(i3g_ctx *c)
 
 int stokes_alloc(i3g_ctx *c)
 {
+    // size limit of the one-block V-cycle tail (I3G_TAIL_NODES=0 turns it off)
+    if (const char *e = getenv("I3G_TAIL_NODES")) c->tail_nodes = atol(e);
     // level geometry (gridcheck, load3mg.c:1220-1282)
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
@@ -1097,19 +1274,57 @@ static void prolong_t(i3g_ctx *c, int l)
 #undef PRL
 }
 
-// V-cycle with the schedule of move3mg.c:2173-2213
+// First level of the one-block tail: the coarsest levels (>= 1) with at most tail_nodes nodes;
+// multinum + 1 when none qualifies.
+static int tail_start(const i3g_ctx *c, int multinum)
+{
+    int lc = multinum + 1;
+    for (int l = multinum; l >= 1 && l > multinum - kTailMax; l--) {
+        if (c->lev[l].n > c->tail_nodes) break;
+        lc = l;
+    }
+    return lc;
+}
+
+template <typename T>
+static void tail_launch(i3g_ctx *c, int lc, int multinum)
+{
+    TailArgs<T> a;
+    memset(&a, 0, sizeof a);
+    a.nl = multinum - lc + 1;
+    a.v0 = (T)c->p.v0koef; a.p0 = (T)c->p.p0koef; a.kv = (T)c->p.v1koef; a.kp = (T)c->p.p1koef;
+    for (int q = 0; q < a.nl; q++) {
+        Level &L = c->lev[lc + q];
+        TailLevel<T> &TL = a.L[q];
+        TL.v = view<T>(L, fields<T>(L));
+        for (int v = 0; v < 4; v++) {
+            const BcList &B = L.bcl[v];
+            TL.bc[v] = BcDev{B.n, B.node, B.pnode, B.depth, B.onode, B.ocomp, B.c, B.k, B.ok};
+            if (q + 1 < a.nl)
+                for (int ax = 0; ax < 3; ax++) TL.tr[v][ax] = trview(L.tr[ax][kStag[v][ax]]);
+        }
+        TL.down = c->p.multinnn[0][lc + q];
+        TL.up = c->p.multinnn[1][lc + q];
+    }
+    LAUNCH(k_vcycle_tail<T>, 1, kTailThreads, a);
+}
+
+// V-cycle with the schedule of move3mg.c:2173-2213; the small coarse levels run in the
+// one-block tail kernel.
 template <typename T>
 static void vcycle_t(i3g_ctx *c, int multinum, bool homogeneous)
 {
-    for (int l = 0; l < multinum; l++) {
+    const int lc = tail_start(c, multinum);
+    for (int l = 0; l < multinum && l < lc; l++) {
         const int n = c->p.multinnn[0][l];
         if (n > 0) smooth_t<T>(c, l, n, homogeneous, true);
         else residual_t<T>(c, l);
         restrict_t<T>(c, l + 1);
     }
-    for (int l = multinum; l > 0; l--) {
+    if (lc <= multinum) tail_launch<T>(c, lc, multinum);
+    for (int l = std::min(lc, multinum); l > 0; l--) {
         const int n = c->p.multinnn[1][l];
-        if (n > 0) smooth_t<T>(c, l, n, homogeneous, false);
+        if (n > 0 && l != lc) smooth_t<T>(c, l, n, homogeneous, false);
         prolong_t<T>(c, l);
     }
     if (c->p.multinnn[1][0] > 0) smooth_t<T>(c, 0, c->p.multinnn[1][0], homogeneous, false);
@@ -1395,8 +1610,7 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     bool conv = mom <= rtol && cont <= rtol;
     const double p0_save = c->p.p0koef, p1_save = c->p.p1koef;
     const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;
-    double prev = std::max(mom, cont);
-    int rises = 0;
+    double best = std::max(mom, cont);
     bool switched = false;
     while (!conv && cycles < maxc) {
         for (int i = 0; i < ncyc && cycles < maxc && !conv; i++) {
@@ -1408,18 +1622,18 @@ int stokes_solve(i3g_ctx *c, double *timestep)
             relres_read(c, &mom, &cont);
             if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
             conv = mom <= rtol && cont <= rtol;
-            // Safeguard: a residual that grows three cycles running switches to the file row's
-            // second relaxation set early (the reference switches after multstp iterations,
-            // move3mg.c:2585-2593).
+            // Safeguard: a residual 30x above the best one seen in this solve means the cycle
+            // diverges (transient rises of a convergent cycle stay far below that); switch to the
+            // file row's second relaxation set early (the reference switches after multstp
+            // iterations, move3mg.c:2585-2593).
             const double cur = std::max(mom, cont);
-            rises = cur > prev ? rises + 1 : 0;
-            prev = cur;
-            if (rises >= 3 && !switched && (c->p.p0koef != c->f.p0koef2 || c->p.p1koef != c->f.p1koef2)) {
+            best = std::min(best, cur);
+            if (cur > 30.0 * best && !switched && (c->p.p0koef != c->f.p0koef2 || c->p.p1koef != c->f.p1koef2)) {
                 c->p.p0koef = c->f.p0koef2;
                 c->p.p1koef = c->f.p1koef2;
                 multinum = std::min(c->f.multinum2 > 0 ? c->f.multinum2 : multinum, c->nlev - 1);
                 switched = true;
-                rises = 0;
+                best = cur;
             }
         }
         outer++;

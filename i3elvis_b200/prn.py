@@ -118,7 +118,8 @@ def read_prn(path) -> Prn:
 
 
 def write_prn(path, prn: Prn) -> None:
-    """Write ``prn`` in the exact byte layout of ``saver`` (``load3mg.c:898-1063``)."""
+    """Write ``prn`` in the exact byte layout of ``saver`` (``load3mg.c:898-1063``).  Node and
+    marker records are assembled and written in chunks of 2^20 records."""
     h = dict(prn.head)
     h["bondnum"] = int(prn.bond.shape[0])
     h["marknum"] = int(prn.marks["x"].shape[0])
@@ -126,25 +127,30 @@ def write_prn(path, prn: Prn) -> None:
     for name in _HEAD.names:
         head_rec[name] = h[name]
     nodenum = prn.nodenum
-    nrec = np.empty(nodenum, _NODE)
-    for f in NODE_FIELDS:
-        nrec[f] = prn.nodes[f]
-    mrec = np.empty(h["marknum"], _MARK)
-    for f in MARK_FIELDS:
-        mrec[f] = prn.marks[f]
-    mrec["t"] = prn.marks["t"]
     bond = np.ascontiguousarray(prn.bond, dtype=_BOND)
+    chunk = 1 << 20
     with open(path, "wb") as fh:
         fh.write(bytes([4, 8, 4, 8]))
         fh.write(head_rec.tobytes())
         for name in ROCK_FIELDS:
             fh.write(np.asarray(prn.rocks[name], "<f8").tobytes())
-        fh.write(nrec.tobytes())
+        for a in range(0, nodenum, chunk):
+            e = min(nodenum, a + chunk)
+            nrec = np.empty(e - a, _NODE)
+            for f in NODE_FIELDS:
+                nrec[f] = prn.nodes[f][a:e]
+            fh.write(nrec.tobytes())
         fh.write(np.asarray(prn.gx, "<f4").tobytes())
         fh.write(np.asarray(prn.gy, "<f4").tobytes())
         fh.write(np.asarray(prn.gz, "<f4").tobytes())
         fh.write(bond.tobytes())
-        fh.write(mrec.tobytes())
+        for a in range(0, h["marknum"], chunk):
+            e = min(h["marknum"], a + chunk)
+            mrec = np.empty(e - a, _MARK)
+            for f in MARK_FIELDS:
+                mrec[f] = prn.marks[f][a:e]
+            mrec["t"] = prn.marks["t"][a:e]
+            fh.write(mrec.tobytes())
 
 
 def empty_bond(n: int) -> np.ndarray:

@@ -153,6 +153,24 @@ def run_reference(workdir, *args, threads=1, timeout=3600):
     return None
 
 
+def run_reference_lines(workdir, *args, threads=1, timeout=3600):
+    """Like ``run_reference`` but returns every JSON line the harness printed, in order."""
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([REF, *map(str, args)], cwd=workdir, env=env, stdin=subprocess.DEVNULL,
+                       capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise OracleError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
+    out = []
+    for line in r.stdout.splitlines():
+        i = line.find("{\"")
+        if i >= 0:
+            try:
+                out.append(json.loads(line[i:]))
+            except json.JSONDecodeError:
+                continue
+    return out
+
+
 def read_csr(path):
     with open(path, "rb") as fh:
         nrows, nnz = np.frombuffer(fh.read(16), np.int64)

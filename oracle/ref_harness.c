@@ -228,6 +228,48 @@ static void dump_nodes(const char *prefix)
     fclose(f);
 }
 
+/* The initial-condition passes of in3mg.c:990-1031: nodes from markers, hydrostatic
+ * pressure (in3mg.c:1010-1021), nodes from markers again. */
+static void prepare_state(void)
+{
+    long m1, m3, m4, m2;
+    double ts = timestep;
+    timestep = 0;
+    ronurecalc();
+    if (GYKOEF > 0)
+        for (m3 = 1; m3 < znumz; m3++)
+            for (m1 = 1; m1 < xnumx; m1++) {
+                m4 = xynumxy * m3 + m1 * ynumy + 1;
+                pr[m4] = pinit;
+                for (m2 = 2; m2 < ynumy; m2++) {
+                    m4++;
+                    pr[m4] = pr[m4 - 1] + (gy[m2] - gy[m2 - 2]) / 2.0 * GYKOEF *
+                             (ro[m4 - 1] + ro[m4 - ynumy - 1] + ro[m4 - xynumxy - 1] + ro[m4 - xynumxy - ynumy - 1]) / 4.0;
+                }
+            }
+    ronurecalc();
+    gridcheck();
+    timestep = ts;
+}
+
+/* Level-0 velocities from sol0 into vx, vy, vz (move3mg.c:2246-2317) and the marker time
+ * step limit maxxystep / max|v| (move3mg.c:2608-2632). */
+static void velocities_and_cfl(void)
+{
+    long m1, m2, m3, n;
+    double vmax[3] = {0, 0, 0};
+    for (m3 = 0; m3 < znumz; m3++)
+        for (m1 = 0; m1 < xnumx; m1++)
+            for (m2 = 0; m2 < ynumy; m2++) {
+                n = m3 * xynumxy + m1 * ynumy + m2;
+                if (m2 < ynumy - 1 && m3 < znumz - 1) { vx[n] = (float)sol0[4 * n + 1]; if (fabs(vx[n]) > vmax[0]) vmax[0] = fabs(vx[n]); }
+                if (m1 < xnumx - 1 && m3 < znumz - 1) { vy[n] = (float)sol0[4 * n + 2]; if (fabs(vy[n]) > vmax[1]) vmax[1] = fabs(vy[n]); }
+                if (m1 < xnumx - 1 && m2 < ynumy - 1) { vz[n] = (float)sol0[4 * n + 3]; if (fabs(vz[n]) > vmax[2]) vmax[2] = fabs(vz[n]); }
+            }
+    for (int k = 0; k < 3; k++)
+        if (vmax[k] > 0 && timestep > maxxystep / vmax[k]) timestep = maxxystep / vmax[k];
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 2) { fprintf(stderr, "usage: ref_harness CMD ...\n"); return 2; }
@@ -237,22 +279,7 @@ int main(int argc, char **argv)
     file_params(0);
     timestep = maxtmstep;
     if (!strcmp(cmd, "prepare") && argc == 3) {
-        long m1, m3, m4, m2;
-        timestep = 0;
-        ronurecalc();
-        if (GYKOEF > 0)   /* in3mg.c:1010-1021 */
-            for (m3 = 1; m3 < znumz; m3++)
-                for (m1 = 1; m1 < xnumx; m1++) {
-                    m4 = xynumxy * m3 + m1 * ynumy + 1;
-                    pr[m4] = pinit;
-                    for (m2 = 2; m2 < ynumy; m2++) {
-                        m4++;
-                        pr[m4] = pr[m4 - 1] + (gy[m2] - gy[m2 - 2]) / 2.0 * GYKOEF *
-                                 (ro[m4 - 1] + ro[m4 - ynumy - 1] + ro[m4 - xynumxy - 1] + ro[m4 - xynumxy - ynumy - 1]) / 4.0;
-                    }
-                }
-        ronurecalc();
-        gridcheck();
+        prepare_state();
         snprintf(fl1out, sizeof fl1out, "%s", argv[2]);
         saver(0, 0);
         return 0;
@@ -377,24 +404,40 @@ int main(int argc, char **argv)
         dump_nodes(argv[2]);
         return 0;
     }
-    if (!strcmp(cmd, "sample") && argc == 3) {
-        /* bounded timing sample of one time step: the reference's set-up and one V-cycle of
-         * vpiterate (move3mg.c:1948-2223), titerate, movemark and ronurecalc, wall clock */
+    if (!strcmp(cmd, "sample") && argc >= 3) {
+        /* Bounded timing sample of time steps: SAMPLE NCYC [REPS [PREP]].  Optionally the
+         * initial-condition passes first (PREP=1, timed apart); then REPS times: the reference's
+         * vpiterate set-up (ronurestrict and row assembly, move3mg.c:1948-2159) and NCYC V-cycles,
+         * the velocities and CFL time step from that iterate, titerate, movemark and ronurecalc.
+         * Wall clock, one JSON line per repetition. */
         int ncyc = atoi(argv[2]);
-        double t0 = omp_get_wtime();
-        stokes_assemble();
-        double t1 = omp_get_wtime();
-        for (int i = 0; i < ncyc; i++) vcycle();
-        double t2 = omp_get_wtime();
-        if (tempmod) titerate(0);
-        double t3 = omp_get_wtime();
-        if (markmod) movemark();
-        double t4 = omp_get_wtime();
-        if (gridmod) ronurecalc();
-        double t5 = omp_get_wtime();
-        printf("{\"assemble_s\": %.4f, \"vcycle_s\": %.4f, \"ncyc\": %d, \"heat_s\": %.4f, \"move_s\": %.4f, "
-               "\"r2n_s\": %.4f, \"threads\": %d}\n", t1 - t0, (t2 - t1) / (ncyc > 0 ? ncyc : 1), ncyc, t3 - t2,
-               t4 - t3, t5 - t4, omp_get_max_threads());
+        int reps = argc >= 4 ? atoi(argv[3]) : 1;
+        double tp = 0;
+        if (argc >= 5 && atoi(argv[4])) {
+            double a = omp_get_wtime();
+            prepare_state();
+            tp = omp_get_wtime() - a;
+        }
+        for (int r = 0; r < reps; r++) {
+            timestep = maxtmstep;
+            double t0 = omp_get_wtime();
+            stokes_assemble();
+            double t1 = omp_get_wtime();
+            for (int i = 0; i < ncyc; i++) vcycle();
+            double t2 = omp_get_wtime();
+            velocities_and_cfl();
+            if (tempmod) titerate(0);
+            double t3 = omp_get_wtime();
+            if (markmod) movemark();
+            double t4 = omp_get_wtime();
+            if (gridmod) ronurecalc();
+            double t5 = omp_get_wtime();
+            printf("{\"rep\": %d, \"assemble_s\": %.4f, \"vcycle_s\": %.4f, \"ncyc\": %d, \"heat_s\": %.4f, "
+                   "\"move_s\": %.4f, \"r2n_s\": %.4f, \"prepare_s\": %.4f, \"timestep\": %.6e, \"threads\": %d}\n",
+                   r, t1 - t0, (t2 - t1) / (ncyc > 0 ? ncyc : 1), ncyc, t3 - t2, t4 - t3, t5 - t4, tp, timestep,
+                   omp_get_max_threads());
+            fflush(stdout);
+        }
         return 0;
     }
     if (!strcmp(cmd, "step") && argc == 3) {

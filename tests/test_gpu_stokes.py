@@ -72,8 +72,12 @@ def test_residual_smooth_transfer_bit_exact(name):
         assert np.array_equal(g.get(abi.A_SOL, l - 1, 4 * sizes[l - 1]), o.get(abi.A_SOL, l - 1, 4 * sizes[l - 1])), ("prolong", l)
 
 
+@pytest.mark.parametrize("tail", ["12000", "2000", "0"])
 @pytest.mark.parametrize("name", ["sphere13", "sphere17"])
-def test_vcycles_bit_exact(name):
+def test_vcycles_bit_exact(name, tail, monkeypatch):
+    """V-cycles equal the oracle's bit for bit, with the small levels in the one-block tail
+    kernel (default) and with one kernel per phase on every level (I3G_TAIL_NODES=0)."""
+    monkeypatch.setenv("I3G_TAIL_NODES", tail)
     p, mode, fx, g, o = pair(name)
     g.call("i3g_stokes_setup")
     o.call("orc_stokes_setup")

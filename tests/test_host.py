@@ -89,7 +89,10 @@ def test_prn_reader_rejects_truncated_file(tmp_path):
 
 
 def _rundir(path, name, steps):
-    p, mode = cases.build(name)
+    """A run directory holding a prepared model (node fields from the reference's marker->node
+    pass), like the .prn files the reference's initial-condition program writes."""
+    from conftest import golden
+    p, mode, _ = golden(name)
     mode.files[0].cyc0max = steps
     mode.infile = "in0.prn"
     P.write_prn(os.path.join(path, "in0.prn"), p)
