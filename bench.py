@@ -74,6 +74,26 @@ def build_case(name, seed_offset=0, sweeps=None):
     return prn, mode
 
 
+def host_threads():
+    """CPU threads this process may use: its affinity set, capped by a cgroup CPU quota."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as fh:
+            quota, period = fh.read().split()[:2]
+        if quota != "max":
+            n = max(1, min(n, int(int(quota) / int(period))))
+    except (OSError, ValueError):
+        pass
+    return n
+
+
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -126,16 +146,22 @@ class Clocks:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
 
 
+# titerate (heat3mg.c:463-560) repeats its iteration block until heatsum <= HEATMIN, which its
+# racy multi-threaded relaxation may never reach; the reference samples stop it after this many
+# blocks (the count used is in each sample's "heat_blocks")
+REF_HEAT_CAP = 20
+
+
 def _est(r, ncyc):
     """Step estimate from one sample: set-up + ncyc V-cycles + heat + advection + marker->node."""
     return r["assemble_s"] + ncyc * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
 
 
-def reference_sample(prn, mode, ncyc_for_1e8, threads):
+def reference_sample(prn, mode, ncyc_for_1e8, threads, dt=0.0):
     """Time the reference's own functions on this workload (bounded sample, all host threads):
-    vpiterate set-up + one V-cycle, titerate, movemark, ronurecalc on the prepared model.  The
-    step estimate scales the V-cycle by the number of V-cycles this multigrid needs for
-    relative residual 1e-8."""
+    its initial-condition passes, then two steps of vpiterate set-up + one V-cycle, titerate,
+    movemark and ronurecalc; the second (warm) step is the sample.  The step estimate scales
+    the V-cycle by the number of V-cycles this multigrid needs for relative residual 1e-8."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.have_reference():
@@ -144,7 +170,11 @@ def reference_sample(prn, mode, ncyc_for_1e8, threads):
         write_prn(os.path.join(d, "in0.prn"), prn)
         config.write_mode(os.path.join(d, "mode.t3c"), mode)
         config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-        rs = O.run_reference_lines(d, "sample", 1, 1, 0, threads=threads, timeout=1200)
+        rs = O.run_reference_lines(d, "sample", 1, 2, 1, REF_HEAT_CAP, repr(float(dt)), threads=threads, timeout=600)
+        if rs and not rs[-1].get("vmax", 1.0) > 0 and threads > 8:
+            # the reference's multi-threaded V-cycle left no finite velocity (seen with 16 threads
+            # at 129^3); time it again with 8 threads
+            rs = O.run_reference_lines(d, "sample", 1, 2, 1, REF_HEAT_CAP, repr(float(dt)), threads=8, timeout=600)
     if not rs:
         return None
     return _est(rs[-1], ncyc_for_1e8), rs[-1]
@@ -155,7 +185,7 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     prn, mode = build_case(args.workload, sweeps=args.sweeps)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -169,13 +199,19 @@ def run_reference_arm(args):
         config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
         # one process: the reference's initial-condition passes (in3mg.c:990-1031), then
         # warmup + timed steps, each a sample of the step (see the harness's sample command)
-        rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, threads=threads, timeout=3000)
+        rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, REF_HEAT_CAP, repr(args.ref_dt),
+                                   threads=threads, timeout=3000)
+        if rs and not rs[-1].get("vmax", 1.0) > 0 and threads > 8:
+            threads = 8   # see reference_sample
+            rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, REF_HEAT_CAP, repr(args.ref_dt),
+                                       threads=threads, timeout=3000)
     timed = rs[args.warmup:]
     times = [_est(r, ncyc) for r in timed]
     detail = timed[-1] if timed else None
     v = float(np.mean(times))
     sample = (f"per step: reference vpiterate set-up + 1 V-cycle (x {ncyc} V-cycles, the count this multigrid "
-              f"needs for relative residual 1e-8), velocities and CFL step from that iterate, titerate, movemark, "
+              f"needs for relative residual 1e-8), time step {args.ref_dt:.4g} s (the GPU run's CFL step), titerate (at most "
+              f"{REF_HEAT_CAP} iteration blocks), movemark, "
               f"ronurecalc on the full {args.workload} model, {threads} OpenMP threads, one process after the "
               f"reference's initial-condition passes; last timed step {json.dumps(detail)}")
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s/step", "n_gpus": args.gpus,
@@ -197,10 +233,14 @@ def main():
     ap.add_argument("--workload", default="incl129", choices=tuple(WORKLOADS))
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--sweeps", default=None, help="relaxation sweeps per level, 'down,../up,..'")
+    ap.add_argument("--krylov", type=int, default=16,
+                    help="mixed precision: FGMRES restart length around the FP32 V-cycle (0: plain defect correction)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # V-cycles per step that the reference-arm estimate charges: the count the FP64 multigrid
     # takes to relative residual 1e-8 on incl129 on the GPU (21-22 per step after warm-up)
     ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("I3G_REF_CYCLES", "21")))
+    # time step of the reference-arm samples: the CFL step the GPU run takes on incl129 (s)
+    ap.add_argument("--ref-dt", type=float, default=3.5635e10)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -217,11 +257,14 @@ def main():
 
     prn, mode = build_case(args.workload, seed_offset=rank, sweeps=args.sweeps)
     prec = 1 if args.precision == "mixed" else 0
-    par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec)
+    krylov = args.krylov if prec == 1 else 0
+    par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec, krylov=krylov)
     buf = abi.ModelBuffers(prn, pinned=True)
     ctx = lib.Context(buf, par, abi.make_file_params(mode.files[0]))
     f = mode.files[0]
+    log("model built and uploaded")
     runtime.prepare(ctx)
+    log("prepared")
     cycles = []
     for i in range(args.warmup):
         runtime.time_step(ctx, mode, f, i)
@@ -232,6 +275,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    log(f"warm-up done, V-cycles {cycles}")
     clocks = Clocks(local)
     l0 = ctx.stats()["kernel_launches"]
     barrier()
@@ -253,6 +297,7 @@ def main():
     ms_max = float(t.item())
     value = ms_max / 1e3 / (args.steps * world)
 
+    log(f"timed steps done: {ms_max / args.steps:.1f} ms/step")
     # end to end through the C ABI with host buffers: full state up, step, full state down
     e2e_steps = max(1, min(args.steps, 2))
     n, m = prn.nodenum, prn.marknum
@@ -290,8 +335,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32-in-f64", "data": "synthetic",
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "precision": args.precision,
-                   "stokes_rtol": args.rtol, "sweeps": [list(mode.multinnn[0]), list(mode.multinnn[1])],
+                   "stokes_rtol": args.rtol, "krylov": krylov, "sweeps": [list(mode.multinnn[0]), list(mode.multinnn[1])],
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "timestep_s": float(np.median([lg["timestep"] for lg in logs])),
         "stokes_cycles": cycles[args.warmup:], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in
                                                            ("ms_stokes", "ms_heat", "ms_move", "ms_r2n")},
         "gpu_launches": int(launches),
@@ -302,18 +348,22 @@ def main():
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ncyc = int(np.median(cycles)) if cycles else 40
-        ctx.download(abi.SYNC_ALL)
+        ncyc = int(np.median(cycles[args.warmup:])) if cycles[args.warmup:] else 21
         try:
-            r = reference_sample(buf.to_prn(), mode, ncyc, os.cpu_count() or 1)
+            log("cpu baseline: reference sample")
+            dts = [lg["timestep"] for lg in logs if lg.get("timestep")]
+            r = reference_sample(prn, mode, ncyc, host_threads(), float(np.median(dts)) if dts else 0.0)
+            log("cpu baseline done")
         except Exception as e:  # the CPU baseline is reported, never required
             r = None
             out["cpu_baseline_error"] = str(e)[:300]
         if r:
             est, detail = r
             out["cpu_baseline"] = {"value": est, "unit": "s/step", "cores": detail["threads"], "kind": "reference",
-                                   "sample": f"reference set-up + 1 V-cycle x {ncyc} V-cycles (this run's count to 1e-8), "
-                                             f"titerate, movemark, ronurecalc on the same model; phases {json.dumps(detail)}"}
+                                   "sample": f"one warm step of the reference on the same model after its initial-condition "
+                                             f"passes: set-up + 1 V-cycle x {ncyc} V-cycles (this run's count to 1e-8), this run's time "
+                                             f"step, titerate (at most {REF_HEAT_CAP} iteration blocks), movemark, "
+                                             f"ronurecalc; {json.dumps(detail)}"}
     ctx.close()
     if rank == 0:
         print(json.dumps(out))

@@ -68,6 +68,7 @@ class Params(C.Structure):
         ("timebeg", C.c_double), ("timeend", C.c_double), ("tempend", C.c_double),
         ("stokes_rtol", C.c_double), ("stokes_maxcyc", C.c_int32), ("heat_rtol", C.c_double),
         ("heat_maxcyc", C.c_int32), ("precision", C.c_int32), ("warm_start", C.c_int32),
+        ("krylov", C.c_int32),
     ]
 
 
@@ -199,6 +200,7 @@ def make_params(mode: Mode, **solver) -> Params:
     p.heat_maxcyc = solver.get("heat_maxcyc", 2000)
     p.precision = solver.get("precision", 0)
     p.warm_start = solver.get("warm_start", 1)
+    p.krylov = solver.get("krylov", 0)
     return p
 
 

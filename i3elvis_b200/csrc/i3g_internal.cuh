@@ -119,6 +119,7 @@ struct i3g_ctx {
     long sg_nodes = 0;
     double *dscale = nullptr;                   // device scale factors of the FP32 correction solve
     long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
+    void *kry = nullptr;       // FGMRES state of the mixed-precision Stokes solve
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state
 };

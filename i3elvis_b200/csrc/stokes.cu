@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 #include "i3g_internal.cuh"
 
@@ -38,6 +39,16 @@ struct Ar<float> {
     static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
 };
+
+// Programmatic dependent launch: every kernel of this file is launched with programmatic
+// stream serialization, so the next kernel is scheduled while this one runs; it waits for its
+// predecessor's completion (and memory) before touching any data, then lets its own successor
+// launch.  On the latency-bound coarse levels this hides most of the launch gap.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // Level view passed by value to kernels.
 template <typename T>
@@ -247,8 +258,9 @@ __device__ __forceinline__ void relax_vel_at(const View<T> &L, long t, int color
 }
 
 template <typename T, int V>
-__global__ void __launch_bounds__(256) k_relax_vel(View<T> L, int color, T koef)
+__global__ void __launch_bounds__(256, 4) k_relax_vel(View<T> L, int color, T koef)
 {
+    pdl_enter();
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)((L.ny + 1) >> 1) * L.nx * L.nz) return;
     relax_vel_at<T, V>(L, t, color, koef);
@@ -269,8 +281,9 @@ __device__ __forceinline__ void relax_p_at(const View<T> &L, long n, T koef)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_relax_p(View<T> L, T koef)
+__global__ void __launch_bounds__(256, 4) k_relax_p(View<T> L, T koef)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.nxy * L.nz) return;
     relax_p_at<T>(L, n, koef);
@@ -296,6 +309,7 @@ template <typename T>
 __global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const int *depth,
                            const double *cc, const double *kk, int use_c)
 {
+    pdl_enter();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     bc_apply_at<T>(u, t, node, pnode, depth, cc, kk, use_c);
@@ -320,6 +334,7 @@ __device__ __forceinline__ void residual_at(const View<T> &L, long n)
 template <typename T>
 __global__ void __launch_bounds__(256) k_residual(View<T> L)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.nxy * L.nz) return;
     residual_at<T>(L, n);
@@ -345,6 +360,7 @@ template <typename T>
 __global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const int *onode, const int *ocomp,
                               const double *ok)
 {
+    pdl_enter();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     bc_residual_at<T>(L, V, t, node, onode, ocomp, ok);
@@ -410,6 +426,7 @@ __device__ __forceinline__ void restrict_at(const View<T> &F, const View<T> &Cc,
 template <typename T, int V>
 __global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Cc.nxy * Cc.nz) return;
     restrict_at<T, V>(F, Cc, tx, ty, tz, n);
@@ -445,6 +462,7 @@ __device__ __forceinline__ void prolong_at(const View<T> &F, const View<T> &Cc, 
 template <typename T, int V>
 __global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView tx, TrView ty, TrView tz, T koef)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= F.nxy * F.nz) return;
     prolong_at<T, V>(F, Cc, tx, ty, tz, koef, n);
@@ -572,6 +590,7 @@ __device__ void tail_prolong(const TailLevel<T> &F, const TailLevel<T> &C, T kv,
 template <typename T>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_constant__ TailArgs<T> a)
 {
+    pdl_enter();
     for (int q = 0; q + 1 < a.nl; q++) {
         if (a.L[q].down > 0) tail_smooth<T>(a.L[q], a.L[q].down, a.v0, a.p0);
         tail_residual<T>(a.L[q]);
@@ -588,6 +607,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_co
 __global__ void k_nu_restrict(const float *nuf, int fnx, int fny, int fnz, float *nuc, int cnx, int cny, int cnz,
                               TrView tx, TrView ty, TrView tz, int viscmod)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long N = (long)cnx * cny * cnz;
     if (n >= N) return;
@@ -665,6 +685,7 @@ __device__ __forceinline__ double clampnu(double n, double b, double e)
 
 __global__ void k_eta(EtaArgs a)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long NY = a.ny, NXY = (long)a.nx * a.ny, N = NXY * a.nz;
     if (n >= N) return;
@@ -704,6 +725,7 @@ __global__ void k_eta(EtaArgs a)
 __global__ void k_eta_f32(long n, const double *ec, const double *exy, const double *exz, const double *eyz,
                           const float *nd, float *fc, float *fxy, float *fxz, float *fyz, float *fnd, double inv_ref)
 {
+    pdl_enter();
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     fc[t] = (float)(ec[t] * inv_ref);
@@ -716,6 +738,7 @@ __global__ void k_eta_f32(long n, const double *ec, const double *exy, const dou
 // level-0 right-hand side (move3mg.c:751, 942, 1140) and boundary constants
 __global__ void k_rhs0(View<double> L, const float *ro, double gx, double gy, double gz)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long NY = L.ny, NXY = L.nxy, N = NXY * L.nz;
     if (n >= N) return;
@@ -741,6 +764,7 @@ __global__ void k_rhs0(View<double> L, const float *ro, double gx, double gy, do
 
 __global__ void k_bc_rhs(double *f, int n, const int *node, const double *oc)
 {
+    pdl_enter();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) f[node[t]] = oc[t];
 }
@@ -748,6 +772,7 @@ __global__ void k_bc_rhs(double *f, int n, const int *node, const double *oc)
 // load the current v,P into the level-0 solution (move3mg.c:1969-2019)
 __global__ void k_load_sol(View<double> L, const double *pr, const float *vx, const float *vy, const float *vz)
 {
+    pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long NY = L.ny, N = L.nxy * L.nz;
     if (n >= N) return;
@@ -775,6 +800,7 @@ __device__ __forceinline__ double warp_sum(double v)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_relres_part(View<T> L, double *part)
 {
+    pdl_enter();
     __shared__ double sh[kRedQ][kRedThreads / 32];
     double q[kRedQ] = {0, 0, 0, 0};
     const long N = L.nxy * L.nz;
@@ -814,6 +840,7 @@ __global__ void __launch_bounds__(kRedThreads) k_relres_part(View<T> L, double *
 
 __global__ void k_red_final(const double *part, int nblk, int nq, double *out)
 {
+    pdl_enter();
     // one warp per quantity, fixed order
     const int qi = threadIdx.x >> 5, ln = threadIdx.x & 31;
     if (qi >= nq) return;
@@ -1113,9 +1140,12 @@ int stokes_alloc(i3g_ctx *c)
     return 0;
 }
 
+static void kry_free(i3g_ctx *c);
+
 void stokes_free(i3g_ctx *c)
 {
     stokes_graph_free(c);
+    kry_free(c);
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
         delete[] L.gx; delete[] L.gy; delete[] L.gz;
@@ -1146,9 +1176,27 @@ void stokes_free(i3g_ctx *c)
     c->hred = nullptr;
 }
 
+static bool g_pdl = getenv("I3G_PDL") == nullptr || atoi(getenv("I3G_PDL")) != 0;
+
+template <typename... KArgs, typename... Args>
+static void launch_pdl(cudaStream_t st, void (*kern)(KArgs...), dim3 grid, dim3 block, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 #define LAUNCH(kern, grid, block, ...)                                                     \
     do {                                                                                   \
-        kern<<<(grid), (block), 0, c->st>>>(__VA_ARGS__);                                  \
+        launch_pdl(c->st, kern, dim3(grid), dim3(block), __VA_ARGS__);                     \
         c->launches++;                                                                     \
     } while (0)
 
@@ -1370,6 +1418,7 @@ int stokes_relres(i3g_ctx *c, double *mom, double *cont)
 // ------------------------------------------------------------------------------------
 __global__ void k_max_abs(const double *a, long n, double *part)
 {
+    pdl_enter();
     __shared__ double sh[8];
     double m = 0;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) m = fmax(m, fabs(a[t]));
@@ -1388,6 +1437,7 @@ __global__ void k_max_abs(const double *a, long n, double *part)
 // scale = {momentum rhs factor, continuity rhs factor, sp, sv}
 __global__ void k_scale(const double *part, int nparts, double h, double er, double *scale)
 {
+    pdl_enter();
     __shared__ double sh[32];
     double m = 0;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) m = fmax(m, part[i]);
@@ -1410,6 +1460,7 @@ __global__ void k_to_f32(long n, const double *r0, const double *r1, const doubl
                          float *f0, float *f1, float *f2, float *f3, float *u0, float *u1, float *u2, float *u3,
                          const uint8_t *bc, const double *scale)
 {
+    pdl_enter();
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const double sm = scale[0], sc = scale[1];
@@ -1424,6 +1475,7 @@ __global__ void k_to_f32(long n, const double *r0, const double *r1, const doubl
 __global__ void k_add_correction(long n, double *x0, double *x1, double *x2, double *x3, const float *e0,
                                  const float *e1, const float *e2, const float *e3, const double *scale)
 {
+    pdl_enter();
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const double sp = scale[2], sv = scale[3];
@@ -1438,6 +1490,7 @@ __global__ void k_add_correction(long n, double *x0, double *x1, double *x2, dou
 // ------------------------------------------------------------------------------------
 __global__ void k_copy_back(View<double> L, long pin, double pinit, double *pr, float *vx, float *vy, float *vz, double *part)
 {
+    pdl_enter();
     __shared__ double sh[4][8];
     double m[4] = {0, 0, 0, -1e300};
     const long N = L.nxy * L.nz;
@@ -1470,6 +1523,7 @@ __global__ void k_eps_sig(int nx, int ny, int nz, const float *vx, const float *
                           const double *icx, const double *isx, const double *icy, const double *isy,
                           const double *icz, const double *isz, float **eps, float **sig)
 {
+    pdl_enter();
     const long NY = ny, NXY = (long)nx * ny, N = NXY * nz;
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
@@ -1585,6 +1639,336 @@ void stokes_graph_free(i3g_ctx *c)
     c->dscale = nullptr;
 }
 
+// ------------------------------------------------------------------------------------
+// FGMRES acceleration of the mixed-precision correction solve
+// ------------------------------------------------------------------------------------
+// With krylov = m > 0 the FP64 defect correction is restarted FGMRES(m) (Saad 1993, flexible
+// right preconditioning) whose preconditioner is the FP32 V-cycle on the scaled correction
+// problem.  The Krylov vectors live in a row-scaled residual space, D r with D = 1/||b_mom||
+// on velocity rows and h / (sqrt(#continuity rows) RMS(v)) on pressure rows, so that the
+// minimised norm ||D r||^2 = mom^2 + cont^2 matches the stopping test.  Each Arnoldi step (the
+// V-cycle, the FP64 operator and classical Gram-Schmidt with one re-orthogonalisation) is one
+// CUDA graph per step index; the host applies the Givens rotations between steps.
+constexpr int kKryMax = 16;
+constexpr int kKryNq = kKryMax + 2;
+
+struct KrylovState {
+    int m = 0;
+    long N = 0;
+    double *V = nullptr;     // m+1 basis vectors, vector j component v at V + (4j + v) N
+    double *Z = nullptr;     // m preconditioned directions, same layout
+    double *W = nullptr;     // work vector (4N)
+    double *F0 = nullptr;    // zero right-hand side (4N)
+    double *part = nullptr;  // partial dot products [blocks][kKryNq]
+    double *hdev = nullptr;  // [3][kKryNq]: first and second projection, squared norm; then 2 weights
+    double *hhost = nullptr; // pinned mirror of hdev
+    cudaGraphExec_t g[kKryMax] = {};
+    int g_multinum = -1;
+    double g_p0 = 0, g_p1 = 0, g_v0 = 0, g_v1 = 0;
+};
+
+static KrylovState *kry(i3g_ctx *c) { return (KrylovState *)c->kry; }
+
+// d[0] = velocity-row weight, d[1] = pressure-row weight (device, so that the captured steps
+// stay valid when the weights change between restarts)
+__global__ void k_kr_from_r(long N, const double *r0, const double *r1, const double *r2, const double *r3, double *v,
+                            const double *d)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const double dv = d[0], dp = d[1];
+    v[t] = dp * r0[t]; v[N + t] = dv * r1[t]; v[2 * N + t] = dv * r2[t]; v[3 * N + t] = dv * r3[t];
+}
+
+__global__ void k_kr_to_r(long N, const double *v, double *r0, double *r1, double *r2, double *r3, const double *d)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const double dv = d[0], dp = d[1];
+    r0[t] = v[t] / dp; r1[t] = v[N + t] / dv; r2[t] = v[2 * N + t] / dv; r3[t] = v[3 * N + t] / dv;
+}
+
+// z = scaled FP32 correction (the FP64 image of the V-cycle's result)
+__global__ void k_kr_store(long N, double *z, const float *e0, const float *e1, const float *e2, const float *e3,
+                           const double *scale)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const double sp = scale[2], sv = scale[3];
+    z[t] = sp * (double)e0[t]; z[N + t] = sv * (double)e1[t]; z[2 * N + t] = sv * (double)e2[t]; z[3 * N + t] = sv * (double)e3[t];
+}
+
+// w = -D w  (the residual kernels leave -A z in w)
+__global__ void k_kr_negscale(long N, double *w, const double *d)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const double dv = d[0], dp = d[1];
+    w[t] *= -dp; w[N + t] *= -dv; w[2 * N + t] *= -dv; w[3 * N + t] *= -dv;
+}
+
+// partial sums of w . v_i (i < nv) and, in slot nv, w . w
+__global__ void __launch_bounds__(256) k_kr_dots(const double *w, const double *V, int nv, long n4, double *part)
+{
+    pdl_enter();
+    __shared__ double sh[kKryNq][8];
+    double q[kKryNq], qq = 0;
+#pragma unroll
+    for (int i = 0; i < kKryNq; i++) q[i] = 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += (long)gridDim.x * blockDim.x) {
+        const double x = w[t];
+#pragma unroll
+        for (int i = 0; i < kKryNq - 1; i++)
+            if (i < nv) q[i] += x * V[i * n4 + t];
+        qq += x * x;
+    }
+    const int wi = threadIdx.x >> 5, ln = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < kKryNq; i++) {
+        if (i > nv) break;
+        const double v = warp_sum(i == nv ? qq : q[i]);
+        if (ln == 0) sh[i][wi] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x <= nv) {
+        double v = 0;
+        for (int a = 0; a < 8; a++) v += sh[threadIdx.x][a];
+        part[(long)blockIdx.x * kKryNq + threadIdx.x] = v;
+    }
+}
+
+__global__ void k_kr_dot_final(const double *part, int nblk, int nq, double *out)
+{
+    pdl_enter();
+    const int qi = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (qi >= nq) return;
+    double v = 0;
+    for (int b = ln; b < nblk; b += 32) v += part[(long)b * kKryNq + qi];
+    v = warp_sum(v);
+    if (ln == 0) out[qi] = v;
+}
+
+// w -= sum_i h_i v_i
+__global__ void k_kr_axpy(double *w, const double *V, int nv, long n4, const double *h)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    double x = w[t];
+    for (int i = 0; i < nv; i++) x -= h[i] * V[i * n4 + t];
+    w[t] = x;
+}
+
+// v = w / sqrt(nrm2)
+__global__ void k_kr_normalize(long n4, const double *w, double *v, const double *nrm2)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    v[t] = w[t] / sqrt(*nrm2);
+}
+
+struct KrY { double y[kKryMax]; };
+
+// x += sum_j y_j z_j
+__global__ void k_kr_update(long N, double *x0, double *x1, double *x2, double *x3, const double *Z, int k, KrY y)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int j = 0; j < k; j++) {
+        const double *z = Z + (long)j * 4 * N;
+        a0 += y.y[j] * z[t]; a1 += y.y[j] * z[N + t]; a2 += y.y[j] * z[2 * N + t]; a3 += y.y[j] * z[3 * N + t];
+    }
+    x0[t] += a0; x1[t] += a1; x2[t] += a2; x3[t] += a3;
+}
+
+static int kry_alloc(i3g_ctx *c, int m)
+{
+    KrylovState *K = kry(c);
+    if (K && K->m == m) return 0;
+    if (K) {
+        for (int j = 0; j < kKryMax; j++) if (K->g[j]) cudaGraphExecDestroy(K->g[j]);
+        cudaFree(K->V); cudaFree(K->Z); cudaFree(K->W); cudaFree(K->F0); cudaFree(K->part); cudaFree(K->hdev);
+        cudaFreeHost(K->hhost);
+        delete K;
+        c->kry = nullptr;
+    }
+    K = new KrylovState();
+    c->kry = K;
+    K->m = m;
+    K->N = c->lev[0].n;
+    const long n4 = 4 * K->N;
+    ALLOC(K->V, double, (m + 1) * n4);
+    ALLOC(K->Z, double, m * n4);
+    ALLOC(K->W, double, n4);
+    ALLOC(K->F0, double, n4);
+    ALLOC(K->part, double, (long)c->red_blocks * kKryNq);
+    ALLOC(K->hdev, double, 3 * kKryNq + 2);
+    I3G_CUDA(cudaMallocHost((void **)&K->hhost, (3 * kKryNq + 2) * sizeof(double)));
+    I3G_CUDA(cudaMemsetAsync(K->W, 0, n4 * 8, c->st));
+    I3G_CUDA(cudaMemsetAsync(K->F0, 0, n4 * 8, c->st));
+    return 0;
+}
+
+static void kry_free(i3g_ctx *c)
+{
+    KrylovState *K = kry(c);
+    if (!K) return;
+    for (int j = 0; j < kKryMax; j++) if (K->g[j]) cudaGraphExecDestroy(K->g[j]);
+    cudaFree(K->V); cudaFree(K->Z); cudaFree(K->W); cudaFree(K->F0); cudaFree(K->part); cudaFree(K->hdev);
+    cudaFreeHost(K->hhost);
+    delete K;
+    c->kry = nullptr;
+}
+
+// Arnoldi step j: z_j = M^-1 D^-1 v_j, w = D A z_j orthogonalised against v_0..v_j, v_{j+1} = w/|w|;
+// projections and the squared norm land in hhost.
+static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
+{
+    KrylovState *K = kry(c);
+    Level &L0 = c->lev[0];
+    const long N = K->N, n4 = 4 * N;
+    double *vj = K->V + (long)j * n4, *zj = K->Z + (long)j * n4;
+    // preconditioner: the FP32 V-cycle on the unscaled vector
+    const double *d = K->hdev + 3 * kKryNq;
+    LAUNCH(k_kr_to_r, nblk(N), 256, N, (const double *)vj, L0.d.r[0], L0.d.r[1], L0.d.r[2], L0.d.r[3], d);
+    const int nb = c->red_blocks;
+    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], N, c->dred);
+    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], N, c->dred + nb);
+    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], N, c->dred + 2 * nb);
+    LAUNCH(k_scale, 1, 1024, (const double *)c->dred, 3 * nb, c->h_ref, c->eta_ref, c->dscale);
+    LAUNCH(k_to_f32, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+           (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
+           L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, (const double *)c->dscale);
+    vcycle_t<float>(c, multinum, true);
+    LAUNCH(k_kr_store, nblk(N), 256, N, zj, (const float *)L0.s.u[0], (const float *)L0.s.u[1],
+           (const float *)L0.s.u[2], (const float *)L0.s.u[3], (const double *)c->dscale);
+    // w = D A z_j: the FP64 residual of z_j with a zero right-hand side is -A z_j
+    View<double> Vz = view<double>(L0, L0.d);
+    Vz.u0 = zj; Vz.u1 = zj + N; Vz.u2 = zj + 2 * N; Vz.u3 = zj + 3 * N;
+    Vz.f0 = K->F0; Vz.f1 = K->F0 + N; Vz.f2 = K->F0 + 2 * N; Vz.f3 = K->F0 + 3 * N;
+    Vz.r0 = K->W; Vz.r1 = K->W + N; Vz.r2 = K->W + 2 * N; Vz.r3 = K->W + 3 * N;
+    LAUNCH(k_residual<double>, nblk(N), 256, Vz);
+    for (int v = 0; v < 4; v++) {
+        BcList &B = L0.bcl[v];
+        if (B.n) LAUNCH(k_bc_residual<double>, nblk(B.n), 256, Vz, v, B.n, (const int *)B.node, (const int *)B.onode,
+                        (const int *)B.ocomp, (const double *)B.ok);
+    }
+    LAUNCH(k_kr_negscale, nblk(N), 256, N, K->W, d);
+    // classical Gram-Schmidt, twice
+    for (int pass = 0; pass < 2; pass++) {
+        double *h = K->hdev + pass * kKryNq;
+        LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
+        LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h);
+        LAUNCH(k_kr_axpy, nblk(n4), 256, K->W, (const double *)K->V, j + 1, n4, (const double *)h);
+    }
+    double *nrm = K->hdev + 2 * kKryNq;
+    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, 0, n4, K->part);
+    LAUNCH(k_kr_dot_final, 1, 32, (const double *)K->part, nb, 1, nrm);
+    LAUNCH(k_kr_normalize, nblk(n4), 256, n4, (const double *)K->W, K->V + (long)(j + 1) * n4, (const double *)nrm);
+    I3G_CUDA(cudaMemcpyAsync(K->hhost, K->hdev, 3 * kKryNq * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return 0;
+}
+
+static int kry_graph(i3g_ctx *c, int j, int multinum)
+{
+    KrylovState *K = kry(c);
+    if (K->g_multinum != multinum || K->g_p0 != c->p.p0koef || K->g_p1 != c->p.p1koef || K->g_v0 != c->p.v0koef ||
+        K->g_v1 != c->p.v1koef) {
+        for (int q = 0; q < kKryMax; q++) if (K->g[q]) { cudaGraphExecDestroy(K->g[q]); K->g[q] = nullptr; }
+        K->g_multinum = multinum; K->g_p0 = c->p.p0koef; K->g_p1 = c->p.p1koef; K->g_v0 = c->p.v0koef;
+        K->g_v1 = c->p.v1koef;
+    }
+    if (K->g[j]) return 0;
+    const int64_t l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    I3G_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int rc = kry_enqueue_step(c, j, multinum);
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&K->g[j], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    c->launches = l0;
+    return 0;
+}
+
+// One FGMRES restart cycle from the current level-0 solution; *steps += Arnoldi steps taken.
+static int kry_cycle(i3g_ctx *c, int multinum, double rtol, int maxsteps, int *steps)
+{
+    KrylovState *K = kry(c);
+    Level &L0 = c->lev[0];
+    const long N = K->N, n4 = 4 * N;
+    const int m = K->m;
+    // weights from the current norms (relres_enqueue has filled hred)
+    const double *q = c->hred;
+    const double dv = q[1] > 0 ? 1.0 / std::sqrt(q[1]) : 1.0;
+    const double rmsv = (c->nvel > 0 && q[3] > 0) ? std::sqrt(q[3] / c->nvel) : 0.0;
+    const double dp = (c->ncont > 0 && rmsv > 0) ? c->h_ref / (std::sqrt(c->ncont) * rmsv) : 1.0;
+    // weights to the device, then v_0 = D r / |D r|
+    K->hhost[3 * kKryNq] = dv;
+    K->hhost[3 * kKryNq + 1] = dp;
+    I3G_CUDA(cudaMemcpyAsync(K->hdev + 3 * kKryNq, K->hhost + 3 * kKryNq, 2 * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    const double *d = K->hdev + 3 * kKryNq;
+    residual_t<double>(c, 0);
+    LAUNCH(k_kr_from_r, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+           (const double *)L0.d.r[2], (const double *)L0.d.r[3], K->V, d);
+    double *nrm = K->hdev + 2 * kKryNq;
+    LAUNCH(k_kr_dots, c->red_blocks, 256, (const double *)K->V, (const double *)K->V, 0, n4, K->part);
+    LAUNCH(k_kr_dot_final, 1, 32, (const double *)K->part, c->red_blocks, 1, nrm);
+    I3G_CUDA(cudaMemcpyAsync(K->hhost + 2 * kKryNq, nrm, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    LAUNCH(k_kr_normalize, nblk(n4), 256, n4, (const double *)K->V, K->V, (const double *)nrm);
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    const double beta = std::sqrt(K->hhost[2 * kKryNq]);
+    if (!(beta > 0)) return 0;
+    double H[kKryMax + 1][kKryMax], cs[kKryMax], sn[kKryMax], g[kKryMax + 1];
+    for (int i = 0; i <= m; i++) g[i] = 0;
+    g[0] = beta;
+    int k = 0;
+    for (int j = 0; j < m && *steps < maxsteps; j++) {
+        int rc = kry_graph(c, j, multinum);
+        if (rc) return rc;
+        I3G_CUDA(cudaGraphLaunch(K->g[j], c->st));
+        I3G_CUDA(cudaStreamSynchronize(c->st));
+        (*steps)++;
+        k = j + 1;
+        const double *h = K->hhost;
+        for (int i = 0; i <= j; i++) H[i][j] = h[i] + h[kKryNq + i];
+        const double hn = std::sqrt(std::max(0.0, h[2 * kKryNq]));
+        // previous rotations, then a new one that zeroes H[j+1][j]
+        for (int i = 0; i < j; i++) {
+            const double a = H[i][j], b = H[i + 1][j];
+            H[i][j] = cs[i] * a + sn[i] * b;
+            H[i + 1][j] = -sn[i] * a + cs[i] * b;
+        }
+        const double a = H[j][j], r = std::hypot(a, hn);
+        cs[j] = r > 0 ? a / r : 1.0;
+        sn[j] = r > 0 ? hn / r : 0.0;
+        H[j][j] = r;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        if (!(g[j + 1] == g[j + 1])) return set_error(c, I3G_E_NAN, "NaN in the FGMRES step");
+        // |g[j+1]| = ||D r||, and ||D r||^2 = mom^2 + cont^2: both criteria hold once it is <= rtol
+        if (std::fabs(g[j + 1]) <= rtol || !(hn > 0)) break;
+    }
+    // y = R^-1 g, x += Z y
+    KrY y;
+    for (int i = k - 1; i >= 0; i--) {
+        double sum = g[i];
+        for (int l = i + 1; l < k; l++) sum -= H[i][l] * y.y[l];
+        y.y[i] = H[i][i] != 0 ? sum / H[i][i] : 0.0;
+    }
+    LAUNCH(k_kr_update, nblk(N), 256, N, L0.d.u[0], L0.d.u[1], L0.d.u[2], L0.d.u[3], (const double *)K->Z, k, y);
+    return 0;
+}
+
 int stokes_solve(i3g_ctx *c, double *timestep)
 {
     if (c->p.p2koef != 0 || c->f.p2koef != 0 || c->f.p2koef2 != 0)
@@ -1612,6 +1996,20 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;
     double best = std::max(mom, cont);
     bool switched = false;
+    static const bool trace = getenv("I3G_TRACE") != nullptr;   // per-cycle residuals on stderr
+    if (c->p.precision == 1 && c->p.krylov > 0) {
+        if (c->p.krylov > kKryMax) return set_error(c, I3G_E_ARG, "krylov restart length %d above %d", c->p.krylov, kKryMax);
+        if ((rc = kry_alloc(c, c->p.krylov))) return rc;
+        if (!c->dscale) I3G_CUDA(cudaMalloc((void **)&c->dscale, 16 * sizeof(double)));
+        while (!conv && cycles < maxc) {
+            if ((rc = kry_cycle(c, multinum, rtol, maxc, &cycles))) return rc;
+            outer++;
+            if ((rc = stokes_relres(c, &mom, &cont))) return rc;
+            if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
+            conv = mom <= rtol && cont <= rtol;
+            if (trace) fprintf(stderr, "i3g stokes fgmres restart %d cycles %d mom %.3e cont %.3e\n", outer, cycles, mom, cont);
+        }
+    }
     while (!conv && cycles < maxc) {
         for (int i = 0; i < ncyc && cycles < maxc && !conv; i++) {
             if ((rc = iteration_graph(c, multinum))) return rc;
@@ -1622,6 +2020,8 @@ int stokes_solve(i3g_ctx *c, double *timestep)
             relres_read(c, &mom, &cont);
             if (!(mom == mom) || !(cont == cont)) return set_error(c, I3G_E_NAN, "NaN residual after %d V-cycles", cycles);
             conv = mom <= rtol && cont <= rtol;
+            if (trace) fprintf(stderr, "i3g stokes cycle %d mom %.3e cont %.3e p0 %.3g p1 %.3g multinum %d\n", cycles, mom, cont,
+                               c->p.p0koef, c->p.p1koef, multinum);
             // Safeguard: a residual 30x above the best one seen in this solve means the cycle
             // diverges (transient rises of a convergent cycle stay far below that); switch to the
             // file row's second relaxation set early (the reference switches after multstp

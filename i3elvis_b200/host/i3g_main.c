@@ -3,7 +3,7 @@
  *
  * Run in a directory holding file.t3c, mode.t3c and the input .prn, like the reference:
  *
- *     i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-files N]
+ *     i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-files N]
  *     i3g -roundtrip in.prn out.prn      (read and rewrite a .prn; no GPU used)
  *     i3g -dump-mode mode.t3c            (print the parsed parameters; no GPU used)
  *
@@ -74,7 +74,7 @@ static int roundtrip(const char *in, const char *out)
 int main(int argc, char **argv)
 {
     double rtol = 1e-8, heat_rtol = 1e-10;
-    int maxcyc = 2000, precision = 0, max_files = -1;
+    int maxcyc = 2000, precision = 0, max_files = -1, krylov = 0;
     for (int a = 1; a < argc; a++) {
         if (!strcmp(argv[a], "-roundtrip") && a + 2 < argc) return roundtrip(argv[a + 1], argv[a + 2]);
         else if (!strcmp(argv[a], "-dump-mode") && a + 1 < argc) return dump_mode(argv[a + 1]);
@@ -82,9 +82,10 @@ int main(int argc, char **argv)
         else if (!strcmp(argv[a], "-heat-rtol") && a + 1 < argc) heat_rtol = atof(argv[++a]);
         else if (!strcmp(argv[a], "-maxcyc") && a + 1 < argc) maxcyc = atoi(argv[++a]);
         else if (!strcmp(argv[a], "-mixed")) precision = 1;
+        else if (!strcmp(argv[a], "-krylov") && a + 1 < argc) krylov = atoi(argv[++a]);
         else if (!strcmp(argv[a], "-files") && a + 1 < argc) max_files = atoi(argv[++a]);
         else {
-            fprintf(stderr, "usage: i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-files N]\n"
+            fprintf(stderr, "usage: i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-files N]\n"
                             "       i3g -roundtrip in.prn out.prn\n");
             return 2;
         }
@@ -105,6 +106,7 @@ int main(int argc, char **argv)
     md.p.heat_maxcyc = maxcyc;
     md.p.precision = precision;
     md.p.warm_start = 1;
+    md.p.krylov = krylov;
     i3g_ctx *c = NULL;
     if (check(i3g_create(&p.m, &md.p, &c), NULL, "i3g_create")) return 1;
     int rc = 0;

@@ -101,6 +101,9 @@ typedef struct i3g_params {
     int32_t heat_maxcyc;                /* cap on heat V-cycles (0 = 2000)               */
     int32_t precision;                  /* 0: FP64 multigrid, 1: FP32 MG inside FP64 defect correction */
     int32_t warm_start;                 /* 1: start from the previous step's v,P (reference behaviour) */
+    int32_t krylov;                     /* precision 1 only: > 0 accelerates the FP64 defect correction
+                                         * with FGMRES(krylov) preconditioned by the FP32 V-cycle (<= 16);
+                                         * 0: one V-cycle per correction, the reference's iteration */
 } i3g_params;
 
 /* ---- per output file row (load3mg.c:25-58, applied at i3mg.c:64-77) ---------------- */

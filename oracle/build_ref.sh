@@ -1,9 +1,11 @@
 #!/bin/sh
 # Builds oracle/_ref/ref_harness: the reference's own solver functions, compiled from the
 # reference sources where they lie, driven by oracle/ref_harness.c (test infrastructure).
-# The only change is to the static array sizes of head3mg.c:8-20 (the shipped sizes need
-# 78 GB of static storage); the size-patched copy is a temporary build input and is removed
-# after compilation.  Outputs go to oracle/_ref/ only.
+# Two changes, both in temporary copies removed after compilation: the static array sizes of
+# head3mg.c:8-20 (the shipped sizes need 78 GB of static storage), and an optional cap on the
+# outer iteration blocks of titerate (heat3mg.c:463-560 loops until heatsum <= HEATMIN, which
+# its racy multi-threaded relaxation may never reach); the cap is unlimited unless the
+# harness's sample command sets it.  Outputs go to oracle/_ref/ only.
 set -e
 REF=${I3G_REFERENCE_DIR:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -21,8 +23,11 @@ sed -e 's/^#define MAXMAT .*/#define MAXMAT  160000000/' \
     -e 's/^#define MAXMRK .*/#define MAXMRK  60000000/' \
     -e 's/^#define MAXBON .*/#define MAXBON   4000000/' \
     "$REF/head3mg.c" > "$OUT/gen/head3mg.c"
+sed -e 's/^while(heatsum>HEATMIN);/while(heatsum>HEATMIN \&\& ++i3g_heat_blocks < i3g_heat_block_cap);/' \
+    "$REF/heat3mg.c" > "$OUT/gen/heat3mg.c"
+grep -q "i3g_heat_block_cap" "$OUT/gen/heat3mg.c" || { echo "heat3mg.c loop not found" >&2; exit 1; }
 gcc -O2 -fopenmp -mcmodel=medium -w -I"$OUT/gen" -I"$REF" "$HERE/ref_harness.c" \
     -o "$OUT/ref_harness" -lm
-rm -f "$OUT/gen/head3mg.c"
+rm -f "$OUT/gen/head3mg.c" "$OUT/gen/heat3mg.c"
 rmdir "$OUT/gen" 2>/dev/null || true
 echo "built $OUT/ref_harness"

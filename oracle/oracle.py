@@ -156,8 +156,12 @@ def run_reference(workdir, *args, threads=1, timeout=3600):
 def run_reference_lines(workdir, *args, threads=1, timeout=3600):
     """Like ``run_reference`` but returns every JSON line the harness printed, in order."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    r = subprocess.run([REF, *map(str, args)], cwd=workdir, env=env, stdin=subprocess.DEVNULL,
-                       capture_output=True, text=True, timeout=timeout)
+    try:
+        r = subprocess.run([REF, *map(str, args)], cwd=workdir, env=env, stdin=subprocess.DEVNULL,
+                           capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired as e:
+        err = e.stderr.decode(errors="replace") if isinstance(e.stderr, bytes) else (e.stderr or "")
+        raise OracleError(f"reference harness timed out after {timeout} s; last progress: {err[-400:]}")
     if r.returncode != 0:
         raise OracleError(f"reference harness failed ({r.returncode}): {r.stderr[-2000:]}")
     out = []

@@ -27,6 +27,8 @@
 #include <omp.h>
 #include <time.h>
 
+/* cap on titerate's outer iteration blocks (see build_ref.sh); unlimited by default */
+static long i3g_heat_blocks = 0, i3g_heat_block_cap = 0x7fffffffffffffffL;
 #include "head3mg.c"
 #include "load3mg.c"
 #include "move3mg.c"
@@ -254,6 +256,8 @@ static void prepare_state(void)
 
 /* Level-0 velocities from sol0 into vx, vy, vz (move3mg.c:2246-2317) and the marker time
  * step limit maxxystep / max|v| (move3mg.c:2608-2632). */
+static double sample_vmax = 0;
+
 static void velocities_and_cfl(void)
 {
     long m1, m2, m3, n;
@@ -268,16 +272,19 @@ static void velocities_and_cfl(void)
             }
     for (int k = 0; k < 3; k++)
         if (vmax[k] > 0 && timestep > maxxystep / vmax[k]) timestep = maxxystep / vmax[k];
+    sample_vmax = fmax(vmax[0], fmax(vmax[1], vmax[2]));
 }
 
 int main(int argc, char **argv)
 {
     if (argc < 2) { fprintf(stderr, "usage: ref_harness CMD ...\n"); return 2; }
     const char *cmd = argv[1];
+    double tl = omp_get_wtime();
     loadconf();
     loader();
     file_params(0);
     timestep = maxtmstep;
+    fprintf(stderr, "loaded in %.1f s\n", omp_get_wtime() - tl);
     if (!strcmp(cmd, "prepare") && argc == 3) {
         prepare_state();
         snprintf(fl1out, sizeof fl1out, "%s", argv[2]);
@@ -405,37 +412,47 @@ int main(int argc, char **argv)
         return 0;
     }
     if (!strcmp(cmd, "sample") && argc >= 3) {
-        /* Bounded timing sample of time steps: SAMPLE NCYC [REPS [PREP]].  Optionally the
+        /* Bounded timing sample of time steps: SAMPLE NCYC [REPS [PREP [HEATCAP [DT]]]].  Optionally the
          * initial-condition passes first (PREP=1, timed apart); then REPS times: the reference's
          * vpiterate set-up (ronurestrict and row assembly, move3mg.c:1948-2159) and NCYC V-cycles,
-         * the velocities and CFL time step from that iterate, titerate, movemark and ronurecalc.
-         * Wall clock, one JSON line per repetition. */
+         * the velocities and CFL time step from that iterate (or DT seconds when given), titerate (at most HEATCAP outer
+         * iteration blocks), movemark and ronurecalc.  Wall clock, one JSON line per repetition. */
         int ncyc = atoi(argv[2]);
         int reps = argc >= 4 ? atoi(argv[3]) : 1;
+        if (argc >= 6 && atol(argv[5]) > 0) i3g_heat_block_cap = atol(argv[5]);
+        const double dt_fixed = argc >= 7 ? atof(argv[6]) : 0.0;
         double tp = 0;
         if (argc >= 5 && atoi(argv[4])) {
             double a = omp_get_wtime();
             prepare_state();
             tp = omp_get_wtime() - a;
         }
+        fprintf(stderr, "sample: prepared in %.1f s\n", tp);
         for (int r = 0; r < reps; r++) {
             timestep = maxtmstep;
             double t0 = omp_get_wtime();
             stokes_assemble();
             double t1 = omp_get_wtime();
+            fprintf(stderr, "sample %d: set-up %.1f s\n", r, t1 - t0);
             for (int i = 0; i < ncyc; i++) vcycle();
             double t2 = omp_get_wtime();
+            fprintf(stderr, "sample %d: %d V-cycles %.1f s\n", r, ncyc, t2 - t1);
             velocities_and_cfl();
+            if (dt_fixed > 0) timestep = dt_fixed;
+            i3g_heat_blocks = 0;
             if (tempmod) titerate(0);
             double t3 = omp_get_wtime();
+            fprintf(stderr, "sample %d: titerate %.1f s\n", r, t3 - t2);
             if (markmod) movemark();
             double t4 = omp_get_wtime();
+            fprintf(stderr, "sample %d: movemark %.1f s\n", r, t4 - t3);
             if (gridmod) ronurecalc();
             double t5 = omp_get_wtime();
             printf("{\"rep\": %d, \"assemble_s\": %.4f, \"vcycle_s\": %.4f, \"ncyc\": %d, \"heat_s\": %.4f, "
-                   "\"move_s\": %.4f, \"r2n_s\": %.4f, \"prepare_s\": %.4f, \"timestep\": %.6e, \"threads\": %d}\n",
+                   "\"move_s\": %.4f, \"r2n_s\": %.4f, \"prepare_s\": %.4f, \"timestep\": %.6e, \"vmax\": %.3e, "
+                   "\"heat_blocks\": %ld, \"threads\": %d}\n",
                    r, t1 - t0, (t2 - t1) / (ncyc > 0 ? ncyc : 1), ncyc, t3 - t2, t4 - t3, t5 - t4, tp, timestep,
-                   omp_get_max_threads());
+                   sample_vmax, i3g_heat_blocks + 1, omp_get_max_threads());
             fflush(stdout);
         }
         return 0;

@@ -105,13 +105,14 @@ def _compare_to_reference(p, sol, ref, tol):
     return errs
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision,krylov", [(0, 0), (1, 0), (1, 8)])
 @pytest.mark.parametrize("name", ["sphere13", "sphere17"])
-def test_solve_matches_reference(name, precision):
+def test_solve_matches_reference(name, precision, krylov):
     """Converged velocity and pressure equal the reference's converged FP64 solution to
-    relative L2 1e-8 (FP64 multigrid and FP32 multigrid inside FP64 defect correction)."""
+    relative L2 1e-8 (FP64 multigrid; FP32 multigrid inside FP64 defect correction, plain and
+    FGMRES-accelerated)."""
     p, mode, fx = golden(name)
-    par = abi.make_params(mode, stokes_rtol=1e-11, stokes_maxcyc=3000, precision=precision)
+    par = abi.make_params(mode, stokes_rtol=1e-11, stokes_maxcyc=3000, precision=precision, krylov=krylov)
     g = lib.Context(abi.ModelBuffers(p), par, abi.make_file_params(mode.files[0]))
     dt = g.stokes(0, 1e30)
     st = g.stats()
