@@ -157,6 +157,23 @@ int i3g_set_file_params(i3g_ctx *c, const i3g_file_params *f)
     return 0;
 }
 
+int i3g_set_params(i3g_ctx *c, const i3g_params *p)
+{
+    if (!c || !p) return I3G_E_ARG;
+    if (p->multimax != c->p.multimax)
+        return set_error(c, I3G_E_ARG, "multimax %d differs from the %d levels the context was built with", p->multimax,
+                         c->p.multimax);
+    c->p = *p;
+    // the current output-file row keeps overriding these (i3mg.c:64-77)
+    c->p.nubeg = c->f.nubeg;
+    c->p.nuend = c->f.nuend;
+    c->p.p0koef = c->f.p0koef;
+    c->p.p1koef = c->f.p1koef;
+    c->p.p2koef = c->f.p2koef;
+    i3g::stokes_params_changed(c);
+    return 0;
+}
+
 int i3g_stokes(i3g_ctx *c, int n0, double *timestep)
 {
     (void)n0;

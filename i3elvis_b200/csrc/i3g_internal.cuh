@@ -133,6 +133,7 @@ namespace i3g {
 int stokes_alloc(i3g_ctx *c);
 void stokes_free(i3g_ctx *c);
 void stokes_graph_free(i3g_ctx *c);
+void stokes_params_changed(i3g_ctx *c);
 int stokes_setup(i3g_ctx *c);
 int stokes_residual(i3g_ctx *c, int level);
 int stokes_smooth(i3g_ctx *c, int level, int nsweeps);

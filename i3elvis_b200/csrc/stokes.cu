@@ -1663,6 +1663,7 @@ struct KrylovState {
     double *hdev = nullptr;  // [3][kKryNq]: first and second projection, squared norm; then 2 weights
     double *hhost = nullptr; // pinned mirror of hdev
     cudaGraphExec_t g[kKryMax] = {};
+    long g_nodes[kKryMax] = {};   // kernels per captured step
     int g_multinum = -1;
     double g_p0 = 0, g_p1 = 0, g_v0 = 0, g_v1 = 0;
 };
@@ -1827,6 +1828,17 @@ static void kry_free(i3g_ctx *c)
     c->kry = nullptr;
 }
 
+// Captured iterations depend on the sweep counts and relaxation factors: drop them.
+void stokes_params_changed(i3g_ctx *c)
+{
+    if (c->sgraph) cudaGraphExecDestroy(c->sgraph);
+    c->sgraph = nullptr;
+    KrylovState *K = kry(c);
+    if (K)
+        for (int q = 0; q < kKryMax; q++)
+            if (K->g[q]) { cudaGraphExecDestroy(K->g[q]); K->g[q] = nullptr; }
+}
+
 // Arnoldi step j: z_j = M^-1 D^-1 v_j, w = D A z_j orthogonalised against v_0..v_j, v_{j+1} = w/|w|;
 // projections and the squared norm land in hhost.
 static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
@@ -1896,6 +1908,7 @@ static int kry_graph(i3g_ctx *c, int j, int multinum)
     e = cudaGraphInstantiate(&K->g[j], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    K->g_nodes[j] = c->launches - l0;
     c->launches = l0;
     return 0;
 }
@@ -1936,6 +1949,7 @@ static int kry_cycle(i3g_ctx *c, int multinum, double rtol, int maxsteps, int *s
         int rc = kry_graph(c, j, multinum);
         if (rc) return rc;
         I3G_CUDA(cudaGraphLaunch(K->g[j], c->st));
+        c->launches += K->g_nodes[j];
         I3G_CUDA(cudaStreamSynchronize(c->st));
         (*steps)++;
         k = j + 1;

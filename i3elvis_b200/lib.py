@@ -39,6 +39,7 @@ def load():
     L.i3g_last_error.argtypes = [P]
     L.i3g_last_error.restype = C.c_char_p
     L.i3g_set_file_params.argtypes = [P, C.POINTER(abi.FileParams)]
+    L.i3g_set_params.argtypes = [P, C.POINTER(abi.Params)]
     L.i3g_stokes.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
     L.i3g_heat.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
     L.i3g_move_markers.argtypes = [P, C.c_double]
@@ -95,6 +96,9 @@ class Context:
 
     def set_file_params(self, fp: abi.FileParams):
         self.call("i3g_set_file_params", C.byref(fp))
+
+    def set_params(self, p: abi.Params):
+        self.call("i3g_set_params", C.byref(p))
 
     # the four time-step calls of the host loop (i3mg.c:98-137)
     def stokes(self, n0: int, timestep: float) -> float:

@@ -140,6 +140,11 @@ const char *i3g_last_error(const i3g_ctx *c);   /* valid for c == NULL too */
 /* Per-output-file parameters (i3mg.c:64-77). */
 int i3g_set_file_params(i3g_ctx *c, const i3g_file_params *f);
 
+/* Replace the run parameters (no reference counterpart: the reference reads mode.t3c once,
+ * load3mg.c:2-170).  The level count (multimax) must stay the one the context was built with;
+ * the current file row's nubeg, nuend and p*koef keep overriding the mode values. */
+int i3g_set_params(i3g_ctx *c, const i3g_params *p);
+
 /* vpiterate(n0,f0) (move3mg.c:1585-2636): Stokes + continuity on the staggered grid.
  * Stops when the relative residual (momentum ||b-Ax||/||b|| and continuity
  * ||div v|| * h / ||v||, both <= stokes_rtol) is met, or -- when stokes_rtol <= 0 -- on the
