@@ -602,10 +602,11 @@ __device__ __forceinline__ void phase_density(const Phys &P, int mm2, double mtk
 
 // Each CTA owns one tile; markers are sorted by cell inside the tile.  A warp takes one cell:
 // lanes first compute the properties of up to 32 of its markers (stage 1, one marker per
-// lane) into a shared staging area, then lane = 4 * node + group accumulates, for one of the
-// cell's 8 nodes, one group of the 18 node sums over all staged markers (stage 2).  Cells are
-// visited in 8 parity classes; cells of one class share no node, so the per-cell sums are
-// added to the shared node sums without atomics, in a fixed order.
+// lane) into a shared staging area, then lane = 4 * node + subset accumulates all 18 sums of
+// one of the cell's 8 nodes over every fourth staged marker (stage 2, the same instruction
+// stream in every lane), and two shuffles combine the subsets.  Cells are visited in 8 parity
+// classes; cells of one class share no node, so the per-cell sums are added to the shared node
+// sums without atomics, in a fixed order.
 constexpr int kR2nWarps = 16;
 constexpr int kStage = 14;   // ddx0 ddx1 ddy0 ddy1 ddz0 ddz1 vnu mro mcp*mro mkt mht mbb mtk mrr
 
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *my = stg + warp * 32 * kStage;
-    const int nd = lane >> 2, grp = lane & 3;
+    const int nd = lane >> 2, sub = lane & 3;   // node of the cell, marker subset (m % 4)
     const int iz = nd >> 2, ix = (nd >> 1) & 1, iy = nd & 1;
     const int vm = P.viscmod;
     for (int colour = 0; colour < 8; colour++) {
@@ -635,7 +636,9 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
             const long cell = (long)tile * CPT + (lz * TX + lx) * TY + ly;
             const int beg = coff[cell], end = coff[cell + 1];
             if (beg == end) continue;   // uniform over the warp
-            double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+            double a[NACC];
+#pragma unroll
+            for (int q = 0; q < NACC; q++) a[q] = 0;
             for (int base = beg; base < end; base += 32) {
                 // stage 1: one marker per lane
                 bool ok = false;
@@ -695,47 +698,46 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
                 }
                 unsigned valid = __ballot_sync(0xffffffffu, ok);
                 __syncwarp();
-                // stage 2: lane (node, group) over the staged markers, in lane order
-                for (; valid; valid &= valid - 1) {
-                    const double *st = my + (__ffs(valid) - 1) * kStage;
+                // stage 2: lane (node, subset) over the staged markers m of its subset, all 18 sums
+                for (unsigned mine = valid & (0x11111111u << sub); mine; mine &= mine - 1) {
+                    const double *st = my + (__ffs(mine) - 1) * kStage;
                     const double ddx = st[ix], ddy = st[2 + iy], ddz = st[4 + iz];
                     const double swt = ddx * ddy * ddz;
                     const double vnu = st[6];
-                    if (grp == 0) {
-                        if (swt > 0) { s0 += st[7] * swt; s1 += st[8] * swt; s2 += st[9] * swt; s3 += st[10] * swt; }
-                    } else if (grp == 1) {
-                        if (swt > 0) { s0 += st[11] * swt; s1 += st[12] * swt; s2 += st[13] * swt; s3 += swt; }
-                    } else if (grp == 2) {
-                        if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { s0 += vnu * swt; s1 += swt; }
-                        if (ix && iy && iz) {
-                            const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
-                            s2 += vnu * w1; s3 += w1;
-                        }
-                    } else {
-                        if (!iz && ddx > 0.5 && ddy > 0.5) {
-                            const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
-                            s0 += vnu * w1; s1 += w1;
-                        }
-                        if (!iy && ddx > 0.5 && ddz > 0.5) {
-                            const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
-                            s2 += vnu * w1; s3 += w1;
-                        }
-                        if (!ix && ddy > 0.5 && ddz > 0.5) {
-                            const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
-                            s4 += vnu * w1; s5 += w1;
-                        }
+                    if (swt > 0) {
+                        a[A_RO] += st[7] * swt; a[A_CP] += st[8] * swt; a[A_KT] += st[9] * swt; a[A_HT] += st[10] * swt;
+                        a[A_ET] += st[11] * swt; a[A_TK] += st[12] * swt; a[A_RR] += st[13] * swt; a[W_P] += swt;
+                    }
+                    if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { a[A_NU] += vnu * swt; a[W_NU] += swt; }
+                    if (ix && iy && iz) {
+                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
+                        a[A_XX] += vnu * w1; a[W_XX] += w1;
+                    }
+                    if (!iz && ddx > 0.5 && ddy > 0.5) {
+                        const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
+                        a[A_XY] += vnu * w1; a[W_XY] += w1;
+                    }
+                    if (!iy && ddx > 0.5 && ddz > 0.5) {
+                        const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
+                        a[A_XZ] += vnu * w1; a[W_XZ] += w1;
+                    }
+                    if (!ix && ddy > 0.5 && ddz > 0.5) {
+                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
+                        a[A_YZ] += vnu * w1; a[W_YZ] += w1;
                     }
                 }
                 __syncwarp();
             }
-            const int lb = ((lz + iz) * NBX + (lx + ix)) * NBY + (ly + iy);
-            double *a = sacc + lb;
-            if (grp == 0) { a[A_RO * NBOX] += s0; a[A_CP * NBOX] += s1; a[A_KT * NBOX] += s2; a[A_HT * NBOX] += s3; }
-            else if (grp == 1) { a[A_ET * NBOX] += s0; a[A_TK * NBOX] += s1; a[A_RR * NBOX] += s2; a[W_P * NBOX] += s3; }
-            else if (grp == 2) { a[A_NU * NBOX] += s0; a[W_NU * NBOX] += s1; a[A_XX * NBOX] += s2; a[W_XX * NBOX] += s3; }
-            else {
-                a[A_XY * NBOX] += s0; a[W_XY * NBOX] += s1; a[A_XZ * NBOX] += s2; a[W_XZ * NBOX] += s3;
-                a[A_YZ * NBOX] += s4; a[W_YZ * NBOX] += s5;
+            // the four subsets of each node, then one lane per node adds the cell's sums
+#pragma unroll
+            for (int q = 0; q < NACC; q++) {
+                a[q] += __shfl_xor_sync(0xffffffffu, a[q], 1);
+                a[q] += __shfl_xor_sync(0xffffffffu, a[q], 2);
+            }
+            if (sub == 0) {
+                double *acc_n = sacc + ((lz + iz) * NBX + (lx + ix)) * NBY + (ly + iy);
+#pragma unroll
+                for (int q = 0; q < NACC; q++) acc_n[q * NBOX] += a[q];
             }
         }
         __syncthreads();

@@ -1764,6 +1764,20 @@ __global__ void k_kr_axpy(double *w, const double *V, int nv, long n4, const dou
     w[t] = x;
 }
 
+// v = (w - sum_i h_i v_i) / |.|, the squared norm taken as w.w - sum_i h_i^2 (hw[nv] = w.w from
+// the projection pass; v_0..v_{nv-1} are orthonormal)
+__global__ void k_kr_axpy_normalize(double *v, const double *w, const double *V, int nv, long n4, const double *hw)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    double nrm2 = hw[nv];
+    for (int i = 0; i < nv; i++) nrm2 -= hw[i] * hw[i];
+    double x = w[t];
+    for (int i = 0; i < nv; i++) x -= hw[i] * V[i * n4 + t];
+    v[t] = x / sqrt(nrm2);
+}
+
 // v = w / sqrt(nrm2)
 __global__ void k_kr_normalize(long n4, const double *w, double *v, const double *nrm2)
 {
@@ -1873,18 +1887,17 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
                         (const int *)B.ocomp, (const double *)B.ok);
     }
     LAUNCH(k_kr_negscale, nblk(N), 256, N, K->W, d);
-    // classical Gram-Schmidt, twice
-    for (int pass = 0; pass < 2; pass++) {
-        double *h = K->hdev + pass * kKryNq;
-        LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
-        LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h);
-        LAUNCH(k_kr_axpy, nblk(n4), 256, K->W, (const double *)K->V, j + 1, n4, (const double *)h);
-    }
-    double *nrm = K->hdev + 2 * kKryNq;
-    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, 0, n4, K->part);
-    LAUNCH(k_kr_dot_final, 1, 32, (const double *)K->part, nb, 1, nrm);
-    LAUNCH(k_kr_normalize, nblk(n4), 256, n4, (const double *)K->W, K->V + (long)(j + 1) * n4, (const double *)nrm);
-    I3G_CUDA(cudaMemcpyAsync(K->hhost, K->hdev, 3 * kKryNq * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    // classical Gram-Schmidt, twice; the second projection's pass also yields w.w, from which the
+    // last kernel forms the norm while it subtracts the projection and normalises
+    double *h1 = K->hdev, *h2 = K->hdev + kKryNq;
+    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
+    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h1);
+    LAUNCH(k_kr_axpy, nblk(n4), 256, K->W, (const double *)K->V, j + 1, n4, (const double *)h1);
+    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
+    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h2);
+    LAUNCH(k_kr_axpy_normalize, nblk(n4), 256, K->V + (long)(j + 1) * n4, (const double *)K->W, (const double *)K->V,
+           j + 1, n4, (const double *)h2);
+    I3G_CUDA(cudaMemcpyAsync(K->hhost, K->hdev, 2 * kKryNq * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     return 0;
 }
 
@@ -1955,7 +1968,9 @@ static int kry_cycle(i3g_ctx *c, int multinum, double rtol, int maxsteps, int *s
         k = j + 1;
         const double *h = K->hhost;
         for (int i = 0; i <= j; i++) H[i][j] = h[i] + h[kKryNq + i];
-        const double hn = std::sqrt(std::max(0.0, h[2 * kKryNq]));
+        double hn2 = h[kKryNq + j + 1];   // w.w before the second projection
+        for (int i = 0; i <= j; i++) hn2 -= h[kKryNq + i] * h[kKryNq + i];
+        const double hn = std::sqrt(std::max(0.0, hn2));
         // previous rotations, then a new one that zeroes H[j+1][j]
         for (int i = 0; i < j; i++) {
             const double a = H[i][j], b = H[i + 1][j];
