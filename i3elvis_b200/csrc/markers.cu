@@ -62,6 +62,7 @@ struct Grid {
     int nx, ny, nz;
     double xsize, ysize, zsize;
     const double *gx, *gy, *gz;     // shared-memory copies inside kernels
+    double ux, uy, uz;              // 1 / spacing of a uniform axis, 0 when not uniform
 };
 
 __device__ __forceinline__ int bsearch_g(const double *g, int n, double x)
@@ -73,6 +74,24 @@ __device__ __forceinline__ int bsearch_g(const double *g, int n, double x)
     } while ((b - a) > 1);
     if (a > n - 2) a = n - 2;
     return a;
+}
+
+// bsearch_g's result without the search on (nearly) uniform axes: a guess from the spacing,
+// accepted only if it or a neighbour brackets x exactly as the search would; otherwise the
+// search.  Identical results for any strictly increasing grid.
+__device__ __forceinline__ int locate(const double *g, int n, double x, double inv)
+{
+    if (inv > 0) {
+        const double t = (x - g[0]) * inv;
+        if (t >= 0 && t < (double)n) {   // false for NaN
+            int m = (int)t;
+            if (m > n - 2) m = n - 2;
+            if (g[m] <= x && (m == n - 2 || x < g[m + 1])) return m;
+            if (m > 0 && g[m - 1] <= x && x < g[m]) return m - 1;
+            if (m + 1 <= n - 2 && g[m + 1] <= x && (m + 1 == n - 2 || x < g[m + 2])) return m + 1;
+        }
+    }
+    return bsearch_g(g, n, x);
 }
 
 __device__ __forceinline__ double clamp01(double d) { return d < 0 ? 0.0 : (d > 1.0 ? 1.0 : d); }
@@ -93,7 +112,7 @@ __device__ void vxyz(const Grid &G, const NodeF &F, double x, double y, double z
     if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
     if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
-    const int m1 = wn[0] = bsearch_g(gx, X, x), m2 = wn[1] = bsearch_g(gy, Y, y), m3 = wn[2] = bsearch_g(gz, Z, z);
+    const int m1 = wn[0] = locate(gx, X, x, G.ux), m2 = wn[1] = locate(gy, Y, y, G.uy), m3 = wn[2] = locate(gz, Z, z, G.uz);
     int a, b, c;
     double dx, dy, dz, ddx, ddy, ddz;
     a = m1; if (a < 0) a = 0; if (a > X - 2) a = X - 2;
@@ -237,7 +256,7 @@ __device__ double pr_at(const Grid &G, const double *pr, long NY, long NXY, doub
     if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
     if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
-    const int m1 = wn[0] = bsearch_g(gx, X, x), m2 = wn[1] = bsearch_g(gy, Y, y), m3 = wn[2] = bsearch_g(gz, Z, z);
+    const int m1 = wn[0] = locate(gx, X, x, G.ux), m2 = wn[1] = locate(gy, Y, y, G.uy), m3 = wn[2] = locate(gz, Z, z, G.uz);
     int a = m1, b = m2, c = m3;
     if (x > (gx[a] + gx[a + 1]) / 2.0) a += 1; if (a < 1) a = 1; if (a > X - 2) a = X - 2;
     if (y > (gy[b] + gy[b + 1]) / 2.0) b += 1; if (b < 1) b = 1; if (b > Y - 2) b = Y - 2;
@@ -470,7 +489,7 @@ __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *c
             if (xd > G.xsize) xd = G.xsize;
             if (yd > G.ysize) yd = G.ysize;
             if (zd > G.zsize) zd = G.zsize;
-            kk = cell_key(bsearch_g(G.gx, G.nx, xd), bsearch_g(G.gy, G.ny, yd), bsearch_g(G.gz, G.nz, zd), T);
+            kk = cell_key(locate(G.gx, G.nx, xd, G.ux), locate(G.gy, G.ny, yd, G.uy), locate(G.gz, G.nz, zd, G.uz), T);
         }
         key[i] = kk;
     }
@@ -767,7 +786,7 @@ struct TkF { const float *tk0, *tk1, *tk, *tk2, *kt, *ro, *cp; long NY, NXY; };
 __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, double y, double z, double *e, int *wn,
                                       long *nodes, double *wi)
 {
-    const int m10 = wn[0] = bsearch_g(G.gx, G.nx, x), m20 = wn[1] = bsearch_g(G.gy, G.ny, y), m30 = wn[2] = bsearch_g(G.gz, G.nz, z);
+    const int m10 = wn[0] = locate(G.gx, G.nx, x, G.ux), m20 = wn[1] = locate(G.gy, G.ny, y, G.uy), m30 = wn[2] = locate(G.gz, G.nz, z, G.uz);
     const double dx = wi[8] = G.gx[m10 + 1] - G.gx[m10];
     const double dy = wi[9] = G.gy[m20 + 1] - G.gy[m20];
     const double dz = wi[10] = G.gz[m30 + 1] - G.gz[m30];
@@ -1001,12 +1020,24 @@ static void free_marks(Marks &M)
     cudaFree(M.id);
 }
 
+// 1 / spacing when the grid lines are equally spaced to 1e-6, else 0 (locate() then searches)
+static double uniform_inv(const double *g, int n)
+{
+    if (n < 2) return 0.0;
+    const double h = (g[n - 1] - g[0]) / (n - 1);
+    if (!(h > 0)) return 0.0;
+    for (int i = 0; i + 1 < n; i++)
+        if (std::fabs((g[i + 1] - g[i]) - h) > 1e-6 * h) return 0.0;
+    return 1.0 / h;
+}
+
 static Grid grid_of(i3g_ctx *c)
 {
     Grid G;
     G.nx = (int)c->m.xnumx; G.ny = (int)c->m.ynumy; G.nz = (int)c->m.znumz;
     G.xsize = c->m.xsize; G.ysize = c->m.ysize; G.zsize = c->m.zsize;
     G.gx = c->gx0; G.gy = c->gy0; G.gz = c->gz0;
+    G.ux = uniform_inv(c->hgx, G.nx); G.uy = uniform_inv(c->hgy, G.ny); G.uz = uniform_inv(c->hgz, G.nz);
     return G;
 }
 
