@@ -87,6 +87,7 @@ __device__ __forceinline__ double hsum(const HView &V, const HRow &R, long n, do
 
 __global__ void __launch_bounds__(256) k_heat_relax(HView V, int color, double koef)
 {
+    pdl_enter();
     const int hy = (V.ny + 1) >> 1;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)hy * V.nx * V.nz) return;
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(256) k_heat_relax(HView V, int color, double k
 
 __global__ void k_heat_residual(HView V)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= V.nxy * V.nz) return;
     if (V.bc[n]) return;
@@ -117,6 +119,7 @@ __global__ void k_heat_residual(HView V)
 __global__ void k_heat_bc(double *u, int n, const int *node, const int *pn, const int *dep, const double *cc,
                           const double *kk, int use_c)
 {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     double v = pn[t] >= 0 ? u[pn[t]] : 0.0;
@@ -127,6 +130,7 @@ __global__ void k_heat_bc(double *u, int n, const int *node, const int *pn, cons
 
 __global__ void k_heat_bc_res(const double *u, const double *f, double *r, int n, const int *node, const int *on, const double *ok)
 {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int nd = node[t];
@@ -140,6 +144,7 @@ struct TrV { const int *gptr, *gf; const double *gw; const int *a; const double 
 // node-centred residual restriction, weight-normalised, boundary rows excluded
 __global__ void k_heat_restrict(HView F, HView Cc, TrV tx, TrV ty, TrV tz)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Cc.nxy * Cc.nz) return;
     const int j = (int)(n % Cc.ny);
@@ -162,6 +167,7 @@ __global__ void k_heat_restrict(HView F, HView Cc, TrV tx, TrV ty, TrV tz)
 
 __global__ void k_heat_prolong(HView F, HView Cc, TrV tx, TrV ty, TrV tz, double koef)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= F.nxy * F.nz) return;
     const int j = (int)(n % F.ny);
@@ -182,6 +188,7 @@ __global__ void k_heat_prolong(HView F, HView Cc, TrV tx, TrV ty, TrV tz, double
 // conductivity and volumetric heat capacity of a coarse level (volume weights)
 __global__ void k_heat_coef_restrict(HView F, HView Cc, float *ktc, double *rocpc, TrV tx, TrV ty, TrV tz)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Cc.nxy * Cc.nz) return;
     const int j = (int)(n % Cc.ny);
@@ -218,6 +225,7 @@ struct H0Args {
 
 __global__ void k_heat_setup0(H0Args a)
 {
+    pdl_enter();
     __shared__ double sh[8];
     const long NY = a.ny, NXY = (long)a.nx * a.ny, N = NXY * a.nz;
     double m = 0;
@@ -264,6 +272,7 @@ __global__ void k_heat_setup0(H0Args a)
 __global__ void k_heat_substep0(long N, const float *tk, float *tk0, const float *tk1, const double *rocp, const uint8_t *bc,
                                 double *u, double *f, double dt)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     const float t = tk[n];
@@ -275,18 +284,21 @@ __global__ void k_heat_substep0(long N, const float *tk, float *tk0, const float
 // level-0 boundary constants (tbonderr, heat3mg.c:817-824)
 __global__ void k_bc_rhs_heat(double *f, int n, const int *node, const double *oc)
 {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) f[node[t]] = oc[t];
 }
 
 __global__ void k_heat_store(long N, const double *u, float *tk)
 {
+    pdl_enter();
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n < N) tk[n] = (float)u[n];
 }
 
 __global__ void k_heat_norm_part(HView V, double *part)
 {
+    pdl_enter();
     __shared__ double sh[2][8];
     double q[2] = {0, 0};
     const long N = V.nxy * V.nz;
@@ -320,7 +332,7 @@ static inline unsigned nb(long n, int t = 256) { return (unsigned)((n + t - 1) /
 
 #define LAUNCH(kern, grid, block, ...)                                                     \
     do {                                                                                   \
-        kern<<<(grid), (block), 0, c->st>>>(__VA_ARGS__);                                  \
+        launch_pdl(c->st, kern, dim3(grid), dim3(block), __VA_ARGS__);                     \
         c->launches++;                                                                     \
     } while (0)
 

@@ -7,6 +7,8 @@
 #pragma once
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
+#include <utility>
 #include <cuda_runtime.h>
 #include "../../include/i3g.h"
 
@@ -17,6 +19,38 @@
     } while (0)
 
 namespace i3g {
+
+// Programmatic dependent launch: kernels launched through launch_pdl() are scheduled while their
+// predecessor on the stream still runs; each such kernel must start with pdl_enter(), which waits
+// for the predecessor's completion (and memory) before any data is touched and then lets its own
+// successor launch.  On latency-bound launches this hides most of the launch gap.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+inline bool pdl_enabled()
+{
+    static const bool on = getenv("I3G_PDL") == nullptr || atoi(getenv("I3G_PDL")) != 0;
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(cudaStream_t st, void (*kern)(KArgs...), dim3 grid, dim3 block, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 constexpr int kMaxBcDepth = 4;   // boundary chains x_a = c + k x_b, x_b = c' + k' x_c, ...
 

@@ -40,16 +40,6 @@ struct Ar<float> {
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
 };
 
-// Programmatic dependent launch: every kernel of this file is launched with programmatic
-// stream serialization, so the next kernel is scheduled while this one runs; it waits for its
-// predecessor's completion (and memory) before touching any data, then lets its own successor
-// launch.  On the latency-bound coarse levels this hides most of the launch gap.
-__device__ __forceinline__ void pdl_enter()
-{
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // Level view passed by value to kernels.
 template <typename T>
 struct View {
@@ -258,7 +248,7 @@ __device__ __forceinline__ void relax_vel_at(const View<T> &L, long t, int color
 }
 
 template <typename T, int V>
-__global__ void __launch_bounds__(256, 4) k_relax_vel(View<T> L, int color, T koef)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_relax_vel(View<T> L, int color, T koef)
 {
     pdl_enter();
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,7 +271,7 @@ __device__ __forceinline__ void relax_p_at(const View<T> &L, long n, T koef)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 4) k_relax_p(View<T> L, T koef)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_relax_p(View<T> L, T koef)
 {
     pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -332,7 +322,7 @@ __device__ __forceinline__ void residual_at(const View<T> &L, long n)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual(View<T> L)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_residual(View<T> L)
 {
     pdl_enter();
     long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1174,24 +1164,6 @@ void stokes_free(i3g_ctx *c)
     cudaFree(c->dred);
     if (c->hred) cudaFreeHost(c->hred);
     c->hred = nullptr;
-}
-
-static bool g_pdl = getenv("I3G_PDL") == nullptr || atoi(getenv("I3G_PDL")) != 0;
-
-template <typename... KArgs, typename... Args>
-static void launch_pdl(cudaStream_t st, void (*kern)(KArgs...), dim3 grid, dim3 block, Args &&...args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = g_pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
 #define LAUNCH(kern, grid, block, ...)                                                     \
