@@ -245,6 +245,8 @@ def main():
     ap.add_argument("--workload", default="incl129", choices=tuple(WORKLOADS))
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--sweeps", default=None, help="relaxation sweeps per level, 'down,../up,..'")
+    ap.add_argument("--warm", type=int, default=2, choices=(1, 2),
+                    help="mixed precision: 1 previous step's solution, 2 linear extrapolation from the last two")
     ap.add_argument("--krylov", type=int, default=12,
                     help="mixed precision: FGMRES restart length around the FP32 V-cycle (0: plain defect correction)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -275,7 +277,9 @@ def main():
         sweeps = MIXED_SWEEPS.get(WORKLOADS[args.workload]["multinum"])
     prn, mode = build_case(args.workload, seed_offset=rank, sweeps=sweeps)
     krylov = args.krylov if prec == 1 else 0
-    par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec, krylov=krylov)
+    warm = args.warm if prec == 1 else 1
+    par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec, krylov=krylov,
+                          warm_start=warm)
     buf = abi.ModelBuffers(prn, pinned=True)
     ctx = lib.Context(buf, par, abi.make_file_params(mode.files[0]))
     f = mode.files[0]
@@ -376,7 +380,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32-in-f64", "data": "synthetic",
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "precision": args.precision,
-                   "stokes_rtol": args.rtol, "krylov": krylov, "sweeps": [list(mode.multinnn[0]), list(mode.multinnn[1])],
+                   "stokes_rtol": args.rtol, "krylov": krylov, "warm_start": warm, "sweeps": [list(mode.multinnn[0]), list(mode.multinnn[1])],
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "timestep_s": float(np.median([lg["timestep"] for lg in logs])),
         "stokes_cycles": cycles[args.warmup:], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in

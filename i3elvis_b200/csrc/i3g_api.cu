@@ -241,6 +241,7 @@ int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask)
     if (!c || !m) return I3G_E_ARG;
     const long N = c->nodenum;
     if (mask & I3G_SYNC_NODES) {
+        c->nhist = 0;   // new state: no extrapolation across it
         H2D(c->pr, m->pr, N, 8);
         H2D(c->vx, m->vx, N, 4); H2D(c->vy, m->vy, N, 4); H2D(c->vz, m->vz, N, 4);
         H2D(c->ro, m->ro, N, 4); H2D(c->lev[0].nu, m->nu, N, 4);

@@ -153,6 +153,9 @@ struct i3g_ctx {
     long sg_nodes = 0;
     double *dscale = nullptr;                   // device scale factors of the FP32 correction solve
     long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
+    double *hist[2][4] = {};                    // last two converged level-0 solutions (warm_start 2)
+    double hist_dt[2] = {0, 0};                 // time steps taken after them
+    int nhist = 0;
     void *kry = nullptr;       // FGMRES state of the mixed-precision Stokes solve
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state

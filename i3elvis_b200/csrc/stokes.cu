@@ -1136,6 +1136,8 @@ void stokes_free(i3g_ctx *c)
 {
     stokes_graph_free(c);
     kry_free(c);
+    for (int h = 0; h < 2; h++)
+        for (int v = 0; v < 4; v++) { cudaFree(c->hist[h][v]); c->hist[h][v] = nullptr; }
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
         delete[] L.gx; delete[] L.gy; delete[] L.gz;
@@ -1775,6 +1777,15 @@ __global__ void k_kr_update(long N, double *x0, double *x1, double *x2, double *
     x0[t] += a0; x1[t] += a1; x2[t] += a2; x3[t] += a3;
 }
 
+// u = a + r (a - b): the next solution predicted from the last two
+__global__ void k_extrapolate(long n, double *u, const double *a, const double *b, double r)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    u[t] = a[t] + r * (a[t] - b[t]);
+}
+
 static int kry_alloc(i3g_ctx *c, int m)
 {
     KrylovState *K = kry(c);
@@ -1983,6 +1994,13 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     Level &L0 = c->lev[0];
     if (!c->p.warm_start)
         for (int v = 0; v < 4; v++) I3G_CUDA(cudaMemsetAsync(L0.d.u[v], 0, L0.n * 8, c->st));
+    if (c->p.warm_start == 2 && c->nhist == 2 && c->hist_dt[0] > 0) {
+        // linear extrapolation in time from the last two converged solutions
+        const double r = c->hist_dt[1] / c->hist_dt[0];
+        for (int v = 0; v < 4; v++)
+            LAUNCH(k_extrapolate, nblk(L0.n), 256, L0.n, L0.d.u[v], (const double *)c->hist[1][v],
+                   (const double *)c->hist[0][v], r);
+    }
     // boundary rows of the initial guess consistent with their partners
     for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
     const int maxc = c->p.stokes_maxcyc > 0 ? c->p.stokes_maxcyc : 2000;
@@ -2052,7 +2070,21 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     c->st_.stokes_rel = std::max(mom, cont);
     c->st_.stokes_mom_rel = mom;
     c->st_.stokes_cont_rel = cont;
+    if (c->p.warm_start == 2 && conv) {
+        if (!c->hist[0][0])
+            for (int h = 0; h < 2; h++)
+                for (int v = 0; v < 4; v++) ALLOC(c->hist[h][v], double, L0.n);
+        for (int v = 0; v < 4; v++) {
+            std::swap(c->hist[0][v], c->hist[1][v]);
+            I3G_CUDA(cudaMemcpyAsync(c->hist[1][v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+        }
+    }
     if ((rc = finish_solve(c, timestep))) return rc;
+    if (c->p.warm_start == 2 && conv) {
+        c->hist_dt[0] = c->hist_dt[1];
+        c->hist_dt[1] = *timestep;
+        c->nhist = std::min(c->nhist + 1, 2);
+    }
     I3G_CUDA(cudaEventRecord(e1, c->st));
     I3G_CUDA(cudaEventSynchronize(e1));
     float ms = 0;

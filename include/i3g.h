@@ -100,7 +100,9 @@ typedef struct i3g_params {
     double heat_rtol;                   /* > 0: stop on relative heat residual           */
     int32_t heat_maxcyc;                /* cap on heat V-cycles (0 = 2000)               */
     int32_t precision;                  /* 0: FP64 multigrid, 1: FP32 MG inside FP64 defect correction */
-    int32_t warm_start;                 /* 1: start from the previous step's v,P (reference behaviour) */
+    int32_t warm_start;                 /* 0: zero start; 1: the previous step's v,P (reference behaviour);
+                                         * 2: linear extrapolation in time from the last two converged
+                                         * solutions (falls back to 1 until two exist; reset by i3g_upload) */
     int32_t krylov;                     /* precision 1 only: > 0 accelerates the FP64 defect correction
                                          * with FGMRES(krylov) preconditioned by the FP32 V-cycle (<= 16);
                                          * 0: one V-cycle per correction, the reference's iteration */

@@ -120,3 +120,28 @@ def test_solve_matches_reference(name, precision, krylov):
     n0 = cases.level_sizes(p, mode.multinum)[0]
     _compare_to_reference(p, g.get(abi.A_SOL, 0, 4 * n0), fx["solve_sol"], 1e-8)
     assert 0 < dt < 1e30
+
+
+def test_extrapolated_warm_start_reaches_same_solution():
+    """warm_start 2 (linear extrapolation from the last two solutions) changes only the start of
+    the iteration: after three time steps the state equals the one of warm_start 1 to the
+    solver tolerance, with no more V-cycles."""
+    from i3elvis_b200 import runtime
+    sols, cyc = [], []
+    for warm in (1, 2):
+        p, mode, fx = golden("sphere17")
+        par = abi.make_params(mode, stokes_rtol=1e-10, stokes_maxcyc=3000, precision=1, krylov=8, warm_start=warm)
+        g = lib.Context(abi.ModelBuffers(p), par, abi.make_file_params(mode.files[0]))
+        f = mode.files[0]
+        c = []
+        for n0 in range(3):
+            runtime.time_step(g, mode, f, n0)
+            c.append(g.stats()["stokes_cycles"])
+        n0 = cases.level_sizes(p, mode.multinum)[0]
+        sols.append(g.get(abi.A_SOL, 0, 4 * n0))
+        cyc.append(c)
+        g.close()
+    a, b = sols[0].reshape(-1, 4), sols[1].reshape(-1, 4)
+    for k in (1, 2, 3):
+        assert np.linalg.norm(a[:, k] - b[:, k]) <= 1e-6 * np.linalg.norm(a[:, k]), (k, cyc)
+    assert cyc[1][2] <= cyc[0][2] + 2, cyc
