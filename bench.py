@@ -54,7 +54,8 @@ def default_sweeps(mn):
 
 # Sweeps of the FP32 V-cycle when it preconditions FGMRES: the Krylov iteration removes the slow
 # components, so a lighter cycle (a quarter of the reference's sweeps) reaches the tolerance sooner
-# in time (incl129: 24 V-cycles in 82 ms against 14 in 104 ms with the full sweeps).
+# in time (incl129, previous-step start: 24 V-cycles in 82 ms against 14 in 104 ms with the full
+# sweeps; with the extrapolated start FGMRES(8), (12) and (16) all take 15-17 V-cycles, 51-54 ms).
 MIXED_SWEEPS = {4: "2,4,4,8/2,4,4,8,16", 3: "2,4,4/2,4,4,8", 2: "2,4/2,4,8"}
 
 
@@ -100,6 +101,22 @@ def host_threads():
     except (OSError, ValueError):
         pass
     return n
+
+
+def max_over_ranks(x, world, device):
+    """Largest value of x over all ranks (the job's time is the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def per_step_seconds(ms_max, steps, world):
+    """Aggregate seconds per time step of the whole job: world replicas each ran `steps` steps
+    in ms_max milliseconds."""
+    return ms_max / 1e3 / (steps * world)
 
 
 def log(msg):
@@ -247,7 +264,7 @@ def main():
     ap.add_argument("--sweeps", default=None, help="relaxation sweeps per level, 'down,../up,..'")
     ap.add_argument("--warm", type=int, default=2, choices=(1, 2),
                     help="mixed precision: 1 previous step's solution, 2 linear extrapolation from the last two")
-    ap.add_argument("--krylov", type=int, default=12,
+    ap.add_argument("--krylov", type=int, default=8,
                     help="mixed precision: FGMRES restart length around the FP32 V-cycle (0: plain defect correction)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true",
@@ -312,11 +329,8 @@ def main():
     barrier()
     clk = clocks.stop()
     launches = ctx.stats()["kernel_launches"] - l0
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = ms_max / 1e3 / (args.steps * world)
+    ms_max = max_over_ranks(ms, world, "cuda")
+    value = per_step_seconds(ms_max, args.steps, world)
 
     log(f"timed steps done: {ms_max / args.steps:.1f} ms/step")
     # the plain FP64 multigrid (the reference's iteration and sweeps) on the same state, for the
@@ -357,10 +371,7 @@ def main():
         ctx.download(abi.SYNC_ALL)
     barrier()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = float(tt.item()) / world
+    e2e_value = max_over_ranks(e2e_s, world, "cuda") / world
 
     # roofline of the dominant kernel: the multicolour Stokes relaxation of this precision
     kind = 7 if prec == 1 else 0
