@@ -63,6 +63,7 @@ void i3g_destroy(i3g_ctx *c)
                  c->kt, c->ht, c->rr, c->gx0, c->gy0, c->gz0, c->lev[0].nu, c->deps, c->dsig};
     for (void *p : f) cudaFree(p);
     for (int a = 0; a < 6; a++) { cudaFree(c->eps[a]); cudaFree(c->sig[a]); }
+    for (int v = 0; v < 4; v++) cudaFree(c->guess[v]);
     if (c->hstage) cudaFreeHost(c->hstage);
     if (c->tev[0]) { cudaEventDestroy(c->tev[0]); cudaEventDestroy(c->tev[1]); }
     delete[] c->hgx; delete[] c->hgy; delete[] c->hgz;
@@ -389,6 +390,15 @@ int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, doubl
     if (kind == 4 || kind == 5) return i3g::markers_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
     if (kind == 6) return i3g::heat_time_kernel(c, reps, ms_per_launch, bytes_per_launch);
     return i3g::stokes_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
+}
+
+int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default)
+{
+    if (!c) return I3G_E_ARG;
+    if (used) *used = c->guess_used;
+    if (rel_guess) *rel_guess = c->guess_rel[0];
+    if (rel_default) *rel_default = c->guess_rel[1];
+    return 0;
 }
 
 int i3g_timer(i3g_ctx *c, int op, double *ms)

@@ -156,6 +156,12 @@ struct i3g_ctx {
     double *hist[2][4] = {};                    // last two converged level-0 solutions (warm_start 2)
     double hist_dt[2] = {0, 0};                 // time steps taken after them
     int nhist = 0;
+    // staged start for the next Stokes solve (i3g_unet_predict); kept only when its relative
+    // residual is below the default start's
+    double *guess[4] = {};
+    int guess_pending = 0;
+    int guess_used = -1;                        // last solve: -1 none staged, 0 rejected, 1 used
+    double guess_rel[2] = {0, 0};               // relative residual of the staged / default start
     void *kry = nullptr;       // FGMRES state of the mixed-precision Stokes solve
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state

@@ -2008,6 +2008,32 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     int multinum = c->f.multinum > 0 ? std::min(c->f.multinum, c->nlev - 1) : std::min(c->p.multimax, c->nlev - 1);
     double mom, cont;
     if ((rc = stokes_relres(c, &mom, &cont))) return rc;
+    c->guess_used = -1;
+    if (c->guess_pending) {
+        // a staged (learned) start competes with the default one: keep the lower residual.
+        // The residual arrays are free here (the norms are computed on the fly), so they hold
+        // the default start meanwhile.
+        c->guess_pending = 0;
+        const double dmom = mom, dcont = cont;
+        for (int v = 0; v < 4; v++) {
+            I3G_CUDA(cudaMemcpyAsync(L0.d.r[v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+            I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], c->guess[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+        }
+        for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
+        double gm, gc;
+        if ((rc = stokes_relres(c, &gm, &gc))) return rc;
+        const double rg = std::max(gm, gc), rdef = std::max(dmom, dcont);
+        c->guess_rel[0] = rg;
+        c->guess_rel[1] = rdef;
+        c->guess_used = rg < rdef ? 1 : 0;   // false for a NaN guess too
+        if (c->guess_used) {
+            mom = gm;
+            cont = gc;
+        } else {
+            for (int v = 0; v < 4; v++)
+                I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], L0.d.r[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+        }
+    }
     c->st_.stokes_rel0 = std::max(mom, cont);
     int cycles = 0, outer = 0;
     bool conv = mom <= rtol && cont <= rtol;

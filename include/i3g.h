@@ -216,6 +216,56 @@ int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, doubl
  * the stop event, waits for it and returns the elapsed milliseconds in *ms. */
 int i3g_timer(i3g_ctx *c, int op, double *ms);
 
+/* ---- learned warm start: 3-D U-Net (no counterpart in the reference) ---------------- */
+/* The reference starts every Stokes solve from the previous step's v, P
+ * (move3mg.c:1969-2019).  The network maps log10 viscosity, density and that previous
+ * velocity on the level-0 node grid to a correction (dP, dVx, dVy, dVz) of that start; the
+ * solver keeps the corrected start only when its relative residual is lower and then iterates
+ * to the same tolerance, so the network changes the cycle count, never the converged answer.
+ * 4 levels of 16/32/64/128 channels, 15 convolutions of 3x3x3 on tcgen05 tensor cores (BF16
+ * operands, FP32 accumulation), Adam on FP32 master weights.  Every grid axis needs n >= 9
+ * and n-1 divisible by 8.  Host arrays of nodal data are planar in the solver's node order
+ * (node = z*nx*ny + x*ny + y): in5 = [5][n] log10 eta, rho, vx, vy, vz; tg4 / out4 = [4][n]
+ * dP, dVx, dVy, dVz.  The handle owns its device memory and its own stream; calls that take a
+ * context first wait for the context's stream.  Errors: i3g_last_error(NULL). */
+typedef struct i3g_unet i3g_unet;
+/* capacity: training samples kept on the device (36 bytes per node each). */
+int i3g_unet_create(int nx, int ny, int nz, int capacity, uint64_t seed, i3g_unet **out);
+void i3g_unet_destroy(i3g_unet *u);
+int i3g_unet_nparams(const i3g_unet *u, int64_t *n);
+/* Flat FP32 parameters: per layer W[27][cout][cin] (tap = (dz+1)*9 + (dx+1)*3 + (dy+1)) then b[cout]. */
+int i3g_unet_get_params(i3g_unet *u, float *host, int64_t n);
+int i3g_unet_set_params(i3g_unet *u, const float *host, int64_t n);   /* also resets Adam */
+/* s = {log10-eta mean, 1/std, rho mean, 1/std, velocity scale, pressure scale} */
+int i3g_unet_set_scales(i3g_unet *u, const float s[6]);
+int i3g_unet_set_sample(i3g_unet *u, int slot, const float *in5, const float *tg4);
+int i3g_unet_get_sample(i3g_unet *u, int slot, float *in5, float *tg4);
+/* Record the inputs of c's next Stokes solve (before i3g_stokes) and, after it, the target:
+ * converged v, P minus that start. */
+int i3g_unet_capture_input(i3g_unet *u, i3g_ctx *c, int slot);
+int i3g_unet_capture_target(i3g_unet *u, i3g_ctx *c, int slot);
+/* One Adam step on the mean loss of the listed samples; *loss = that mean before the step. */
+int i3g_unet_train_step(i3g_unet *u, const int *slots, int nslots, float lr, double *loss);
+int i3g_unet_loss(i3g_unet *u, const int *slots, int nslots, double *loss);
+/* Host data in and out: out4 = correction for in5; with tg4, *loss and (grads != NULL) the
+ * parameter gradients of that one sample's loss. */
+int i3g_unet_eval_host(i3g_unet *u, const float *in5, const float *tg4, float *out4, float *grads, double *loss);
+/* Stage previous v, P + correction as the start of c's next i3g_stokes (see i3g_stokes_guess_info). */
+int i3g_unet_predict(i3g_unet *u, i3g_ctx *c);
+/* Mean device time of one training step on sample slot 0 and of one forward pass. */
+int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward);
+/* Mean device time of the forward convolution of layer 0..14 (inputs of the last forward
+ * pass) and its algorithmic bytes (interior rows of input, output and skip tensor, weights). */
+int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *bytes);
+/* One tensor-core convolution on host BF16 bit patterns over a padded (nz+2)(nx+2)(ny+2) grid:
+ * in [rows][cin], w [27][cout][cin], bias [cout] or NULL, add [rows][cout] or NULL; out FP32
+ * [rows][cout], interior rows only.  cin, cout in {16, 32, 64, 128} as the network pairs them. */
+int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *in, const uint16_t *w,
+                       const float *bias, const uint16_t *add, int relu, float *out);
+/* Last i3g_stokes: used = -1 no staged start, 0 rejected, 1 used; relative residuals of the
+ * staged and of the default start. */
+int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default);
+
 /* ---- allocation-free stopping test (no counterpart in the reference) --------------- */
 /* For host codes that may not allocate device memory after start-up (they give all of it
  * to their own pool allocator, or cannot let a cudaMalloc synchronise the device under work

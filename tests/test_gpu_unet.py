@@ -1,0 +1,117 @@
+"""Learned warm start on the GPU, through the C ABI (i3g_unet_*), against the CPU oracle
+oracle/unet_ref.py: the tcgen05 convolution, the network's output and its parameter
+gradients; then a small training run that must lower the loss and give held-out Stokes
+solves a better start than the default one."""
+import numpy as np
+import pytest
+
+import unet_ref as U
+
+pytestmark = pytest.mark.gpu
+
+PAIRS = [(16, 16), (16, 32), (32, 16), (32, 32), (32, 64), (64, 32), (64, 64), (64, 128), (128, 64), (128, 128)]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    torch.cuda.set_device(0)
+
+
+def _rows(x):
+    """[nz, nx, ny, C] interior -> padded rows [(nz+2)(nx+2)(ny+2), C]."""
+    return np.pad(x, ((1, 1), (1, 1), (1, 1), (0, 0))).reshape(-1, x.shape[3])
+
+
+@pytest.mark.parametrize("cin,cout", PAIRS)
+def test_conv_matches_oracle(cin, cout):
+    from i3elvis_b200 import warmstart as W
+    rng = np.random.default_rng(cin * 1000 + cout)
+    dims = (9, 7, 11)     # 11*9*13 = 1287 padded rows: ten 128-row tiles and a partial one
+    x = U.bf16(rng.normal(size=dims + (cin,)))
+    w = U.bf16(rng.normal(0, 1 / np.sqrt(27 * cin), size=(27, cout, cin)))
+    b = rng.normal(0, 0.1, size=cout).astype(np.float32)
+    add = U.bf16(rng.normal(0, 0.5, size=dims + (cout,)))
+    out = W.conv_host(cin, cout, dims, U.bf16_bits(_rows(x)), U.bf16_bits(w), b, U.bf16_bits(_rows(add)), relu=True)
+    ref = np.maximum(U.conv3(x, w, b.astype(np.float64)) + add, 0.0)
+    got = out.reshape(dims[0] + 2, dims[1] + 2, dims[2] + 2, cout)
+    inner = got[1:-1, 1:-1, 1:-1]
+    # FP32 accumulation of <= 27*128 products against float64
+    assert np.max(np.abs(inner - ref)) <= 2e-5 * np.max(np.abs(ref)) + 1e-6
+    # rows of the zero halo are not written
+    halo = got.copy()
+    halo[1:-1, 1:-1, 1:-1] = 0
+    assert not np.any(halo)
+
+
+def _sample(dims, seed):
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(dims))
+    nz, nx, ny = dims
+    # smooth-ish fields so that every level sees structure
+    zz, xx, yy = np.meshgrid(np.linspace(0, 1, nz), np.linspace(0, 1, nx), np.linspace(0, 1, ny), indexing="ij")
+    le = 21 + 2 * np.sin(3 * xx + 2 * yy) * np.cos(2 * zz) + 0.3 * rng.normal(size=dims)
+    ro = 3300 + 80 * np.cos(4 * yy + xx) + 10 * rng.normal(size=dims)
+    v = [1e-10 * np.sin(k + 3 * xx * yy + zz) for k in range(3)]
+    in5 = np.stack([le.ravel(), ro.ravel()] + [a.ravel() for a in v]).astype(np.float32)
+    tg4 = np.stack([1e6 * np.cos(2 * xx + zz).ravel()] + [2e-10 * np.cos(k + xx + 2 * zz).ravel() for k in range(3)])
+    return in5, tg4.astype(np.float32), n
+
+
+def test_network_output_and_gradients_match_oracle():
+    from i3elvis_b200.warmstart import UNet
+    dims = (9, 17, 9)      # nz, nx, ny
+    scales = (21.0, 0.5, 3300.0, 0.0125, 1e-10, 1e6)
+    par = U.init_params(seed=11)
+    net = UNet(dims[1], dims[2], dims[0], capacity=1, seed=3)
+    assert net.nparams == par.size
+    net.set_params(par)
+    net.set_scales(*scales)
+    assert np.array_equal(net.get_params(), par)
+    in5, tg4, n = _sample(dims, 12)
+    out4, loss, g = net.eval_host(in5, tg4, grads=True)
+    ref = U.Net(par, dims, scales, round_bf16=True)
+    out_ref = ref.output(in5)
+    loss_ref, g_ref = ref.loss_grads(in5, tg4)
+    err = np.linalg.norm(out4 - out_ref) / np.linalg.norm(out_ref)
+    assert err < 3e-2, err
+    assert abs(loss - loss_ref) <= 2e-2 * loss_ref, (loss, loss_ref)
+    offs, _ = U.param_offsets()
+    worst = 0.0
+    for li, ((w, b), (cin, cout)) in enumerate(zip(offs, U.layer_shapes())):
+        gw, gr = g[w:w + 27 * cin * cout], g_ref[w:w + 27 * cin * cout]
+        e = np.linalg.norm(gw - gr) / max(np.linalg.norm(gr), 1e-30)
+        worst = max(worst, e)
+        assert e < 1e-1, (li, e)
+        eb = np.linalg.norm(g[b:b + cout] - g_ref[b:b + cout]) / max(np.linalg.norm(g_ref[b:b + cout]), 1e-30)
+        assert eb < 1e-1, (li, eb)
+    assert np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref) < 5e-2
+    # padded input channels never receive a gradient
+    g0 = g[:27 * 16 * 16].reshape(27, 16, 16)
+    assert not np.any(g0[:, :, U.IN_CH:])
+    # the same sample through the device data set gives the same loss
+    net.set_sample(0, in5, tg4)
+    assert abs(net.loss([0]) - loss) <= 1e-6 * loss
+
+
+def test_training_lowers_loss_and_improves_held_out_starts():
+    from i3elvis_b200 import learned
+    from i3elvis_b200.warmstart import UNet
+    case = learned.Case(n=17, mnum=2, count=8, r_km=(15.0, 35.0))
+    steps = 1
+    net = UNet(case.n, case.n, case.n, capacity=32 * steps, seed=2)
+    slots = learned.record(net, case, range(100, 132), steps)
+    learned.fit_scales(net, slots)
+    hist = learned.train(net, slots, iters=400, batch=4, lr=2e-3)
+    first, last = float(np.mean(hist[:10])), float(np.mean(hist[-20:]))
+    assert last < 0.5 * first, (first, last)
+    rows = learned.compare(net, case, range(900, 906), steps)
+    s = learned.summarize(rows)["step0"]
+    print("learned warm start, 17^3 held-out cold starts:", s)
+    # the learned start is accepted on most held-out models and lowers the starting residual
+    assert s["guess_used"] >= 4, s
+    assert s["rel0_learned_guess"] < 0.9 * s["rel0_default"], s
+    # the solve still reaches the tolerance, in no more V-cycles on average
+    assert s["learned_cycles"] <= s["default_cycles"] + 0.5, s
