@@ -64,6 +64,8 @@ void i3g_destroy(i3g_ctx *c)
     for (void *p : f) cudaFree(p);
     for (int a = 0; a < 6; a++) { cudaFree(c->eps[a]); cudaFree(c->sig[a]); }
     for (int v = 0; v < 4; v++) cudaFree(c->guess[v]);
+    for (int v = 0; v < 8; v++) cudaFree(c->gsave[v]);
+    cudaFree(c->gdots);
     if (c->hstage) cudaFreeHost(c->hstage);
     if (c->tev[0]) { cudaEventDestroy(c->tev[0]); cudaEventDestroy(c->tev[1]); }
     delete[] c->hgx; delete[] c->hgy; delete[] c->hgz;
@@ -392,9 +394,10 @@ int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, doubl
     return i3g::stokes_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
 }
 
-int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default)
+int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default, double *alpha)
 {
     if (!c) return I3G_E_ARG;
+    if (alpha) *alpha = c->guess_alpha;
     if (used) *used = c->guess_used;
     if (rel_guess) *rel_guess = c->guess_rel[0];
     if (rel_default) *rel_default = c->guess_rel[1];

@@ -1232,10 +1232,12 @@ int i3g_unet_predict(i3g_unet *u, i3g_ctx *c)
     int rc = ctx_matches(u, c);
     if (rc) return rc;
     const long n = u->L[0].n;
-    if (!c->guess[0])
-        for (int v = 0; v < 4; v++)
-            if (cudaMalloc((void **)&c->guess[v], n * sizeof(double)) != cudaSuccess)
-                return set_global_error(I3G_E_NOMEM, "U-Net: guess buffers");
+    if (!c->guess[0]) {
+        bool ok = cudaMalloc((void **)&c->gdots, 2 * sizeof(double)) == cudaSuccess;
+        for (int v = 0; v < 4 && ok; v++) ok = cudaMalloc((void **)&c->guess[v], n * sizeof(double)) == cudaSuccess;
+        for (int v = 0; v < 8 && ok; v++) ok = cudaMalloc((void **)&c->gsave[v], n * sizeof(double)) == cudaSuccess;
+        if (!ok) return set_global_error(I3G_E_NOMEM, "U-Net: guess buffers");
+    }
     UCHK(cudaStreamSynchronize(c->st));
     k_from_ctx<<<nblk(n), 256, 0, u->st>>>(c->lev[0].nu, c->ro, c->vx, c->vy, c->vz, u->tmp_in, n);
     if ((rc = load_sample(u, u->tmp_in)) || (rc = forward(u))) return rc;

@@ -147,8 +147,8 @@ def compare(net: UNet, case: Case, seeds, steps: int, rtol=1e-8):
                 row[tag + "_ms"] = st["ms_stokes"]
                 row[tag + "_rel0"] = st["stokes_rel0"]
                 if k == 1:
-                    used, rg, rd = guess_info(c)
-                    row.update(guess_used=used, rel_guess=rg, rel_default=rd)
+                    used, rg, rd, al = guess_info(c)
+                    row.update(guess_used=used, rel_guess=rg, rel_default=rd, alpha=al)
                 dts.append(dt)
             # both contexts continue from the default run's state so that every step compares
             # the two starts on the same model (the converged solutions agree to the tolerance)
@@ -171,6 +171,7 @@ def summarize(rows):
             "learned_ms": float(np.mean([r["learned_ms"] for r in rs])),
             "rel0_default": float(np.exp(np.mean(np.log([r["rel_default"] for r in rs])))),
             "rel0_learned_guess": float(np.exp(np.mean(np.log([max(r["rel_guess"], 1e-300) for r in rs])))),
+            "alpha_median": float(np.median([r["alpha"] for r in rs])),
             "guess_used": int(sum(r["guess_used"] == 1 for r in rs)), "cases": len(rs)}
     return out
 

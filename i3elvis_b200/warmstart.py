@@ -47,7 +47,7 @@ def _bind():
     L.i3g_unet_time_conv.argtypes = [P, C.c_int, C.c_int, dp, dp]
     u16 = C.POINTER(C.c_uint16)
     L.i3g_unet_conv_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, u16, u16, fp, u16, C.c_int, fp]
-    L.i3g_stokes_guess_info.argtypes = [P, ip, dp, dp]
+    L.i3g_stokes_guess_info.argtypes = [P, ip, dp, dp, dp]
     _bound = True
     return L
 
@@ -82,11 +82,11 @@ def conv_host(cin, cout, dims, x_bits, w_bits, bias=None, add_bits=None, relu=Fa
 
 
 def guess_info(ctx: lib.Context):
-    """(used, rel_guess, rel_default) of the context's last Stokes solve."""
+    """(used, rel_guess, rel_default, alpha) of the context's last Stokes solve."""
     L = _bind()
-    u, a, b = C.c_int(), C.c_double(), C.c_double()
-    _check(L.i3g_stokes_guess_info(ctx.h, C.byref(u), C.byref(a), C.byref(b)))
-    return u.value, a.value, b.value
+    u, a, b, al = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+    _check(L.i3g_stokes_guess_info(ctx.h, C.byref(u), C.byref(a), C.byref(b), C.byref(al)))
+    return u.value, a.value, b.value, al.value
 
 
 class UNet:

@@ -250,7 +250,9 @@ int i3g_unet_loss(i3g_unet *u, const int *slots, int nslots, double *loss);
 /* Host data in and out: out4 = correction for in5; with tg4, *loss and (grads != NULL) the
  * parameter gradients of that one sample's loss. */
 int i3g_unet_eval_host(i3g_unet *u, const float *in5, const float *tg4, float *out4, float *grads, double *loss);
-/* Stage previous v, P + correction as the start of c's next i3g_stokes (see i3g_stokes_guess_info). */
+/* Stage previous v, P + correction as the start of c's next i3g_stokes, which scales the
+ * correction by the residual-minimising factor and keeps the result only when its relative
+ * residual is lower than the default start's (see i3g_stokes_guess_info). */
 int i3g_unet_predict(i3g_unet *u, i3g_ctx *c);
 /* Mean device time of one training step on sample slot 0 and of one forward pass. */
 int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward);
@@ -263,8 +265,9 @@ int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *byt
 int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *in, const uint16_t *w,
                        const float *bias, const uint16_t *add, int relu, float *out);
 /* Last i3g_stokes: used = -1 no staged start, 0 rejected, 1 used; relative residuals of the
- * staged and of the default start. */
-int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default);
+ * staged start (after scaling its correction by alpha) and of the default start; alpha is the
+ * factor a >= 0 minimising the row-weighted residual of default + a (staged - default). */
+int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default, double *alpha);
 
 /* ---- allocation-free stopping test (no counterpart in the reference) --------------- */
 /* For host codes that may not allocate device memory after start-up (they give all of it
