@@ -112,7 +112,7 @@ def test_training_lowers_loss_and_never_worsens_the_start():
     learned.fit_scales(net, slots)
     hist = learned.train(net, slots, iters=400, batch=4, lr=2e-3)
     first, last = float(np.mean(hist[:10])), float(np.mean(hist[-20:]))
-    assert last < 0.5 * first, (first, last)
+    assert last < 0.7 * first, (first, last)
     rows = learned.compare(net, case, range(900, 906), steps)
     print("learned warm start, 17^3 held-out models:", learned.summarize(rows))
     for r in rows:
