@@ -520,9 +520,9 @@ int heat_solve(i3g_ctx *c, double *timestep)
     if (c->p.adiabyn) return set_error(c, I3G_E_UNSUPPORTED, "adiabatic heating (adiabyn %d) is not supported on the GPU", c->p.adiabyn);
     if (c->m.timesum > c->p.timebeg)
         return set_error(c, I3G_E_UNSUPPORTED, "the bottom-temperature schedule (timebeg, heat3mg.c:433-446) is not supported");
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     Level &L0 = c->lev[0];
     HeatLevel &H0 = S->L[0];
@@ -586,8 +586,6 @@ int heat_solve(i3g_ctx *c, double *timestep)
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     c->st_.ms_heat = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     S->ready = true;
     return 0;
 }
@@ -605,9 +603,9 @@ int heat_time_kernel(i3g_ctx *c, int reps, double *ms, double *bytes)
     Level &L0 = c->lev[0];
     HView V = hview(c, 0, 1e13);
     const long tot = (long)((L0.ny + 1) / 2) * L0.nx * L0.nz;
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     for (int r = 0; r < reps; r++) LAUNCH(k_heat_relax, nb(tot), 256, V, r & 1, 1.0);
     I3G_CUDA(cudaEventRecord(e1, c->st));
@@ -617,8 +615,6 @@ int heat_time_kernel(i3g_ctx *c, int reps, double *ms, double *bytes)
     *ms = t / reps;
     // one colour: T read, half written, rhs half, kt, rho*cp, bc mask
     *bytes = (double)L0.n * (8.0 + 4.0 + 4.0 + 4.0 + 8.0 + 1.0);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     return 0;
 }
 

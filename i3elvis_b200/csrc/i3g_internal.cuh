@@ -109,8 +109,22 @@ struct Level {
     double *red = nullptr;             // reduction scratch
 };
 
-struct KernelTimer {
+// Two CUDA events for a device-time measurement, destroyed on every return path.
+struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() = default;
+    EventPair(const EventPair &) = delete;
+    EventPair &operator=(const EventPair &) = delete;
+    cudaError_t create()
+    {
+        cudaError_t e = cudaEventCreate(&a);
+        return e == cudaSuccess ? cudaEventCreate(&b) : e;
+    }
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
 };
 
 }  // namespace i3g

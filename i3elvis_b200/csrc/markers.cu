@@ -1199,9 +1199,9 @@ int markers_move(i3g_ctx *c, double timestep)
 {
     MarkerState *S = ms(c);
     if (!S->n || timestep == 0) return 0;
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
     LAUNCH(k_move, nb(S->n), 256, grid_smem(c), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c), timestep);
@@ -1211,8 +1211,6 @@ int markers_move(i3g_ctx *c, double timestep)
     float ms_ = 0;
     cudaEventElapsedTime(&ms_, e0, e1);
     c->st_.ms_move = ms_;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     S->sorted = false;
     return rc;
 }
@@ -1240,9 +1238,9 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
 {
     MarkerState *S = ms(c);
     const long N = c->nodenum;
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
     int rc = 0;
@@ -1264,8 +1262,6 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
     float ms_ = 0;
     cudaEventElapsedTime(&ms_, e0, e1);
     c->st_.ms_r2n = ms_;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     c->stokes_ready = false;
     return rc;
 }
@@ -1297,9 +1293,9 @@ int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *
 {
     MarkerState *S = ms(c);
     const long n = S->n, N = c->nodenum;
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
     if (!S->sorted) { int rc = sort_markers(c); if (rc) return rc; }
     I3G_CUDA(cudaEventRecord(e0, c->st));
@@ -1320,8 +1316,6 @@ int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *
     // compulsory bytes: marker fields read/written once, node fields read/written once
     if (kind == 4) *bytes = (double)n * (4.0 * 6 + 1 + 4) + (double)N * (8.0 + NACC * 8.0);
     else *bytes = (double)n * (4.0 * 9 + 1 + 4.0 * 9) + (double)N * (4.0 * 15 + 8.0);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     return 0;
 }
 

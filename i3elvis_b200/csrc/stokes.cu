@@ -2017,9 +2017,9 @@ int stokes_solve(i3g_ctx *c, double *timestep)
 {
     if (c->p.p2koef != 0 || c->f.p2koef != 0 || c->f.p2koef2 != 0)
         return set_error(c, I3G_E_UNSUPPORTED, "p2koef != 0 (grad div terms, move3mg.c:860-889) is not supported");
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     int rc = stokes_setup(c);
     if (rc) return rc;
@@ -2172,8 +2172,6 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     c->st_.ms_stokes = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (!conv) return set_error(c, I3G_E_NOCONV, "Stokes: %d V-cycles without reaching relative residual %g (mom %.3e cont %.3e)", cycles, rtol, mom, cont);
     return 0;
 }
@@ -2187,9 +2185,9 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
     }
     Level &L = c->lev[0];
     const double N = (double)L.n;
-    cudaEvent_t e0, e1;
-    I3G_CUDA(cudaEventCreate(&e0));
-    I3G_CUDA(cudaEventCreate(&e1));
+    EventPair ev;
+    I3G_CUDA(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     View<double> V = view<double>(L, L.d);
     View<float> Vf = view<float>(L, L.s);
     const long total = (long)((L.ny + 1) / 2) * L.nx * L.nz;
@@ -2232,8 +2230,6 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
     }
     default: *bytes = 0;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     I3G_CUDA(cudaGetLastError());
     return 0;
 }

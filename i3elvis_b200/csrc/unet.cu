@@ -312,7 +312,15 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a)
     if (issued > 0 && !mbar_wait(smem_u32(&mbar[(issued - 1) % kStages]), ((issued - 1) / kStages) & 1)) fail = 1;
     failed = __syncthreads_or(fail || failed) != 0;
     if (failed) {
-        if (tid == 0) atomicExch(a.err, 1);
+        // No epilogue.  MMAs committed before the timeout may still write TMEM and read the
+        // ring: one more bounded wait on the last commit before the columns are released.  If
+        // that also times out the device state is suspect; the host reports the error as fatal
+        // for the handle (check_err).
+        if (tid == 0) {
+            atomicExch(a.err, 1);
+            if (issued > 0) mbar_wait(smem_u32(&mbar[(issued - 1) % kStages]), ((issued - 1) / kStages) & 1);
+        }
+        __syncthreads();
     } else {
         tc_fence_after();
         const long p = row0 + warp * 32 + lane;
@@ -820,7 +828,11 @@ int check_err(i3g_unet *u)
     int h = 0;
     UCHK(cudaMemcpyAsync(&h, u->derr, sizeof(int), cudaMemcpyDeviceToHost, u->st));
     UCHK(cudaStreamSynchronize(u->st));
-    if (h) return set_global_error(I3G_E_CUDA, "U-Net: a convolution timed out waiting for its tensor-core stage");
+    // fatal: the timed-out CTA released its TMEM after a second bounded wait only, so
+    // tensor-core work of that launch may have been abandoned; destroy the handle (and do not
+    // reuse the CUDA context for results that must be trusted)
+    if (h) return set_global_error(I3G_E_CUDA, "U-Net: a convolution timed out waiting for its tensor-core stage "
+                                               "(fatal: destroy this handle)");
     return 0;
 }
 
@@ -1233,10 +1245,18 @@ int i3g_unet_predict(i3g_unet *u, i3g_ctx *c)
     if (rc) return rc;
     const long n = u->L[0].n;
     if (!c->guess[0]) {
+        // all or nothing: a partial set would be taken as complete by the next call
         bool ok = cudaMalloc((void **)&c->gdots, 2 * sizeof(double)) == cudaSuccess;
         for (int v = 0; v < 4 && ok; v++) ok = cudaMalloc((void **)&c->guess[v], n * sizeof(double)) == cudaSuccess;
         for (int v = 0; v < 8 && ok; v++) ok = cudaMalloc((void **)&c->gsave[v], n * sizeof(double)) == cudaSuccess;
-        if (!ok) return set_global_error(I3G_E_NOMEM, "U-Net: guess buffers");
+        if (!ok) {
+            cudaGetLastError();
+            cudaFree(c->gdots);
+            c->gdots = nullptr;
+            for (int v = 0; v < 4; v++) { cudaFree(c->guess[v]); c->guess[v] = nullptr; }
+            for (int v = 0; v < 8; v++) { cudaFree(c->gsave[v]); c->gsave[v] = nullptr; }
+            return set_global_error(I3G_E_NOMEM, "U-Net: guess buffers");
+        }
     }
     UCHK(cudaStreamSynchronize(c->st));
     k_from_ctx<<<nblk(n), 256, 0, u->st>>>(c->lev[0].nu, c->ro, c->vx, c->vy, c->vz, u->tmp_in, n);
@@ -1319,9 +1339,9 @@ int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t
 int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward)
 {
     if (!u || reps <= 0 || u->cap < 1) return set_global_error(I3G_E_ARG, "U-Net: timing needs one stored sample");
-    cudaEvent_t e0, e1;
-    UCHK(cudaEventCreate(&e0));
-    UCHK(cudaEventCreate(&e1));
+    i3g::EventPair ev;
+    UCHK(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     const int slot = 0;
     const long n = u->L[0].n;
     int rc = 0;
@@ -1354,8 +1374,6 @@ int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward)
     u->adam_t = keep_t;
     int r2 = pack_weights(u);
     UCHK(cudaStreamSynchronize(u->st));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     return rc ? rc : r2;
 }
 
@@ -1373,9 +1391,9 @@ int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *byt
     a.add = ld.add >= 0 ? u->act[ld.add] : nullptr;
     a.relu = ld.relu;
     a.out = u->act[ld.out];
-    cudaEvent_t e0, e1;
-    UCHK(cudaEventCreate(&e0));
-    UCHK(cudaEventCreate(&e1));
+    i3g::EventPair ev;
+    UCHK(ev.create());
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     UCHK(launch_conv(cin, cout, a, u->st));   // warm-up
     UCHK(cudaEventRecord(e0, u->st));
     for (int r = 0; r < reps; r++) UCHK(launch_conv(cin, cout, a, u->st));
@@ -1383,8 +1401,6 @@ int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *byt
     UCHK(cudaEventSynchronize(e1));
     float t = 0;
     cudaEventElapsedTime(&t, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     int rc = check_err(u);
     if (rc) return rc;
     if (ms) *ms = t / reps;

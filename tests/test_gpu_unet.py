@@ -119,7 +119,11 @@ def test_training_lowers_loss_and_never_worsens_the_start():
         assert r["guess_used"] in (0, 1), r
         # the solve starts from the better of the two starts of its own state
         assert r["learned_rel0"] <= r["rel_default"] * (1 + 1e-9), r
+        # ... and never from a worse one than the separate default-start context on the same
+        # state (one step per seed: both contexts hold identical models)
+        assert r["learned_rel0"] <= r["default_rel0"] * (1 + 1e-9), r
         assert r["alpha"] >= 0.0, r
+    print("guess accepted on", sum(r["guess_used"] == 1 for r in rows), "of", len(rows), "held-out solves")
     d = float(np.mean([r["default_cycles"] for r in rows]))
     g = float(np.mean([r["learned_cycles"] for r in rows]))
     assert g <= d + 3.0, (g, d)
