@@ -380,6 +380,12 @@ int i3g_stokes_vcycles(i3g_ctx *c, int ncycles)
     return 0;
 }
 
+int i3g_stokes_stresses(i3g_ctx *c)
+{
+    if (!c) return I3G_E_ARG;
+    return i3g::stokes_stresses(c);
+}
+
 int i3g_stokes_relres(i3g_ctx *c, double *mom_rel, double *cont_rel)
 {
     if (!c || !mom_rel || !cont_rel) return I3G_E_ARG;

@@ -201,6 +201,7 @@ int stokes_restrict(i3g_ctx *c, int level);
 int stokes_prolong(i3g_ctx *c, int level);
 int stokes_vcycle(i3g_ctx *c, int multinum);
 int stokes_relres(i3g_ctx *c, double *mom, double *cont);
+int stokes_stresses(i3g_ctx *c);
 int stokes_solve(i3g_ctx *c, double *timestep);
 int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes);
 }  // namespace i3g

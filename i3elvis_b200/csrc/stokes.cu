@@ -1529,6 +1529,28 @@ __global__ void k_eps_sig(int nx, int ny, int nz, const float *vx, const float *
     }
 }
 
+// strain rates and stresses of the level-0 FP32 velocities into c->eps / c->sig
+static void eps_sig_launch(i3g_ctx *c)
+{
+    Level &L = c->lev[0];
+    LAUNCH(k_eps_sig, nblk(L.n), 256, L.nx, L.ny, L.nz, (const float *)c->vx, (const float *)c->vy, (const float *)c->vz,
+           (const double *)L.d.etac, (const double *)L.d.etaxy, (const double *)L.d.etaxz, (const double *)L.d.etayz,
+           (const double *)L.d.ix[0], (const double *)L.d.ix[1], (const double *)L.d.iy[0], (const double *)L.d.iy[1],
+           (const double *)L.d.iz[0], (const double *)L.d.iz[1], c->deps, c->dsig);
+}
+
+// sxxcalc..syzcalc with ynval = 0 (move3mg.c:3-710) for the current nodal velocities and
+// viscosities, as vpiterate recomputes them after its iterations (move3mg.c:2405-2555)
+int stokes_stresses(i3g_ctx *c)
+{
+    int rc = stokes_setup(c);
+    if (rc) return rc;
+    eps_sig_launch(c);
+    I3G_CUDA(cudaGetLastError());
+    I3G_CUDA(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
 static int finish_solve(i3g_ctx *c, double *timestep)
 {
     Level &L = c->lev[0];
@@ -1537,10 +1559,7 @@ static int finish_solve(i3g_ctx *c, double *timestep)
     const int nb = c->red_blocks;
     LAUNCH(k_copy_back, nb, 256, V, pin, c->m.pinit, c->pr, c->vx, c->vy, c->vz, c->dred);
     I3G_CUDA(cudaMemcpyAsync(c->hstage, c->dred, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, c->st));
-    LAUNCH(k_eps_sig, nblk(L.n), 256, L.nx, L.ny, L.nz, (const float *)c->vx, (const float *)c->vy, (const float *)c->vz,
-           (const double *)L.d.etac, (const double *)L.d.etaxy, (const double *)L.d.etaxz, (const double *)L.d.etayz,
-           (const double *)L.d.ix[0], (const double *)L.d.ix[1], (const double *)L.d.iy[0], (const double *)L.d.iy[1],
-           (const double *)L.d.iz[0], (const double *)L.d.iz[1], c->deps, c->dsig);
+    eps_sig_launch(c);
     I3G_CUDA(cudaStreamSynchronize(c->st));
     double vm[4] = {0, 0, 0, -1e300};
     for (int b = 0; b < nb; b++)

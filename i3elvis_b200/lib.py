@@ -51,6 +51,7 @@ def load():
     L.i3g_get_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
     L.i3g_set_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
     L.i3g_stokes_setup.argtypes = [P]
+    L.i3g_stokes_stresses.argtypes = [P]
     for name in ("i3g_stokes_residual", "i3g_stokes_restrict", "i3g_stokes_prolong", "i3g_stokes_vcycles"):
         getattr(L, name).argtypes = [P, C.c_int]
     L.i3g_stokes_smooth.argtypes = [P, C.c_int, C.c_int]

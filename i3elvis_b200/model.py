@@ -212,9 +212,19 @@ class ModelSpec:
     t_top: float = 273.0
     t_bottom: float = 1573.0
     multinum: int = 2
+    stretch: float = 0.0     # 0: uniform grid lines; a in (0, 1): spacing (1 - a cos(2 pi s)) * size/(n-1)
 
 
-def _uniform_grid(n, size):
+def _grid(n, size, stretch=0.0):
+    """Grid lines from 0 to size: uniform as in in3mg.c:96-101, or (stretch = a > 0) the smooth
+    non-uniform map x(s) = size * (s - a sin(2 pi s) / (2 pi)), s = i/(n-1), whose spacing grows
+    from (1 - a) h at the walls to (1 + a) h in the middle -- the reference keeps arbitrary grid
+    lines in the .prn file (load3mg.c:739-751) and every formula uses them."""
+    if stretch:
+        s = np.arange(n, dtype=np.float64) / (n - 1)
+        g = size * (s - stretch * np.sin(2 * np.pi * s) / (2 * np.pi))
+        g[0], g[-1] = 0.0, size
+        return g.astype(np.float32)
     step = size / (n - 1)
     g = np.zeros(n)
     for i in range(1, n):
@@ -271,7 +281,7 @@ def make_prn(spec: ModelSpec, rocks: dict, types: np.ndarray, marks_xyz, seed: i
     nx, ny, nz = spec.shape
     x, y, z = marks_xyz
     nmark = x.size
-    gx, gy, gz = (_uniform_grid(n, s) for n, s in zip(spec.shape, spec.size))
+    gx, gy, gz = (_grid(n, s, spec.stretch) for n, s in zip(spec.shape, spec.size))
     rocknum = max(rocks) + 1
     rtab = {f: np.zeros(rocknum) for f in ROCK_FIELDS}
     for t, r in rocks.items():
@@ -307,16 +317,26 @@ MATRIX, SPHERE = 2, 3
 INCLUSION_TYPES = (3, 4, 5, 6, 9, 10, 11, 12, 13, 14, 15, 19)
 
 
-def sinking_sphere(n=33, size_km=100.0, mnum=3, multinum=2, seed=1, radius_km=20.0):
+def sinking_sphere(n=33, size_km=100.0, mnum=3, multinum=2, seed=1, radius_km=20.0, stretch=0.0,
+                   sphere_rho=3400.0, centre_frac=(0.5, 0.5, 0.5), plastic=None):
     """Plain sinking sphere: eta 1e23 / rho 3400 sphere in eta 1e21 / rho 3300 matrix,
-    g = 10 along the vertical, free slip, linear T 273 -> 1573 K, k = 3, cp = 1000."""
+    g = 10 along the vertical, free slip, linear T 273 -> 1573 K, k = 3, cp = 1000.
+
+    ``stretch`` makes the grid lines non-uniform (see ``_grid``); ``plastic = (a, b)`` gives the
+    matrix Drucker-Prager yielding sigma_y = a + b P (rock columns a0 = a1 = a, b0 = b1 = b,
+    viscalc's brittle branch, mark3mg.c:1148-1198)."""
     L = size_km * 1e3
-    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum)
+    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum, stretch=stretch)
     xyz = build_markers(spec, seed)
     x, y, z = (a.astype(np.float64) for a in xyz)
-    r = np.sqrt((x - L / 2) ** 2 + (y - L / 2) ** 2 + (z - L / 2) ** 2)
+    c = [f * L for f in centre_frac]
+    r = np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2)
     types = np.where(r <= radius_km * 1e3, SPHERE, MATRIX)
-    rocks = {MATRIX: Rock(nu=1e21, ro=3300.0), SPHERE: Rock(nu=1e23, ro=3400.0)}
+    mat = Rock(nu=1e21, ro=3300.0)
+    if plastic:
+        a, b = plastic
+        mat = dataclasses.replace(mat, a0=a, a1=a, b0=b, b1=b, e0=0.0, e1=1.0)
+    rocks = {MATRIX: mat, SPHERE: Rock(nu=1e23, ro=sphere_rho)}
     return make_prn(spec, rocks, types, xyz, seed), spec
 
 

@@ -204,6 +204,11 @@ int i3g_stokes_prolong(i3g_ctx *c, int level);
 int i3g_stokes_vcycles(i3g_ctx *c, int ncycles);
 /* Relative residuals of the level-0 system for the current solution. */
 int i3g_stokes_relres(i3g_ctx *c, double *mom_rel, double *cont_rel);
+/* Strain rates exx..eyz and stresses sxx..syz of the current level-0 velocities and nodal
+ * viscosities: sxxcalc..syzcalc with ynval = 0 (move3mg.c:3-710), as vpiterate recomputes
+ * them after its iterations (move3mg.c:2405-2555).  Builds the level operators first, like
+ * i3g_stokes_setup; read the result with i3g_download(I3G_SYNC_STRESS). */
+int i3g_stokes_stresses(i3g_ctx *c);
 
 /* Time reps launches of one kernel class on the level-0 data with CUDA events on the
  * context stream; returns the mean duration per launch and the algorithmic bytes that one

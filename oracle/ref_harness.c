@@ -17,7 +17,7 @@
  *   move DT PREFIX             loads PREFIX.fields, movemark(); writes PREFIX.marks
  *   r2n PREFIX                 ronurecalc() on the loaded markers; writes PREFIX.nodes
  *   mover2n DT PREFIX          loads PREFIX.fields, movemark(), ronurecalc(); marks + nodes
- *   titerate DT PREFIX         loads PREFIX.fields, titerate(0); marks + nodes
+ *   titerate DT PREFIX [CAP]   loads PREFIX.fields, titerate(0) (at most CAP iteration blocks); marks + nodes
  *   step OUT.prn               one full i3mg time step (i3mg.c:80-147), wall time per phase
  */
 #include <stdio.h>
@@ -398,10 +398,15 @@ int main(int argc, char **argv)
         dump_nodes(argv[3]);
         return 0;
     }
-    if (!strcmp(cmd, "titerate") && argc == 4) {
+    if (!strcmp(cmd, "titerate") && (argc == 4 || argc == 5)) {
         load_fields(argv[3]);
         timestep = atof(argv[2]);
+        if (argc == 5 && atol(argv[4]) > 0) i3g_heat_block_cap = atol(argv[4]);
+        i3g_heat_blocks = 0;
+        double t0 = omp_get_wtime();
         titerate(0);
+        printf("{\"heat_blocks\": %ld, \"seconds\": %.4f, \"timestep\": %.9e}\n", i3g_heat_blocks + 1,
+               omp_get_wtime() - t0, timestep);
         dump_marks(argv[3]);
         dump_nodes(argv[3]);
         return 0;

@@ -31,6 +31,12 @@ def golden(name):
     return p, mode, fx
 
 
-@pytest.fixture(params=["sphere13", "sphere17"])
+# reference-generated cases small enough for the CPU oracle's tests (the 33^3 case runs in
+# the oracle tests that stay fast and in the GPU tests)
+SMALL_CASES = ["sphere13", "sphere17", "incl17", "dp17", "stretch17"]
+ALL_CASES = SMALL_CASES + ["sphere33"]
+
+
+@pytest.fixture(params=SMALL_CASES)
 def golden_case(request):
     return (request.param,) + golden(request.param)

@@ -4,7 +4,7 @@ import pytest
 
 import cases
 import oracle as O
-from conftest import golden
+from conftest import ALL_CASES, golden
 from i3elvis_b200 import abi, lib
 
 pytestmark = pytest.mark.gpu
@@ -30,7 +30,7 @@ def bc_rows(p, mode, level):
     return m
 
 
-@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_setup_bit_exact(name):
     p, mode, fx, g, o = pair(name)
     g.call("i3g_stokes_setup")
@@ -43,7 +43,7 @@ def test_setup_bit_exact(name):
     assert np.array_equal(g.get(abi.A_SOL, 0, 4 * n0), o.get(abi.A_SOL, 0, 4 * n0))
 
 
-@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_residual_smooth_transfer_bit_exact(name):
     p, mode, fx, g, o = pair(name)
     g.call("i3g_stokes_setup")
@@ -73,7 +73,7 @@ def test_residual_smooth_transfer_bit_exact(name):
 
 
 @pytest.mark.parametrize("tail", ["12000", "2000", "0"])
-@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_vcycles_bit_exact(name, tail, monkeypatch):
     """V-cycles equal the oracle's bit for bit, with the small levels in the one-block tail
     kernel (default) and with one kernel per phase on every level (I3G_TAIL_NODES=0)."""
@@ -106,11 +106,13 @@ def _compare_to_reference(p, sol, ref, tol):
 
 
 @pytest.mark.parametrize("precision,krylov", [(0, 0), (1, 0), (1, 8)])
-@pytest.mark.parametrize("name", ["sphere13", "sphere17"])
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_solve_matches_reference(name, precision, krylov):
     """Converged velocity and pressure equal the reference's converged FP64 solution to
     relative L2 1e-8 (FP64 multigrid; FP32 multigrid inside FP64 defect correction, plain and
-    FGMRES-accelerated)."""
+    FGMRES-accelerated).  Cases: sinking spheres (13^3, 17^3, the 33^3 CPU-runnable benchmark
+    configuration, whose own bar is 1e-6), Arrhenius inclusions, Drucker-Prager yielding and a
+    non-uniform grid."""
     p, mode, fx = golden(name)
     par = abi.make_params(mode, stokes_rtol=1e-11, stokes_maxcyc=3000, precision=precision, krylov=krylov)
     g = lib.Context(abi.ModelBuffers(p), par, abi.make_file_params(mode.files[0]))
