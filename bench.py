@@ -43,6 +43,10 @@ WORKLOADS = {
                    desc="65^3 nodes, 200 km cube, 27 markers/cell, 100 inclusions, Arrhenius 1e18-1e24"),
     "sphere33": dict(n=33, mnum=3, multinum=2, seed=1,
                      desc="33^3 nodes, 100 km cube, 27 markers/cell, sinking sphere 1e23/1e21"),
+    "subd257": dict(n=257, mnum=3, multinum=4, seed=11,
+                    desc="257x129x257 nodes (y vertical), 1000x500x1000 km, 27 markers/cell (226.5M), 100 km "
+                         "lithosphere 1e24, 45-degree slab +50 kg/m3, 10 km weak layer 1e19, Arrhenius mantle "
+                         "1e19-1e22, Drucker-Prager 10 MPa + 0.6 P"),
 }
 
 
@@ -66,6 +70,9 @@ def build_case(name, seed_offset=0, sweeps=None):
     if name.startswith("sphere"):
         prn, spec = model.sinking_sphere(n=w["n"], mnum=w["mnum"], multinum=w["multinum"], seed=w["seed"] + seed_offset)
         size = 100e3
+    elif name.startswith("subd"):
+        prn, spec = model.subduction(mnum=w["mnum"], multinum=w["multinum"], seed=w["seed"] + seed_offset)
+        size = 1000e3 * (w["n"] - 1) / 256.0
     else:
         prn, spec = model.random_inclusions(n=w["n"], mnum=w["mnum"], multinum=w["multinum"],
                                             seed=w["seed"] + seed_offset, count=w["count"])
@@ -176,41 +183,52 @@ class Clocks:
 
 
 # titerate (heat3mg.c:463-560) repeats its iteration block until heatsum <= HEATMIN, which its
-# racy multi-threaded relaxation may never reach; the reference samples stop it after this many
-# blocks (the count used is in each sample's "heat_blocks")
+# racy multi-threaded relaxation may never reach; the reference steps stop it after this many
+# blocks (the count used is in each step's "heat_blocks")
 REF_HEAT_CAP = 20
+# V-cycles per reference step: the reference's lexicographic multigrid does not reach relative
+# residual 1e-8 on the inclusion models (65^3: 4e-7 after 300 cycles), so every timed step
+# stops here and reports the residual it reached; its step time is a lower bound of the
+# reference's time to 1e-8 (twice the plain FP64 GPU multigrid's ~20 cycles per step)
+REF_MAX_CYCLES = 40
 
 
-def _est(r, ncyc):
-    """Step estimate from one sample: set-up + ncyc V-cycles + heat + advection + marker->node."""
-    return r["assemble_s"] + ncyc * r["vcycle_s"] + r["heat_s"] + r["move_s"] + r["r2n_s"]
-
-
-def reference_sample(prn, mode, ncyc_for_1e8, threads, dt=0.0):
-    """Time the reference's own functions on this workload (bounded sample, all host threads):
-    its initial-condition passes, then two steps of vpiterate set-up + one V-cycle, titerate,
-    movemark and ronurecalc; the second (warm) step is the sample.  The step estimate scales
-    the V-cycle by the number of V-cycles this multigrid needs for relative residual 1e-8."""
+def reference_steps(prn, mode, rtol, reps, threads, dt=0.0, timeout=3000):
+    """Whole time steps of the reference's own functions on this workload, wall clock, all
+    host threads: its initial-condition passes, then ``reps`` steps of vpiterate set-up,
+    V-cycles to ``rtol`` (at most REF_MAX_CYCLES), titerate, movemark and ronurecalc.  Returns
+    the per-step JSON records (None without the reference harness)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not O.have_reference():
         return None
+    args = ("steps", rtol, REF_MAX_CYCLES, reps, 1, REF_HEAT_CAP) + ((repr(float(dt)),) if dt else ())
     with tempfile.TemporaryDirectory() as d:
         write_prn(os.path.join(d, "in0.prn"), prn)
         config.write_mode(os.path.join(d, "mode.t3c"), mode)
         config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-        rs = O.run_reference_lines(d, "sample", 1, 2, 1, REF_HEAT_CAP, repr(float(dt)), threads=threads, timeout=600)
+        rs = O.run_reference_lines(d, *args, threads=threads, timeout=timeout)
         if rs and not rs[-1].get("vmax", 1.0) > 0 and threads > 8:
-            # the reference's multi-threaded V-cycle left no finite velocity (seen with 16 threads
-            # at 129^3); time it again with 8 threads
-            rs = O.run_reference_lines(d, "sample", 1, 2, 1, REF_HEAT_CAP, repr(float(dt)), threads=8, timeout=600)
-    if not rs:
-        return None
-    return _est(rs[-1], ncyc_for_1e8), rs[-1]
+            # the reference's racy multi-threaded V-cycle left no finite velocity (seen with 16
+            # threads at 129^3): time it again with 8 threads
+            rs = O.run_reference_lines(d, *args, threads=8, timeout=timeout)
+    return rs
+
+
+def _ref_sample_text(rs, workload, rtol):
+    cyc = [r["ncyc"] for r in rs]
+    rel = [r["rel"] for r in rs]
+    return (f"{len(rs)} whole reference time steps on the full {workload} model (one process, after the "
+            f"reference's initial-condition passes and one untimed step): vpiterate set-up, V-cycles until the "
+            f"relative residual <= {rtol:g} or {REF_MAX_CYCLES} cycles (cycles {cyc}, residual reached "
+            f"{', '.join(f'{x:.2e}' for x in rel)}), the CFL step, titerate (at most {REF_HEAT_CAP} iteration blocks), "
+            f"movemark, ronurecalc; {rs[0]['threads']} OpenMP threads")
 
 
 def run_reference_arm(args):
-    """--impl reference: the reference's CPU implementation of the step on this box's cores."""
+    """--impl reference: the reference's CPU implementation of the step on this box's cores.
+    Whole steps are timed (at most 4 after one untimed step, so that the arm ends within a few
+    minutes); ``steps`` and ``warmup`` in the JSON are the counts actually run."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -221,33 +239,21 @@ def run_reference_arm(args):
     if not O.have_reference():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built (reference sources absent at build time)"}))
         return 0
-    ncyc = args.ref_cycles
-    with tempfile.TemporaryDirectory() as d:
-        write_prn(os.path.join(d, "in0.prn"), prn)
-        config.write_mode(os.path.join(d, "mode.t3c"), mode)
-        config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-        # one process: the reference's initial-condition passes (in3mg.c:990-1031), then
-        # warmup + timed steps, each a sample of the step (see the harness's sample command)
-        rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, REF_HEAT_CAP, repr(args.ref_dt),
-                                   threads=threads, timeout=3000)
-        if rs and not rs[-1].get("vmax", 1.0) > 0 and threads > 8:
-            threads = 8   # see reference_sample
-            rs = O.run_reference_lines(d, "sample", 1, args.warmup + args.steps, 1, REF_HEAT_CAP, repr(args.ref_dt),
-                                       threads=threads, timeout=3000)
-    timed = rs[args.warmup:]
-    times = [_est(r, ncyc) for r in timed]
-    detail = timed[-1] if timed else None
-    v = float(np.mean(times))
-    sample = (f"per step: reference vpiterate set-up + 1 V-cycle (x {ncyc} V-cycles, the count this multigrid "
-              f"needs for relative residual 1e-8), time step {args.ref_dt:.4g} s (the GPU run's CFL step), titerate (at most "
-              f"{REF_HEAT_CAP} iteration blocks), movemark, "
-              f"ronurecalc on the full {args.workload} model, {threads} OpenMP threads, one process after the "
-              f"reference's initial-condition passes; last timed step {json.dumps(detail)}")
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 4))
+    rs = reference_steps(prn, mode, args.rtol, warm + steps, threads)
+    timed = rs[warm:]
+    v = float(np.mean([r["step_s"] for r in timed]))
+    sample = _ref_sample_text(timed, args.workload, args.rtol)
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s/step", "n_gpus": args.gpus,
-                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+                      "steps": len(timed), "warmup": warm, "ms_per_step": v * 1e3, "higher_is_better": False,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"]},
-                      "cpu_baseline": {"value": v, "unit": "s/step", "cores": threads, "kind": "reference", "sample": sample},
+                      "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                                 "stokes_rtol": args.rtol, "max_vcycles_per_step": REF_MAX_CYCLES},
+                      "stokes_cycles": [r["ncyc"] for r in timed], "stokes_rel": [r["rel"] for r in timed],
+                      "phases_s": {k: float(np.mean([r[k] for r in timed])) for k in
+                                   ("assemble_s", "stokes_s", "heat_s", "move_s", "r2n_s")},
+                      "cpu_baseline": {"value": v, "unit": "s/step", "cores": timed[-1]["threads"], "kind": "reference",
+                                       "sample": sample},
                       "e2e": {"value": v, "unit": "s/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
     return 0
 
@@ -269,11 +275,6 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="mixed precision: skip the plain FP64 multigrid steps timed for comparison")
-    # V-cycles per step that the reference-arm estimate charges: the count the FP64 multigrid
-    # takes to relative residual 1e-8 on incl129 on the GPU (21-22 per step after warm-up)
-    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("I3G_REF_CYCLES", "21")))
-    # time step of the reference-arm samples: the CFL step the GPU run takes on incl129 (s)
-    ap.add_argument("--ref-dt", type=float, default=3.5635e10)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -293,6 +294,7 @@ def main():
     if sweeps is None and prec == 1 and args.krylov > 0:
         sweeps = MIXED_SWEEPS.get(WORKLOADS[args.workload]["multinum"])
     prn, mode = build_case(args.workload, seed_offset=rank, sweeps=sweeps)
+    prn0 = prn
     krylov = args.krylov if prec == 1 else 0
     warm = args.warm if prec == 1 else 1
     par = abi.make_params(mode, stokes_rtol=args.rtol, stokes_maxcyc=3000, heat_rtol=1e-10, precision=prec, krylov=krylov,
@@ -366,7 +368,9 @@ def main():
     barrier()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        ctx.upload(abi.SYNC_NODES | abi.SYNC_MARKERS)
+        # nodal fields first; the 2.8 GB of marker copies overlap the Stokes solve (they are
+        # first needed by the heat step's marker update)
+        ctx.upload(abi.SYNC_NODES | abi.SYNC_MARKERS | abi.SYNC_ASYNC)
         runtime.time_step(ctx, mode, f, 100 + i)
         ctx.download(abi.SYNC_ALL)
     barrier()
@@ -405,24 +409,19 @@ def main():
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # the reference iterates its own V-cycle: charge the plain FP64 multigrid's count when known
-        ncyc = int(np.median(fp64_mg["stokes_cycles"])) if fp64_mg else (
-            int(np.median(cycles[args.warmup:])) if cycles[args.warmup:] else 21)
         try:
-            log("cpu baseline: reference sample")
+            log("cpu baseline: reference steps")
             dts = [lg["timestep"] for lg in logs if lg.get("timestep")]
-            r = reference_sample(prn, mode, ncyc, host_threads(), float(np.median(dts)) if dts else 0.0)
+            rs = reference_steps(prn0, mode, args.rtol, 2, host_threads(), float(np.median(dts)) if dts else 0.0)
             log("cpu baseline done")
         except Exception as e:  # the CPU baseline is reported, never required
-            r = None
+            rs = None
             out["cpu_baseline_error"] = str(e)[:300]
-        if r:
-            est, detail = r
-            out["cpu_baseline"] = {"value": est, "unit": "s/step", "cores": detail["threads"], "kind": "reference",
-                                   "sample": f"one warm step of the reference on the same model after its initial-condition "
-                                             f"passes: set-up + 1 V-cycle x {ncyc} V-cycles (the plain multigrid's count to 1e-8 here), this run's time "
-                                             f"step, titerate (at most {REF_HEAT_CAP} iteration blocks), movemark, "
-                                             f"ronurecalc; {json.dumps(detail)}"}
+        if rs:
+            r = rs[-1]
+            out["cpu_baseline"] = {"value": r["step_s"], "unit": "s/step", "cores": r["threads"], "kind": "reference",
+                                   "sample": _ref_sample_text(rs[1:], args.workload, args.rtol) +
+                                   f" (time step fixed to this run's {r['timestep']:.4g} s); {json.dumps(r)}"}
     ctx.close()
     if rank == 0:
         print(json.dumps(out))

@@ -21,6 +21,7 @@ c_i8p = C.POINTER(C.c_int8)
 E_CODES = {0: "OK", -1: "ARG", -2: "CUDA", -3: "NOMEM", -4: "UNSUPPORTED", -5: "NOCONV",
            -6: "NAN", -7: "PRESSURE", -8: "BC"}
 SYNC_NODES, SYNC_STRESS, SYNC_MARKERS, SYNC_ALL = 1, 2, 4, 7
+SYNC_ASYNC = 8   # upload: marker copies overlap the following calls (include/i3g.h)
 A_SOL, A_RHS, A_RES, A_NU, A_ETA, A_TK = range(6)
 
 NODE_F32 = ("vx", "vy", "vz", "ro", "nu", "nxx", "nxy", "nxz", "nyz", "tk", "cp", "et", "kt", "ht", "rr")

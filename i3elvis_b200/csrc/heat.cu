@@ -603,18 +603,15 @@ int heat_time_kernel(i3g_ctx *c, int reps, double *ms, double *bytes)
     Level &L0 = c->lev[0];
     HView V = hview(c, 0, 1e13);
     const long tot = (long)((L0.ny + 1) / 2) * L0.nx * L0.nz;
-    EventPair ev;
-    I3G_CUDA(ev.create());
-    cudaEvent_t e0 = ev.a, e1 = ev.b;
-    I3G_CUDA(cudaEventRecord(e0, c->st));
-    for (int r = 0; r < reps; r++) LAUNCH(k_heat_relax, nb(tot), 256, V, r & 1, 1.0);
-    I3G_CUDA(cudaEventRecord(e1, c->st));
-    I3G_CUDA(cudaEventSynchronize(e1));
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    *ms = t / reps;
-    // one colour: T read, half written, rhs half, kt, rho*cp, bc mask
-    *bytes = (double)L0.n * (8.0 + 4.0 + 4.0 + 4.0 + 8.0 + 1.0);
+    // one full sweep (both colours) with an empty L2; 32 B per node: T read and written (FP64),
+    // k and rho cp (FP32), right-hand side (FP64)
+    int rc = cold_time(c, reps, [&]() -> int {
+        LAUNCH(k_heat_relax, nb(tot), 256, V, 0, 1.0);
+        LAUNCH(k_heat_relax, nb(tot), 256, V, 1, 1.0);
+        return 0;
+    }, ms);
+    if (rc) return rc;
+    *bytes = (double)L0.n * 32.0;
     return 0;
 }
 

@@ -11,7 +11,8 @@ int heat_time_kernel(i3g_ctx *c, int reps, double *ms, double *bytes);
 
 int markers_alloc(i3g_ctx *c);
 void markers_free(i3g_ctx *c);
-int markers_upload(i3g_ctx *c, const i3g_model *m);
+// async: copies on the context's copy stream; marker operations wait for them on the device
+int markers_upload(i3g_ctx *c, const i3g_model *m, bool async = false);
 int markers_download(i3g_ctx *c, i3g_model *m);
 int markers_move(i3g_ctx *c, double timestep);
 int markers_to_nodes(i3g_ctx *c, double timestep);

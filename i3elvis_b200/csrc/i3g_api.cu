@@ -69,7 +69,9 @@ void i3g_destroy(i3g_ctx *c)
     if (c->hstage) cudaFreeHost(c->hstage);
     if (c->tev[0]) { cudaEventDestroy(c->tev[0]); cudaEventDestroy(c->tev[1]); }
     delete[] c->hgx; delete[] c->hgy; delete[] c->hgz;
+    cudaFree(c->flush);
     if (c->st) cudaStreamDestroy(c->st);
+    if (c->cst) cudaStreamDestroy(c->cst);
     delete c;
 }
 
@@ -91,8 +93,10 @@ int i3g_create(const i3g_model *m, const i3g_params *p, i3g_ctx **out)
     c->f.p0koef = c->f.p0koef2 = p->p0koef; c->f.p1koef = c->f.p1koef2 = p->p1koef; c->f.p2koef = c->f.p2koef2 = p->p2koef;
     c->f.maxxystep = 0; c->f.maxtkstep = 1e30; c->f.maxtmstep = 1e30; c->f.cyc0max = 1;
     cudaGetDevice(&c->dev);
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cst, cudaStreamNonBlocking) != cudaSuccess) {
         snprintf(g_err, sizeof g_err, "cannot create a CUDA stream (is a GPU present?)");
+        if (c->st) cudaStreamDestroy(c->st);
         delete c;
         return I3G_E_CUDA;
     }
@@ -258,7 +262,7 @@ int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask)
         for (int a = 0; a < 6; a++) { H2D(c->eps[a], he[a], N, 4); H2D(c->sig[a], hs[a], N, 4); }
     }
     if (mask & I3G_SYNC_MARKERS) {
-        int rc = i3g::markers_upload(c, m);
+        int rc = i3g::markers_upload(c, m, (mask & I3G_SYNC_ASYNC) != 0);
         if (rc) return rc;
     }
     c->m.timesum = m->timesum;
@@ -395,7 +399,7 @@ int i3g_stokes_relres(i3g_ctx *c, double *mom_rel, double *cont_rel)
 int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, double *bytes_per_launch)
 {
     if (!c || reps <= 0 || !ms_per_launch || !bytes_per_launch) return I3G_E_ARG;
-    if (kind == 4 || kind == 5) return i3g::markers_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
+    if (kind == 4 || kind == 5 || kind == 9) return i3g::markers_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
     if (kind == 6) return i3g::heat_time_kernel(c, reps, ms_per_launch, bytes_per_launch);
     return i3g::stokes_time_kernel(c, kind, reps, ms_per_launch, bytes_per_launch);
 }

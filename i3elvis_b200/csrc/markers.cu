@@ -43,7 +43,8 @@ struct MarkerState {
     int *bsum = nullptr;            // scan chunk sums
     int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
     long nbins = 0;                 // cells of all tiles + inactive bin + end
-    double *acc = nullptr;          // [NACC * nodenum] node sums
+    double *acc = nullptr;          // [2 * nodenum] node sums of the marker temperature change
+    double *stage = nullptr;        // [ntiles][NACC][NBOX] per-tile node-box sums (no atomics)
     float *tk1 = nullptr;           // copy of T before boundary rows
     double *rock = nullptr;         // [24 * rocknum]
     int *err = nullptr, *herr = nullptr;
@@ -51,6 +52,10 @@ struct MarkerState {
     int *tbc_node = nullptr, *tbc_p = nullptr;
     double *tbc_c = nullptr, *tbc_k = nullptr;
     bool sorted = false;
+    unsigned move_blocks = 1;       // persistent grid of k_move: resident CTAs on all SMs
+    unsigned key_blocks = 1;        // the same for k_tile_key and k_heat_mark_anti
+    cudaEvent_t up_ev = nullptr;    // end of an asynchronous upload on the copy stream
+    bool up_pending = false;        // the compute stream has not waited for it yet
 };
 
 static MarkerState *ms(i3g_ctx *c) { return (MarkerState *)c->mk; }
@@ -103,60 +108,179 @@ struct NodeF {
     long NY, NXY;
 };
 
-// vxyzcalc1 (mark3mg.c:2347-2530)
-__device__ void vxyz(const Grid &G, const NodeF &F, double x, double y, double z, double *v, int *wn)
+// One axis of a trilinear stencil: first node index i and the weights of nodes i and i + 1,
+// computed with the reference's expressions (one correctly rounded division per weight).  The
+// three staggered velocity components, and the four strain-rate groups, use a few distinct
+// kinds per axis; computing each kind once per point, instead of once per corner, removes most
+// of the FP64 divisions of the advection without changing a single rounding.
+struct Ax {
+    int i;
+    double w0, w1;
+};
+
+// node-line stencil of a component along its own axis (vxyzcalc1, e.g. Vx in x,
+// mark3mg.c:2370-2395): i = cell clamped to [lo, n - 2 - hi_off]
+__device__ __forceinline__ Ax ax_line(const double *g, int n, int m, double x, int lo, int hi)
+{
+    int a = m;
+    if (a < lo) a = lo;
+    if (a > n - hi) a = n - hi;
+    const double d = g[a + 1] - g[a];
+    double t0 = (g[a] - x) / d, t1 = (g[a + 1] - x) / d;
+    t0 = -t0;
+    return Ax{a, 1.0 - t0, 1.0 - t1};
+}
+
+// mid-point stencil across a staggered axis (vxyzcalc1, e.g. Vx in y): i = cell, minus one below
+// the cell's mid-point, clamped to [0, n - 3]; nodes are the mid-points (g[k] + g[k+1]) / 2
+__device__ __forceinline__ Ax ax_mid(const double *g, int n, int m, double x)
+{
+    int b = m;
+    if (x < (g[b] + g[b + 1]) / 2.0) b -= 1;
+    if (b < 0) b = 0;
+    if (b > n - 3) b = n - 3;
+    const double d = (g[b + 2] - g[b]) / 2.0;
+    double t0 = ((g[b] + g[b + 1]) / 2.0 - x) / d, t1 = ((g[b + 1] + g[b + 2]) / 2.0 - x) / d;
+    t0 = -t0;
+    return Ax{b, 1.0 - t0, 1.0 - t1};
+}
+
+// cell-centre stencil of epscalc1's normal components (mark3mg.c:2562-2600): i = cell, plus one
+// above the mid-point, clamped to [1, n - 2]; nodes are (g[k-1] + g[k]) / 2; weights in [0, 1]
+__device__ __forceinline__ Ax ax_cent(const double *g, int n, int m, double x)
+{
+    int a = m;
+    if (x > (g[a] + g[a + 1]) / 2.0) a += 1;
+    if (a < 1) a = 1;
+    if (a > n - 2) a = n - 2;
+    const double d = (g[a + 1] - g[a - 1]) / 2.0;
+    double t0 = ((g[a - 1] + g[a]) / 2.0 - x) / d, t1 = ((g[a] + g[a + 1]) / 2.0 - x) / d;
+    t0 = -t0;
+    return Ax{a, clamp01(1.0 - t0), clamp01(1.0 - t1)};
+}
+
+__device__ __forceinline__ Ax clamped(Ax a) { return Ax{a.i, clamp01(a.w0), clamp01(a.w1)}; }
+
+// sum over the 8 corners of f * ((ddx * ddy) * ddz) in the reference's loop order z, x, y
+__device__ __forceinline__ double tri(const float *__restrict__ f, long NY, long NXY, const Ax &X, const Ax &Y, const Ax &Z)
+{
+    double s = 0;
+#pragma unroll
+    for (int k3 = 0; k3 < 2; k3++) {
+        const double ddz = k3 ? Z.w1 : Z.w0;
+#pragma unroll
+        for (int k1 = 0; k1 < 2; k1++) {
+            const double ddx = k1 ? X.w1 : X.w0;
+            const long base = (long)(Z.i + k3) * NXY + (long)(X.i + k1) * NY + Y.i;
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) {
+                const double ddy = k2 ? Y.w1 : Y.w0;
+                s += (double)__ldg(f + base + k2) * (ddx * ddy * ddz);
+            }
+        }
+    }
+    return s;
+}
+
+// Stencils of one point for vxyzcalc1: node-line and mid-point kinds on each axis.
+struct VStencil {
+    Ax lx, ly, lz, mx, my, mz;
+};
+
+// vxyzcalc1 (mark3mg.c:2347-2530): staggered trilinear velocity at a point.  Vx uses
+// (line x, mid y, mid z), Vy (mid x, line y, mid z), Vz (mid x, mid y, line z).
+__device__ __forceinline__ void vxyz(const Grid &G, const NodeF &F, double x, double y, double z, double *v, int *wn,
+                                     VStencil *out = nullptr)
 {
     const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
     const int X = G.nx, Y = G.ny, Z = G.nz;
-    v[0] = v[1] = v[2] = 0;
     if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
     if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
     const int m1 = wn[0] = locate(gx, X, x, G.ux), m2 = wn[1] = locate(gy, Y, y, G.uy), m3 = wn[2] = locate(gz, Z, z, G.uz);
-    int a, b, c;
-    double dx, dy, dz, ddx, ddy, ddz;
-    a = m1; if (a < 0) a = 0; if (a > X - 2) a = X - 2;
-    b = m2; if (y < (gy[b] + gy[b + 1]) / 2.0) b -= 1; if (b < 0) b = 0; if (b > Y - 3) b = Y - 3;
-    c = m3; if (z < (gz[c] + gz[c + 1]) / 2.0) c -= 1; if (c < 0) c = 0; if (c > Z - 3) c = Z - 3;
-    dx = gx[a + 1] - gx[a]; dy = (gy[b + 2] - gy[b]) / 2.0; dz = (gz[c + 2] - gz[c]) / 2.0;
-    for (int k3 = c; k3 <= c + 1; k3++) {
-        ddz = ((gz[k3] + gz[k3 + 1]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
-        for (int k1 = a; k1 <= a + 1; k1++) {
-            ddx = (gx[k1] - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
-            for (int k2 = b; k2 <= b + 1; k2++) {
-                ddy = ((gy[k2] + gy[k2 + 1]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
-                v[0] += (double)F.vx[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
+    VStencil S;
+    S.lx = ax_line(gx, X, m1, x, 0, 2);
+    S.ly = ax_line(gy, Y, m2, y, 0, 2);
+    S.lz = ax_line(gz, Z, m3, z, 0, 2);
+    S.mx = ax_mid(gx, X, m1, x);
+    S.my = ax_mid(gy, Y, m2, y);
+    S.mz = ax_mid(gz, Z, m3, z);
+    v[0] = tri(F.vx, F.NY, F.NXY, S.lx, S.my, S.mz);
+    v[1] = tri(F.vy, F.NY, F.NXY, S.mx, S.ly, S.mz);
+    v[2] = tri(F.vz, F.NY, F.NXY, S.mx, S.my, S.lz);
+    if (out) *out = S;
+}
+
+// one shear group of epscalc1: strain rate, stress and the dissipation term 2 s e w
+__device__ __forceinline__ void edge_group(const float *__restrict__ fe, const float *__restrict__ fs, long NY, long NXY,
+                                           const Ax &AX, const Ax &AY, const Ax &AZ, double &e, double &s, double &d)
+{
+#pragma unroll
+    for (int k3 = 0; k3 < 2; k3++) {
+        const double ddz = k3 ? AZ.w1 : AZ.w0;
+#pragma unroll
+        for (int k1 = 0; k1 < 2; k1++) {
+            const double ddx = k1 ? AX.w1 : AX.w0;
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) {
+                const double ddy = k2 ? AY.w1 : AY.w0;
+                const long n = (long)(AZ.i + k3) * NXY + (long)(AX.i + k1) * NY + (AY.i + k2);
+                const double w = ddx * ddy * ddz;
+                const float ev = __ldg(fe + n), sv = __ldg(fs + n);
+                e += ev * w;
+                s += sv * w;
+                d += 2.0 * sv * ev * w;
             }
         }
     }
-    a = m1; if (x < (gx[a] + gx[a + 1]) / 2.0) a -= 1; if (a < 0) a = 0; if (a > X - 3) a = X - 3;
-    b = m2; if (b < 0) b = 0; if (b > Y - 2) b = Y - 2;
-    c = m3; if (z < (gz[c] + gz[c + 1]) / 2.0) c -= 1; if (c < 0) c = 0; if (c > Z - 3) c = Z - 3;
-    dx = (gx[a + 2] - gx[a]) / 2.0; dy = gy[b + 1] - gy[b]; dz = (gz[c + 2] - gz[c]) / 2.0;
-    for (int k3 = c; k3 <= c + 1; k3++) {
-        ddz = ((gz[k3] + gz[k3 + 1]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
-        for (int k1 = a; k1 <= a + 1; k1++) {
-            ddx = ((gx[k1] + gx[k1 + 1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
-            for (int k2 = b; k2 <= b + 1; k2++) {
-                ddy = (gy[k2] - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
-                v[1] += (double)F.vy[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
+}
+
+// epscalc1 (mark3mg.c:2535-2838) at the point of the first vxyz call, from its cell and
+// mid-point stencils: normal strain rates, stresses and pressure at cell centres, the three
+// shear groups on their edges, and the dissipation sum, each with weights clamped to [0, 1].
+__device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x, double y, double z, const int *wn,
+                                         const VStencil &S, double *e, double *s, double *dis)
+{
+    const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
+    const int X = G.nx, Y = G.ny, Z = G.nz;
+    if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
+    if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
+    const long NY = F.NY, NXY = F.NXY;
+    for (int i = 0; i < 7; i++) e[i] = 0;
+    for (int i = 0; i < 6; i++) s[i] = 0;
+    double d = 0;
+    {
+        const Ax cx = ax_cent(gx, X, wn[0], x), cy = ax_cent(gy, Y, wn[1], y), cz = ax_cent(gz, Z, wn[2], z);
+#pragma unroll
+        for (int k3 = 0; k3 < 2; k3++) {
+            const double ddz = k3 ? cz.w1 : cz.w0;
+#pragma unroll
+            for (int k1 = 0; k1 < 2; k1++) {
+                const double ddx = k1 ? cx.w1 : cx.w0;
+#pragma unroll
+                for (int k2 = 0; k2 < 2; k2++) {
+                    const double ddy = k2 ? cy.w1 : cy.w0;
+                    const long n = (long)(cz.i + k3) * NXY + (long)(cx.i + k1) * NY + (cy.i + k2);
+                    const double w = ddx * ddy * ddz;
+                    const float exx = __ldg(F.e[0] + n), eyy = __ldg(F.e[1] + n), ezz = __ldg(F.e[2] + n);
+                    const float sxx = __ldg(F.s[0] + n), syy = __ldg(F.s[1] + n), szz = __ldg(F.s[2] + n);
+                    e[0] += exx * w; e[1] += eyy * w; e[2] += ezz * w;
+                    s[0] += sxx * w; s[1] += syy * w; s[2] += szz * w;
+                    d += (double)(__fadd_rn(__fadd_rn(__fmul_rn(sxx, exx), __fmul_rn(syy, eyy)), __fmul_rn(szz, ezz))) * w;
+                    e[6] += __ldg(F.pr + n) * w;
+                }
             }
         }
     }
-    a = m1; if (x < (gx[a] + gx[a + 1]) / 2.0) a -= 1; if (a < 0) a = 0; if (a > X - 3) a = X - 3;
-    b = m2; if (y < (gy[b] + gy[b + 1]) / 2.0) b -= 1; if (b < 0) b = 0; if (b > Y - 3) b = Y - 3;
-    c = m3; if (c < 0) c = 0; if (c > Z - 2) c = Z - 2;
-    dx = (gx[a + 2] - gx[a]) / 2.0; dy = (gy[b + 2] - gy[b]) / 2.0; dz = gz[c + 1] - gz[c];
-    for (int k3 = c; k3 <= c + 1; k3++) {
-        ddz = (gz[k3] - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
-        for (int k1 = a; k1 <= a + 1; k1++) {
-            ddx = ((gx[k1] + gx[k1 + 1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
-            for (int k2 = b; k2 <= b + 1; k2++) {
-                ddy = ((gy[k2] + gy[k2 + 1]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
-                v[2] += (double)F.vz[k3 * F.NXY + (long)k1 * F.NY + k2] * (ddx * ddy * ddz);
-            }
-        }
-    }
+    // edge groups: node lines clamped to [1, n - 3] and the mid-point stencils, weights in [0, 1]
+    const Ax ix = clamped(ax_line(gx, X, wn[0], x, 1, 3)), iy = clamped(ax_line(gy, Y, wn[1], y, 1, 3)),
+             iz = clamped(ax_line(gz, Z, wn[2], z, 1, 3));
+    const Ax qx = clamped(S.mx), qy = clamped(S.my), qz = clamped(S.mz);
+    edge_group(F.e[3], F.s[3], NY, NXY, ix, iy, qz, e[3], s[3], d);   // exy
+    edge_group(F.e[4], F.s[4], NY, NXY, ix, qy, iz, e[4], s[4], d);   // exz
+    edge_group(F.e[5], F.s[5], NY, NXY, qx, iy, iz, e[5], s[5], d);   // eyz
+    *dis = d;
 }
 
 // epscalc1 with the cell given (mark3mg.c:2535-2838)
@@ -389,13 +513,9 @@ __device__ __forceinline__ double inv2(const double *e)
 // ------------------------------------------------------------------------------------
 // movemark: rheology update + RK4 (mark3mg.c:49-310)
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
+// one marker of movemark (mark3mg.c:49-310)
+__device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, const NodeF &F, const Phys &P, double timestep)
 {
-    extern __shared__ double shg[];
-    Grid G;
-    load_grid(Gg, shg, G);
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
     int t = M.t[i];
     const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
     const bool inbox = fx >= 0 && fy >= 0 && fz >= 0 && (double)fx <= G.xsize && (double)fy <= G.ysize && (double)fz <= G.zsize;
@@ -404,8 +524,9 @@ __global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF
     const double yold = fy;
     double v1[3], e[7], s[6], dis;
     int wn[3];
-    vxyz(G, F, fx, fy, fz, v1, wn);
-    eps_at(G, F, fx, fy, fz, wn, e, s, &dis);
+    VStencil S0;
+    vxyz(G, F, fx, fy, fz, v1, wn, &S0);
+    eps_from(G, F, fx, fy, fz, wn, S0, e, s, &dis);
     const double eii = inv2(e), sii = inv2(s);
     const double mpb = e[6] * 1e-5;
     float mk = M.k[i], mv = M.v[i], me = M.e[i], mft = M.ft[i], mw = M.w[i];
@@ -453,6 +574,18 @@ __global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF
     M.k[i] = mk; M.v[i] = mv; M.e[i] = me; M.ft[i] = mft; M.w[i] = mw; M.t[i] = (int8_t)t;
 }
 
+// Persistent grid-stride launch (a few CTAs per SM): the grid lines are staged in shared memory
+// once per CTA instead of once per 256 markers.  Markers are in (tile, cell) order from the last
+// sort, so a warp's interpolation corners hit the same L1 lines.
+__global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
+{
+    extern __shared__ double shg[];
+    Grid G;
+    load_grid(Gg, shg, G);
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        move_one(M, i, G, F, P, timestep);
+}
+
 // ------------------------------------------------------------------------------------
 // tile sort
 // ------------------------------------------------------------------------------------
@@ -475,30 +608,34 @@ __device__ __forceinline__ int cell_key(int c1, int c2, int c3, const TileGeo &T
     return tile * CPT + ((c3 % TZ) * TX + (c1 % TX)) * TY + (c2 % TY);
 }
 
+// persistent grid-stride launch (grid lines staged once per CTA); every thread of a CTA runs the
+// same number of iterations, so the warp-wide histogram votes see whole warps
 __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *cnt)
 {
     extern __shared__ double shg[];
     Grid G;
     load_grid(Gg, shg, G);
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    int kk = T.ntiles * CPT;
-    if (i < n) {
-        const float x = M.x[i], y = M.y[i], z = M.z[i];
-        if (r2n_active(G, x, y, z, M.t[i], M.k[i])) {
-            double xd = x, yd = y, zd = z;
-            if (xd > G.xsize) xd = G.xsize;
-            if (yd > G.ysize) yd = G.ysize;
-            if (zd > G.zsize) zd = G.zsize;
-            kk = cell_key(locate(G.gx, G.nx, xd, G.ux), locate(G.gy, G.ny, yd, G.uy), locate(G.gz, G.nz, zd, G.uz), T);
+    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
+        const long i = base + threadIdx.x;
+        int kk = T.ntiles * CPT;
+        if (i < n) {
+            const float x = M.x[i], y = M.y[i], z = M.z[i];
+            if (r2n_active(G, x, y, z, M.t[i], M.k[i])) {
+                double xd = x, yd = y, zd = z;
+                if (xd > G.xsize) xd = G.xsize;
+                if (yd > G.ysize) yd = G.ysize;
+                if (zd > G.zsize) zd = G.zsize;
+                kk = cell_key(locate(G.gx, G.nx, xd, G.ux), locate(G.gy, G.ny, yd, G.uy), locate(G.gz, G.nz, zd, G.uz), T);
+            }
+            key[i] = kk;
         }
-        key[i] = kk;
-    }
-    // warp-aggregated histogram
-    const unsigned act = __ballot_sync(0xffffffffu, i < n);
-    if (i < n) {
-        const unsigned peers = __match_any_sync(act, kk);
-        const int leader = __ffs(peers) - 1;
-        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&cnt[kk], __popc(peers));
+        // warp-aggregated histogram
+        const unsigned act = __ballot_sync(0xffffffffu, i < n);
+        if (i < n) {
+            const unsigned peers = __match_any_sync(act, kk);
+            const int leader = __ffs(peers) - 1;
+            if ((int)(threadIdx.x & 31) == leader) atomicAdd(&cnt[kk], __popc(peers));
+        }
     }
 }
 
@@ -627,15 +764,16 @@ __device__ __forceinline__ void phase_density(const Phys &P, int mm2, double mtk
 // classes; cells of one class share no node, so the per-cell sums are added to the shared node
 // sums without atomics, in a fixed order.
 constexpr int kR2nWarps = 16;
-constexpr int kStage = 14;   // ddx0 ddx1 ddy0 ddy1 ddz0 ddz1 vnu mro mcp*mro mkt mht mbb mtk mrr
+constexpr int kStage = 15;   // ddx0 ddx1 ddy0 ddy1 ddz0 ddz1 vnu mro mcp*mro mkt mht mbb mtk mrr wxx
 
 __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int *coff, Grid Gg, NodeF F, Phys P,
-                                                              TileGeo T, double timestep, double *acc, long N)
+                                                              TileGeo T, double timestep, double *stage)
 {
     extern __shared__ double sm[];
     double *sacc = sm;                                   // [NACC][NBOX]
     double *stg = sm + NACC * NBOX;                      // [kR2nWarps][32][kStage]
     double *shg = stg + kR2nWarps * 32 * kStage;         // grid lines
+    int *scode = (int *)(shg + Gg.nx + Gg.ny + Gg.nz);   // [kR2nWarps][32] per-marker corner masks
     for (int q = threadIdx.x; q < NACC * NBOX; q += blockDim.x) sacc[q] = 0;
     Grid G;
     load_grid(Gg, shg, G);   // contains __syncthreads
@@ -644,6 +782,7 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *my = stg + warp * 32 * kStage;
+    int *mycode = scode + warp * 32;
     const int nd = lane >> 2, sub = lane & 3;   // node of the cell, marker subset (m % 4)
     const int iz = nd >> 2, ix = (nd >> 1) & 1, iy = nd & 1;
     const int vm = P.viscmod;
@@ -692,7 +831,8 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
                             }
                             phase_density(P, mm2, mtk, mpb, mro);
                             const double mcp = RK(P, R_CP, mm2);
-                            const double mkt = (RK(P, R_KT, mm2) + RK(P, R_KF, mm2) / (mtk + 77.0)) * exp(RK(P, R_KP, mm2) * mpb);
+                            const double kp = RK(P, R_KP, mm2);   // exp(0) = 1 exactly: skip it
+                            const double mkt = (RK(P, R_KT, mm2) + RK(P, R_KF, mm2) / (mtk + 77.0)) * (kp != 0 ? exp(kp * mpb) : 1.0);
                             if (fy > P.vdeep && mnu > P.nudeep) mnu = P.nudeep;
                             if (fy < 5e+4 && fx > G.xsize - 1e+4 && fz > 1.5e+5 && fz < 8.7e+5 && mnu > 1e+19) mnu = 1e+19;
                             const int m10 = wn[0], m20 = wn[1], m30 = wn[2];
@@ -712,37 +852,50 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
                             st[11] = mbb;
                             st[12] = mtk;
                             st[13] = M.rr[i];
+                            // cell-centre tent weight (node 1,1,1 only) and the per-axis corner
+                            // masks of the nukoef gate and of the "nearer than half a cell" tests
+                            st[14] = 8.0 * (0.5 - fabs(st[1] - 0.5)) * (0.5 - fabs(st[3] - 0.5)) * (0.5 - fabs(st[5] - 0.5));
+                            const double nk = P.nukoef;
+                            int code = 0;
+#pragma unroll
+                            for (int q = 0; q < 6; q++) code |= (st[q] > nk ? 1 : 0) << q | (st[q] > 0.5 ? 1 : 0) << (8 + q);
+                            mycode[lane] = code;
                         }
                     }
                 }
                 unsigned valid = __ballot_sync(0xffffffffu, ok);
                 __syncwarp();
                 // stage 2: lane (node, subset) over the staged markers m of its subset, all 18 sums
+                // (the sums are compared with the oracle to FP32 rounding, so they use fused
+                // multiply-adds; the weights keep the reference's expressions)
+                const int bx = 1 << ix, by = 4 << iy, bz = 16 << iz;
                 for (unsigned mine = valid & (0x11111111u << sub); mine; mine &= mine - 1) {
-                    const double *st = my + (__ffs(mine) - 1) * kStage;
+                    const int m = __ffs(mine) - 1;
+                    const double *st = my + m * kStage;
+                    const int code = mycode[m];
                     const double ddx = st[ix], ddy = st[2 + iy], ddz = st[4 + iz];
                     const double swt = ddx * ddy * ddz;
                     const double vnu = st[6];
                     if (swt > 0) {
-                        a[A_RO] += st[7] * swt; a[A_CP] += st[8] * swt; a[A_KT] += st[9] * swt; a[A_HT] += st[10] * swt;
-                        a[A_ET] += st[11] * swt; a[A_TK] += st[12] * swt; a[A_RR] += st[13] * swt; a[W_P] += swt;
+                        a[A_RO] = __fma_rn(st[7], swt, a[A_RO]); a[A_CP] = __fma_rn(st[8], swt, a[A_CP]);
+                        a[A_KT] = __fma_rn(st[9], swt, a[A_KT]); a[A_HT] = __fma_rn(st[10], swt, a[A_HT]);
+                        a[A_ET] = __fma_rn(st[11], swt, a[A_ET]); a[A_TK] = __fma_rn(st[12], swt, a[A_TK]);
+                        a[A_RR] = __fma_rn(st[13], swt, a[A_RR]); a[W_P] += swt;
                     }
-                    if (ddx > P.nukoef && ddy > P.nukoef && ddz > P.nukoef) { a[A_NU] += vnu * swt; a[W_NU] += swt; }
-                    if (ix && iy && iz) {
-                        const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (0.5 - fabs(ddy - 0.5)) * (0.5 - fabs(ddz - 0.5));
-                        a[A_XX] += vnu * w1; a[W_XX] += w1;
-                    }
-                    if (!iz && ddx > 0.5 && ddy > 0.5) {
+                    if ((code & (bx | by | bz)) == (bx | by | bz)) { a[A_NU] = __fma_rn(vnu, swt, a[A_NU]); a[W_NU] += swt; }
+                    if (ix && iy && iz) { const double w1 = st[14]; a[A_XX] = __fma_rn(vnu, w1, a[A_XX]); a[W_XX] += w1; }
+                    const int hx = (code >> (8 + ix)) & 1, hy = (code >> (10 + iy)) & 1, hz = (code >> (12 + iz)) & 1;
+                    if (!iz && hx && hy) {
                         const double w1 = 8.0 * (ddx - 0.5) * (ddy - 0.5) * (0.5 - fabs(ddz - 0.5));
-                        a[A_XY] += vnu * w1; a[W_XY] += w1;
+                        a[A_XY] = __fma_rn(vnu, w1, a[A_XY]); a[W_XY] += w1;
                     }
-                    if (!iy && ddx > 0.5 && ddz > 0.5) {
+                    if (!iy && hx && hz) {
                         const double w1 = 8.0 * (ddx - 0.5) * (0.5 - fabs(ddy - 0.5)) * (ddz - 0.5);
-                        a[A_XZ] += vnu * w1; a[W_XZ] += w1;
+                        a[A_XZ] = __fma_rn(vnu, w1, a[A_XZ]); a[W_XZ] += w1;
                     }
-                    if (!ix && ddy > 0.5 && ddz > 0.5) {
+                    if (!ix && hy && hz) {
                         const double w1 = 8.0 * (0.5 - fabs(ddx - 0.5)) * (ddy - 0.5) * (ddz - 0.5);
-                        a[A_YZ] += vnu * w1; a[W_YZ] += w1;
+                        a[A_YZ] = __fma_rn(vnu, w1, a[A_YZ]); a[W_YZ] += w1;
                     }
                 }
                 __syncwarp();
@@ -761,20 +914,19 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
         }
         __syncthreads();
     }
-    // flush: nodes inside the tile box face belong to this tile only
-    for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
-        const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
-        const int gxn = cx0 + lx, gyn = cy0 + ly, gzn = cz0 + lz;
-        if (gxn >= G.nx || gyn >= G.ny || gzn >= G.nz) continue;
-        const long node = (long)gzn * F.NXY + (long)gxn * F.NY + gyn;
-        const bool shared_node = lx == 0 || lx == TX || ly == 0 || ly == TY || lz == 0 || lz == TZ;
-        for (int a = 0; a < NACC; a++) {
-            const double v = sacc[a * NBOX + q];
-            if (v == 0.0) continue;
-            if (shared_node) atomicAdd(acc + a * N + node, v);
-            else acc[a * N + node] = v;
-        }
-    }
+    // the whole node box of the tile to its staging slot; k_r2n_gather adds the boxes that share
+    // a node in a fixed order (no atomics, the same sums on every run)
+    double *dst = stage + (long)tile * NACC * NBOX;
+    for (int q = threadIdx.x; q < NACC * NBOX; q += blockDim.x) dst[q] = sacc[q];
+    (void)cx0; (void)cy0; (void)cz0;
+}
+
+// tiles whose node box holds node coordinate v along one axis (t * T <= v <= t * T + T)
+__device__ __forceinline__ void box_range(int v, int TT, int nt, int &t0, int &t1)
+{
+    t1 = min(v / TT, nt - 1);
+    t0 = v % TT == 0 && v > 0 ? v / TT - 1 : t1;
+    if (t0 > t1) t0 = t1;
 }
 
 // ------------------------------------------------------------------------------------
@@ -791,16 +943,21 @@ __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, dou
     const double dy = wi[9] = G.gy[m20 + 1] - G.gy[m20];
     const double dz = wi[10] = G.gz[m30 + 1] - G.gz[m30];
     e[0] = e[1] = e[2] = e[3] = 0;
+    // per-axis weights 1 - |g - x| / d of the two cell nodes (one division each)
+    const double wz[2] = {1.0 - fabs((G.gz[m30] - z) / dz), 1.0 - fabs((G.gz[m30 + 1] - z) / dz)};
+    const double wx[2] = {1.0 - fabs((G.gx[m10] - x) / dx), 1.0 - fabs((G.gx[m10 + 1] - x) / dx)};
+    const double wy[2] = {1.0 - fabs((G.gy[m20] - y) / dy), 1.0 - fabs((G.gy[m20 + 1] - y) / dy)};
     int q = 0;
-    for (int m3 = m30; m3 <= m30 + 1; m3++) {
-        double ddz = (G.gz[m3] - z) / dz; ddz = 1.0 - fabs(ddz);
-        for (int m1 = m10; m1 <= m10 + 1; m1++) {
-            double ddx = (G.gx[m1] - x) / dx; ddx = 1.0 - fabs(ddx);
-            for (int m2 = m20; m2 <= m20 + 1; m2++) {
-                double ddy = (G.gy[m2] - y) / dy; ddy = 1.0 - fabs(ddy);
-                const double swt = wi[q] = ddx * ddy * ddz;
-                const long m4 = nodes[q] = m3 * T.NXY + (long)m1 * T.NY + m2;
-                e[0] += swt * T.tk0[m4]; e[1] += swt * T.tk1[m4]; e[2] += swt * T.tk[m4]; e[3] += swt * T.tk2[m4];
+#pragma unroll
+    for (int k3 = 0; k3 < 2; k3++) {
+#pragma unroll
+        for (int k1 = 0; k1 < 2; k1++) {
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) {
+                const double swt = wi[q] = wx[k1] * wy[k2] * wz[k3];
+                const long m4 = nodes[q] = (long)(m30 + k3) * T.NXY + (long)(m10 + k1) * T.NY + (m20 + k2);
+                e[0] += swt * __ldg(T.tk0 + m4); e[1] += swt * __ldg(T.tk1 + m4); e[2] += swt * __ldg(T.tk + m4);
+                e[3] += swt * __ldg(T.tk2 + m4);
                 q++;
             }
         }
@@ -814,7 +971,7 @@ constexpr int kHmStage = 9;   // wi[0..7], dtk1
 
 __global__ void __launch_bounds__(32 * kR2nWarps) k_heat_mark_cells(Marks M, const int *coff, Grid Gg, TkF T, TileGeo TG,
                                                                     double timestep, double heatdif, double zdeep,
-                                                                    double tdeep, double *acc, long N)
+                                                                    double tdeep, double *stage)
 {
     extern __shared__ double sm[];
     double *sw0 = sm, *sw1 = sm + NBOX;
@@ -892,23 +1049,33 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_heat_mark_cells(Marks M, con
         }
         __syncthreads();
     }
-    for (int q = threadIdx.x; q < NBOX; q += blockDim.x) {
-        const int ly = q % NBY, r2 = q / NBY, lx = r2 % NBX, lz = r2 / NBX;
-        const int gxn = cx0 + lx, gyn = cy0 + ly, gzn = cz0 + lz;
-        if (gxn >= G.nx || gyn >= G.ny || gzn >= G.nz) continue;
-        const long node = (long)gzn * T.NXY + (long)gxn * T.NY + gyn;
-        const bool shared_node = lx == 0 || lx == TX || ly == 0 || ly == TY || lz == 0 || lz == TZ;
-        const double a0 = sw0[q], a1 = sw1[q];
-        if (a0 == 0.0 && a1 == 0.0) continue;
-        if (shared_node) { atomicAdd(acc + node, a0); atomicAdd(acc + N + node, a1); }
-        else { acc[node] = a0; acc[N + node] = a1; }
-    }
+    double *dst = stage + (long)tile * 2 * NBOX;
+    for (int q = threadIdx.x; q < 2 * NBOX; q += blockDim.x) dst[q] = sm[q];
+    (void)cx0; (void)cy0; (void)cz0;
 }
 
-__global__ void k_heat_mark_norm(double *acc, long N)
+// per node: the weight sum and the weighted temperature change over the tile boxes holding it
+// (fixed tile order), then their ratio: acc[n] = sum w, acc[N + n] = sum w dT / sum w
+__global__ void k_heat_mark_gather(const double *stage, TileGeo TG, int nx, int ny, int nz, double *acc, long N)
 {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < N && acc[n] != 0.0) acc[N + n] /= acc[n];
+    if (n >= N) return;
+    const int y = (int)(n % ny), x = (int)((n / ny) % nx), z = (int)(n / ((long)nx * ny));
+    int x0, x1, y0, y1, z0, z1;
+    box_range(x, TX, TG.ntx, x0, x1);
+    box_range(y, TY, TG.nty, y0, y1);
+    box_range(z, TZ, TG.ntz, z0, z1);
+    double a0 = 0, a1 = 0;
+    for (int tz = z0; tz <= z1; tz++)
+        for (int tx = x0; tx <= x1; tx++)
+            for (int ty = y0; ty <= y1; ty++) {
+                const long tile = ((long)tz * TG.ntx + tx) * TG.nty + ty;
+                const int q = ((z - tz * TZ) * NBX + (x - tx * TX)) * NBY + (y - ty * TY);
+                a0 += stage[tile * 2 * NBOX + q];
+                a1 += stage[tile * 2 * NBOX + NBOX + q];
+            }
+    acc[n] = a0;
+    acc[N + n] = a0 != 0.0 ? a1 / a0 : a1;
 }
 
 // antidiffusion: marker T -= interpolated mean node change (heat3mg.c:722-779)
@@ -917,27 +1084,47 @@ __global__ void k_heat_mark_anti(Marks M, const int *off, int ntiles, Grid Gg, T
     extern __shared__ double shg[];
     Grid G;
     load_grid(Gg, shg, G);
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= off[ntiles]) return;
-    double e[4], wi[11];
-    int wn[3];
-    long nodes[8];
-    tk_at(G, T, M.x[i], M.y[i], M.z[i], e, wn, nodes, wi);
-    double iv = 0;
-    for (int q = 0; q < 8; q++) iv -= acc[N + nodes[q]] * wi[q];
-    M.k[i] = __fadd_rn(M.k[i], (float)iv);
+    const long n = off[ntiles];
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double e[4], wi[11];
+        int wn[3];
+        long nodes[8];
+        tk_at(G, T, M.x[i], M.y[i], M.z[i], e, wn, nodes, wi);
+        double iv = 0;
+        for (int q = 0; q < 8; q++) iv -= acc[N + nodes[q]] * wi[q];
+        M.k[i] = __fadd_rn(M.k[i], (float)iv);
+    }
 }
 
 struct NodeOut {
     float *nu, *nxx, *nxy, *nxz, *nyz, *ro, *cp, *kt, *ht, *et, *tk, *rr, *tk1;
 };
 
-// normalisation (mark3mg.c:938-1002)
-__global__ void k_r2n_norm(const double *acc, long N, NodeOut O, int vm, double nubeg, double nuend)
+// node sums over the tile boxes holding the node (fixed tile order), then the normalisation of
+// mark3mg.c:938-1002
+__global__ void k_r2n_gather(const double *stage, TileGeo TG, int nx, int ny, int nz, NodeOut O, int vm, double nubeg,
+                             double nuend)
 {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long N = (long)nx * ny * nz;
     if (n >= N) return;
-#define ACC(a) acc[(long)(a) * N + n]
+    const int y = (int)(n % ny), x = (int)((n / ny) % nx), z = (int)(n / ((long)nx * ny));
+    int x0, x1, y0, y1, z0, z1;
+    box_range(x, TX, TG.ntx, x0, x1);
+    box_range(y, TY, TG.nty, y0, y1);
+    box_range(z, TZ, TG.ntz, z0, z1);
+    double acc[NACC];
+#pragma unroll
+    for (int a = 0; a < NACC; a++) acc[a] = 0;
+    for (int tz = z0; tz <= z1; tz++)
+        for (int tx = x0; tx <= x1; tx++)
+            for (int ty = y0; ty <= y1; ty++) {
+                const long tile = ((long)tz * TG.ntx + tx) * TG.nty + ty;
+                const double *b = stage + tile * NACC * NBOX + ((z - tz * TZ) * NBX + (x - tx * TX)) * NBY + (y - ty * TY);
+#pragma unroll
+                for (int a = 0; a < NACC; a++) acc[a] += b[a * NBOX];
+            }
+#define ACC(a) acc[a]
 #define FIN(field, A, W) if (ACC(W) > 0.01) { double v_ = ACC(A) / ACC(W); if (vm == 1) v_ = exp(v_); if (vm == 2) v_ = 1.0 / v_; O.field[n] = (float)v_; }
     FIN(nu, A_NU, W_NU);
     FIN(nxx, A_XX, W_XX);
@@ -1068,7 +1255,7 @@ static Phys phys_of(i3g_ctx *c)
 }
 
 static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
-static size_t r2n_smem(i3g_ctx *c) { return sizeof(double) * (NACC * NBOX + kR2nWarps * 32 * kStage) + grid_smem(c); }
+static size_t r2n_smem(i3g_ctx *c) { return sizeof(double) * (NACC * NBOX + kR2nWarps * 32 * kStage) + grid_smem(c) + sizeof(int) * kR2nWarps * 32; }
 static size_t heat_mark_smem(i3g_ctx *c) { return sizeof(double) * (2 * NBOX + kR2nWarps * 32 * kHmStage) + grid_smem(c); }
 
 int markers_alloc(i3g_ctx *c)
@@ -1091,7 +1278,8 @@ int markers_alloc(i3g_ctx *c)
     I3G_CUDA(cudaMalloc((void **)&S->cur, sizeof(int) * S->nbins));
     I3G_CUDA(cudaMalloc((void **)&S->off, sizeof(int) * (S->ntiles + 2)));
     I3G_CUDA(cudaMalloc((void **)&S->bsum, sizeof(int) * nchunks));
-    I3G_CUDA(cudaMalloc((void **)&S->acc, sizeof(double) * NACC * N));
+    I3G_CUDA(cudaMalloc((void **)&S->acc, sizeof(double) * 2 * N));
+    I3G_CUDA(cudaMalloc((void **)&S->stage, sizeof(double) * (size_t)S->ntiles * NACC * NBOX));
     I3G_CUDA(cudaMalloc((void **)&S->tk1, sizeof(float) * N));
     const int rn = c->m.rocknum;
     std::vector<double> rk(24 * (size_t)std::max(rn, 1), 0.0);
@@ -1124,6 +1312,17 @@ int markers_alloc(i3g_ctx *c)
         I3G_CUDA(cudaMemcpyAsync(S->tbc_c, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice, c->st));
         I3G_CUDA(cudaMemcpyAsync(S->tbc_k, tkk.data(), sizeof(double) * tkk.size(), cudaMemcpyHostToDevice, c->st));
     }
+    {
+        int dev = 0, sms = 0, per_sm = 0;
+        I3G_CUDA(cudaGetDevice(&dev));
+        I3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move, 256, grid_smem(c)));
+        S->move_blocks = (unsigned)std::max(1, sms * std::max(per_sm, 1));
+        int a = 0, b = 0;
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tile_key, 256, grid_smem(c)));
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_heat_mark_anti, 256, grid_smem(c)));
+        S->key_blocks = (unsigned)std::max(1, sms * std::max(std::min(a, b), 1));
+    }
     I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
     I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
     I3G_CUDA(cudaStreamSynchronize(c->st));
@@ -1135,32 +1334,62 @@ void markers_free(i3g_ctx *c)
 {
     MarkerState *S = ms(c);
     if (!S) return;
+    if (c->cst) cudaStreamSynchronize(c->cst);   // no upload may still target the buffers freed here
     free_marks(S->a);
     free_marks(S->b);
-    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->coff); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->bsum); cudaFree(S->acc); cudaFree(S->tk1);
+    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->coff); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->bsum); cudaFree(S->acc); cudaFree(S->stage); cudaFree(S->tk1);
     cudaFree(S->rock); cudaFree(S->err);
     if (S->herr) cudaFreeHost(S->herr);
+    if (S->up_ev) cudaEventDestroy(S->up_ev);
     cudaFree(S->tbc_node); cudaFree(S->tbc_p); cudaFree(S->tbc_c); cudaFree(S->tbc_k);
     delete S;
     c->mk = nullptr;
 }
 
-int markers_upload(i3g_ctx *c, const i3g_model *m)
+// make the compute stream wait for an asynchronous marker upload still in flight
+static int markers_wait(i3g_ctx *c)
+{
+    MarkerState *S = ms(c);
+    if (S && S->up_pending) {
+        I3G_CUDA(cudaStreamWaitEvent(c->st, S->up_ev, 0));
+        S->up_pending = false;
+    }
+    return 0;
+}
+
+int markers_upload(i3g_ctx *c, const i3g_model *m, bool async)
 {
     MarkerState *S = ms(c);
     if (!S) return 0;
     const long n = S->n;
     if (m->marknum != n) return set_error(c, I3G_E_ARG, "marker count changed (%lld != %ld)", (long long)m->marknum, n);
+    int rc = markers_wait(c);
+    if (rc) return rc;
+    cudaStream_t st = c->st;
+    if (async) {
+        // the copies may only overwrite the markers once all earlier work on them is done
+        if (!S->up_ev) I3G_CUDA(cudaEventCreateWithFlags(&S->up_ev, cudaEventDisableTiming));
+        I3G_CUDA(cudaEventRecord(S->up_ev, c->st));
+        I3G_CUDA(cudaStreamWaitEvent(c->cst, S->up_ev, 0));
+        st = c->cst;
+    }
     Marks &A = S->a;
     const float *src[12] = {m->markx, m->marky, m->markz, m->markk, m->markw, m->markd, m->markv, m->marke,
                             m->markex, m->markft, m->markrr, m->markrn};
     float *dst[12] = {A.x, A.y, A.z, A.k, A.w, A.d, A.v, A.e, A.ex, A.ft, A.rr, A.rn};
     for (int f = 0; f < 12; f++) {
-        if (src[f]) I3G_CUDA(cudaMemcpyAsync(dst[f], src[f], sizeof(float) * n, cudaMemcpyHostToDevice, c->st));
-        else I3G_CUDA(cudaMemsetAsync(dst[f], 0, sizeof(float) * n, c->st));
+        if (src[f]) I3G_CUDA(cudaMemcpyAsync(dst[f], src[f], sizeof(float) * n, cudaMemcpyHostToDevice, st));
+        else I3G_CUDA(cudaMemsetAsync(dst[f], 0, sizeof(float) * n, st));
     }
-    if (n) I3G_CUDA(cudaMemcpyAsync(A.t, m->markt, n, cudaMemcpyHostToDevice, c->st));
-    if (n) LAUNCH(k_iota, nb(n), 256, 0, A.id, n);
+    if (n) I3G_CUDA(cudaMemcpyAsync(A.t, m->markt, n, cudaMemcpyHostToDevice, st));
+    if (n) {
+        k_iota<<<nb(n), 256, 0, st>>>(A.id, n);
+        c->launches++;
+    }
+    if (async) {
+        I3G_CUDA(cudaEventRecord(S->up_ev, c->cst));
+        S->up_pending = true;
+    }
     S->sorted = false;
     return 0;
 }
@@ -1169,6 +1398,7 @@ int markers_download(i3g_ctx *c, i3g_model *m)
 {
     MarkerState *S = ms(c);
     if (!S || !S->n) return 0;
+    if (int rc = markers_wait(c)) return rc;
     const long n = S->n;
     LAUNCH(k_unsort, nb(n), 256, 0, S->a, S->b, n);
     Marks &B = S->b;
@@ -1199,12 +1429,14 @@ int markers_move(i3g_ctx *c, double timestep)
 {
     MarkerState *S = ms(c);
     if (!S->n || timestep == 0) return 0;
+    if (int rc = markers_wait(c)) return rc;
     EventPair ev;
     I3G_CUDA(ev.create());
     cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
-    LAUNCH(k_move, nb(S->n), 256, grid_smem(c), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c), timestep);
+    LAUNCH(k_move, std::min(nb(S->n), S->move_blocks), 256, grid_smem(c), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c),
+           timestep);
     I3G_CUDA(cudaGetLastError());
     I3G_CUDA(cudaEventRecord(e1, c->st));
     int rc = check_err(c, "movemark");
@@ -1223,7 +1455,7 @@ static int sort_markers(i3g_ctx *c)
     const long nbins = S->nbins;
     const unsigned nchunks = (unsigned)((nbins + kScanChunk - 1) / kScanChunk);
     I3G_CUDA(cudaMemsetAsync(S->cnt, 0, sizeof(int) * nbins, c->st));
-    LAUNCH(k_tile_key, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), T, S->key, S->cnt);
+    LAUNCH(k_tile_key, std::min(nb(n), S->key_blocks), 256, grid_smem(c), S->a, n, grid_of(c), T, S->key, S->cnt);
     LAUNCH(k_scan_part, nchunks, kScanT, 0, (const int *)S->cnt, nbins, S->bsum);
     LAUNCH(k_scan_top, 1, kScanT, 0, S->bsum, (int)nchunks);
     LAUNCH(k_scan_apply, nchunks, kScanT, 0, (const int *)S->cnt, nbins, (const int *)S->bsum, S->coff, S->cur);
@@ -1238,6 +1470,7 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
 {
     MarkerState *S = ms(c);
     const long N = c->nodenum;
+    if (int rc = markers_wait(c)) return rc;
     EventPair ev;
     I3G_CUDA(ev.create());
     cudaEvent_t e0 = ev.a, e1 = ev.b;
@@ -1246,13 +1479,15 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
     int rc = 0;
     if (S->n) rc = sort_markers(c);
     if (rc) return rc;
-    I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
     if (S->n)
         LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff, grid_of(c),
-               nodes_of(c), phys_of(c), T, timestep, S->acc, N);
+               nodes_of(c), phys_of(c), T, timestep, S->stage);
+    else
+        I3G_CUDA(cudaMemsetAsync(S->stage, 0, sizeof(double) * (size_t)S->ntiles * NACC * NBOX, c->st));
     NodeOut O{c->lev[0].nu, c->nxx, c->nxy, c->nxz, c->nyz, c->ro, c->cp, c->kt, c->ht, c->et, c->tk, c->rr, S->tk1};
-    LAUNCH(k_r2n_norm, nb(N), 256, 0, (const double *)S->acc, N, O, c->p.viscmod, c->p.nubeg, c->p.nuend);
+    LAUNCH(k_r2n_gather, nb(N), 256, 0, (const double *)S->stage, T, (int)c->m.xnumx, (int)c->m.ynumy, (int)c->m.znumz, O,
+           c->p.viscmod, c->p.nubeg, c->p.nuend);
     if (S->tbc_n)
         LAUNCH(k_tk_bc, nb(S->tbc_n), 256, 0, c->tk, (const float *)S->tk1, S->tbc_n, (const int *)S->tbc_node,
                (const int *)S->tbc_p, (const double *)S->tbc_c, (const double *)S->tbc_k);
@@ -1270,52 +1505,57 @@ int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const flo
 {
     MarkerState *S = ms(c);
     if (!S->n) return 0;
+    if (int rc = markers_wait(c)) return rc;
     const long N = c->nodenum;
     if (!S->sorted) {
         int rc = sort_markers(c);
         if (rc) return rc;
     }
-    I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * 2 * N, c->st));
     TkF T{tk0, tk1, c->tk, tk2, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
     TileGeo TG{S->ntx, S->nty, S->ntz, S->ntiles};
     LAUNCH(k_heat_mark_cells, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
-           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->acc, N);
+           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
     if (c->p.heatdif != 0) {
-        LAUNCH(k_heat_mark_norm, nb(N), 256, 0, S->acc, N);
-        LAUNCH(k_heat_mark_anti, nb(S->n), 256, grid_smem(c), S->a, (const int *)S->off, S->ntiles, grid_of(c), T,
-               (const double *)S->acc, N);
+        LAUNCH(k_heat_mark_gather, nb(N), 256, 0, (const double *)S->stage, TG, (int)c->m.xnumx, (int)c->m.ynumy,
+               (int)c->m.znumz, S->acc, N);
+        LAUNCH(k_heat_mark_anti, std::min(nb(S->n), S->key_blocks), 256, grid_smem(c), S->a, (const int *)S->off,
+               S->ntiles, grid_of(c), T, (const double *)S->acc, N);
     }
     I3G_CUDA(cudaGetLastError());
     return 0;
 }
 
+// Kernel timing with an empty L2 before every repetition (cold_time).  Bytes per launch are the
+// algorithmic bytes per unit: 4 marker -> node sums (k_r2n_cells): 25 B per marker (x, y, z,
+// type, T, viscosity, rr) + 48 B per node (12 FP32 outputs); 5 RK4 advection (k_move): 45 B per
+// marker + 13 nodal FP32 fields; 9 marker temperature update (k_heat_mark_cells): 42 B per marker.
 int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *bytes)
 {
     MarkerState *S = ms(c);
     const long n = S->n, N = c->nodenum;
-    EventPair ev;
-    I3G_CUDA(ev.create());
-    cudaEvent_t e0 = ev.a, e1 = ev.b;
+    if (int rc = markers_wait(c)) return rc;
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
     if (!S->sorted) { int rc = sort_markers(c); if (rc) return rc; }
-    I3G_CUDA(cudaEventRecord(e0, c->st));
-    for (int r = 0; r < reps; r++) {
-        if (kind == 4) {
-            I3G_CUDA(cudaMemsetAsync(S->acc, 0, sizeof(double) * NACC * N, c->st));
+    TkF TK{c->tk, c->tk, c->tk, c->tk, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
+    auto launch = [&]() -> int {
+        if (kind == 4)
             LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff,
-                   grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->acc, N);
-        } else {
-            LAUNCH(k_move, nb(n), 256, grid_smem(c), S->a, n, grid_of(c), nodes_of(c), phys_of(c), 0.0);
-        }
-    }
-    I3G_CUDA(cudaEventRecord(e1, c->st));
-    I3G_CUDA(cudaEventSynchronize(e1));
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    *ms_out = t / reps;
-    // compulsory bytes: marker fields read/written once, node fields read/written once
-    if (kind == 4) *bytes = (double)n * (4.0 * 6 + 1 + 4) + (double)N * (8.0 + NACC * 8.0);
-    else *bytes = (double)n * (4.0 * 9 + 1 + 4.0 * 9) + (double)N * (4.0 * 15 + 8.0);
+                   grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->stage);
+        else if (kind == 9)
+            LAUNCH(k_heat_mark_cells, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
+                   TK, T, 1e10, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
+        else
+            LAUNCH(k_move, std::min(nb(n), S->move_blocks), 256, grid_smem(c), S->a, n, grid_of(c), nodes_of(c), phys_of(c),
+                   0.0);
+        return 0;
+    };
+    launch();   // warm-up
+    int rc = cold_time(c, reps, launch, ms_out);
+    if (rc) return rc;
+    if (kind == 4) *bytes = (double)n * 25.0 + (double)N * 48.0;
+    else if (kind == 9) *bytes = (double)n * 42.0;
+    else *bytes = (double)n * 45.0 + (double)N * 13.0 * 4.0;
+    I3G_CUDA(cudaGetLastError());
     return 0;
 }
 

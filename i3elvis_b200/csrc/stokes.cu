@@ -2195,7 +2195,13 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     return 0;
 }
 
-// Timing of single kernel classes on level 0 with CUDA events on the context stream.
+// Timing of kernel classes on level 0 with an empty L2 before every repetition (cold_time).
+// Bytes are the algorithmic (compulsory) bytes of the unit timed: per node of level 0,
+//   0 / 7  one colour of Vx (FP64 / FP32): vx, vy, vz, P and three viscosity arrays read, the
+//          right-hand side and the writes of half the rows, the boundary mask;
+//   8 / 10 one full sweep (FP32 / FP64: Vx, Vy, Vz red and black, boundary rows, pressure):
+//          4 unknowns read and written, 4 right-hand sides read, 5 FP32 viscosities: 68 / 116 B;
+//   1      FP64 residual: 116 B;  2  restriction: 4 s (1 + 1/8) B;  3  prolongation: 4 s (2 + 1/8) B.
 int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes)
 {
     if (!c->stokes_ready) {
@@ -2204,49 +2210,35 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
     }
     Level &L = c->lev[0];
     const double N = (double)L.n;
-    EventPair ev;
-    I3G_CUDA(ev.create());
-    cudaEvent_t e0 = ev.a, e1 = ev.b;
     View<double> V = view<double>(L, L.d);
     View<float> Vf = view<float>(L, L.s);
     const long total = (long)((L.ny + 1) / 2) * L.nx * L.nz;
-    // warm-up
-    for (int w = 0; w < 3; w++) {
-        if (kind == 0) LAUNCH((k_relax_vel<double, 1>), nblk(total), 256, V, 0, c->p.v0koef);
-        else if (kind == 7) LAUNCH((k_relax_vel<float, 1>), nblk(total), 256, Vf, 0, (float)c->p.v0koef);
-        else if (kind == 1) LAUNCH(k_residual<double>, nblk(L.n), 256, V);
-        else if (kind == 2 && c->nlev > 1) restrict_t<double>(c, 1);
-        else if (kind == 3 && c->nlev > 1) prolong_t<double>(c, 1);
-    }
-    I3G_CUDA(cudaEventRecord(e0, c->st));
-    for (int r = 0; r < reps; r++) {
-        if (kind == 0) LAUNCH((k_relax_vel<double, 1>), nblk(total), 256, V, r & 1, c->p.v0koef);
-        else if (kind == 7) LAUNCH((k_relax_vel<float, 1>), nblk(total), 256, Vf, r & 1, (float)c->p.v0koef);
-        else if (kind == 1) LAUNCH(k_residual<double>, nblk(L.n), 256, V);
-        else if (kind == 2 && c->nlev > 1) restrict_t<double>(c, 1);
-        else if (kind == 3 && c->nlev > 1) prolong_t<double>(c, 1);
-    }
-    I3G_CUDA(cudaEventRecord(e1, c->st));
-    I3G_CUDA(cudaEventSynchronize(e1));
-    float t = 0;
-    cudaEventElapsedTime(&t, e0, e1);
-    *ms = t / reps;
-    // compulsory bytes of one launch (each datum read or written once)
+    int r = 0;
+    auto launch = [&]() -> int {
+        switch (kind) {
+        case 0: LAUNCH((k_relax_vel<double, 1>), nblk(total), 256, V, r & 1, c->p.v0koef); break;
+        case 7: LAUNCH((k_relax_vel<float, 1>), nblk(total), 256, Vf, r & 1, (float)c->p.v0koef); break;
+        case 8: smooth_t<float>(c, 0, 1, true, false); break;
+        case 10: smooth_t<double>(c, 0, 1, false, false); break;
+        case 1: LAUNCH(k_residual<double>, nblk(L.n), 256, V); break;
+        case 2: if (c->nlev > 1) restrict_t<double>(c, 1); break;
+        case 3: if (c->nlev > 1) prolong_t<double>(c, 1); break;
+        default: break;
+        }
+        r++;
+        return 0;
+    };
+    for (int w = 0; w < 2; w++) launch();   // warm-up (instruction caches, first-touch)
+    int rc = cold_time(c, reps, launch, ms);
+    if (rc) return rc;
     switch (kind) {
-    case 0:   // one colour of Vx: vx, vy, vz, P, eta c/xy/xz read; rhs and writes of half the rows; bc mask
-        *bytes = N * (8.0 * 7 + 8.0 * 0.5 + 8.0 * 0.5 + 1.0); break;
-    case 7:
-        *bytes = N * (4.0 * 7 + 4.0 * 0.5 + 4.0 * 0.5 + 1.0); break;
-    case 1:   // residual: 4 unknowns, 4 rhs, 4 eta read, 4 residuals written, nd unused, bc mask
-        *bytes = N * (8.0 * 4 + 8.0 * 4 + 8.0 * 4 + 8.0 * 4 + 1.0); break;
-    case 2: { // restriction: fine residuals + bc mask + nd read, coarse rhs + sol written
-        const double Nc = (double)c->lev[1].n;
-        *bytes = N * (8.0 * 4 + 1.0 + 4.0) + Nc * (8.0 * 8 + 4.0); break;
-    }
-    case 3: { // prolongation: fine sol read+write, coarse sol read
-        const double Nc = (double)c->lev[1].n;
-        *bytes = N * 8.0 * 4 * 2 + Nc * 8.0 * 4; break;
-    }
+    case 0: *bytes = N * (8.0 * 7 + 8.0 * 0.5 + 8.0 * 0.5 + 1.0); break;
+    case 7: *bytes = N * (4.0 * 7 + 4.0 * 0.5 + 4.0 * 0.5 + 1.0); break;
+    case 8: *bytes = N * 68.0; break;
+    case 10: *bytes = N * 116.0; break;
+    case 1: *bytes = N * 116.0; break;
+    case 2: *bytes = N * 4.0 * 8.0 * (1.0 + 1.0 / 8.0); break;
+    case 3: *bytes = N * 4.0 * 8.0 * (2.0 + 1.0 / 8.0); break;
     default: *bytes = 0;
     }
     I3G_CUDA(cudaGetLastError());

@@ -382,3 +382,49 @@ def random_inclusions(n=129, size_km=200.0, mnum=3, multinum=4, seed=7, count=10
         d2 = ((x[idx] - cen[i, 0]) ** 2 + (y[idx] - cen[i, 1]) ** 2 + (z[idx] - cen[i, 2]) ** 2)
         types[idx[d2 <= r * r]] = INCLUSION_TYPES[tbin[i]]
     return make_prn(spec, rocks, types, xyz, seed), spec
+
+
+LITHO, SLAB, WEAK = 3, 4, 5
+
+
+def subduction(nx=257, ny=129, nz=257, size_km=(1000.0, 500.0, 1000.0), mnum=3, multinum=4, seed=11,
+               litho_km=100.0, weak_km=10.0, dip_deg=45.0, trench_frac=0.35, slab_depth_km=300.0,
+               cohesion=1e7, friction=0.6, mantle_eta=(1e19, 1e22), activation=3e5):
+    """Visco-plastic subduction-like model (x and z horizontal, y vertical and downward).
+
+    * lithosphere: the top ``litho_km``, eta 1e24, rho 3300, Drucker-Prager yielding
+      sigma_y = cohesion + friction * P (viscalc's brittle branch, mark3mg.c:1148-1198);
+    * slab: a lithosphere-thick plate dipping at ``dip_deg`` from the trench at
+      x = ``trench_frac`` * xsize down to ``slab_depth_km``, rho 3350 (+50), eta 1e24, yielding;
+    * weak layer: ``weak_km`` on top of the slab and along the trench, eta 1e19;
+    * mantle: Arrhenius eta = A exp(E / RT) (viscalc branch B, mark3mg.c:1281-1299) with E =
+      ``activation``, A set so that the mantle's temperatures span ``mantle_eta`` (clamps
+      n0 / n1 = ``mantle_eta``), rho 3300;
+    * free slip on all walls, T linear from 273 K at the top to 1573 K at the bottom.
+    The slab extends over the whole z range (a plate boundary along z)."""
+    Lx, Ly, Lz = (s * 1e3 for s in size_km)
+    spec = ModelSpec(shape=(nx, ny, nz), size=(Lx, Ly, Lz), mnum=(mnum,) * 3, multinum=multinum)
+    xyz = build_markers(spec, seed)
+    x, y = (a.astype(np.float64) for a in xyz[:2])
+    # Arrhenius prefactor: eta(T_bottom) = mantle_eta[0] at the bottom temperature
+    A = mantle_eta[0] / np.exp(activation / (8.314 * spec.t_bottom))
+    mantle = Rock(nu=A, dh=activation, mm=1.0, n0=mantle_eta[0], n1=mantle_eta[1], ro=3300.0)
+    plastic = dict(a0=cohesion, a1=cohesion, b0=friction, b1=friction, e0=0.0, e1=1.0)
+    rocks = {MATRIX: mantle,
+             LITHO: Rock(nu=1e24, n0=1e18, n1=1e24, ro=3300.0, **plastic),
+             SLAB: Rock(nu=1e24, n0=1e18, n1=1e24, ro=3350.0, **plastic),
+             WEAK: Rock(nu=1e19, n0=1e18, n1=1e24, ro=3300.0)}
+    H, W = litho_km * 1e3, weak_km * 1e3
+    xt = trench_frac * Lx
+    t = np.tan(np.radians(dip_deg))
+    c = np.cos(np.radians(dip_deg))
+    # distance below the slab's upper surface y_s(x) = (x - xt) * tan(dip), measured normal to it
+    dn = (y - (x - xt) * t) * c
+    in_slab_x = x >= xt
+    types = np.full(x.size, MATRIX, np.int8)
+    types[y <= H] = LITHO
+    slab = in_slab_x & (dn >= 0) & (dn <= H) & (y <= slab_depth_km * 1e3)
+    types[slab & (y > H)] = SLAB
+    weak = in_slab_x & (dn < 0) & (dn >= -W) & (y <= slab_depth_km * 1e3)
+    types[weak] = WEAK
+    return make_prn(spec, rocks, types, xyz, seed), spec

@@ -168,8 +168,14 @@ int i3g_markers_to_nodes(i3g_ctx *c, double timestep);
 /* Advance model time (i3mg.c:146). */
 int i3g_add_time(i3g_ctx *c, double timestep);
 
-/* Host <-> device copies of the model arrays.  mask: I3G_SYNC_* bits. */
-enum { I3G_SYNC_NODES = 1, I3G_SYNC_STRESS = 2, I3G_SYNC_MARKERS = 4, I3G_SYNC_ALL = 7 };
+/* Host <-> device copies of the model arrays.  mask: I3G_SYNC_* bits.
+ * I3G_SYNC_ASYNC (upload only): the marker copies run on the context's copy stream and i3g_upload
+ * returns once the nodal copies are done; the Stokes solve then overlaps the marker copies, and
+ * the first call that needs the markers (i3g_heat's marker update, i3g_move_markers,
+ * i3g_markers_to_nodes, a marker download) waits for them on the device.  The host marker
+ * arrays must stay unchanged until such a call has returned.  (The reference keeps the state in
+ * static arrays and copies nothing: head3mg.c:33-101.) */
+enum { I3G_SYNC_NODES = 1, I3G_SYNC_STRESS = 2, I3G_SYNC_MARKERS = 4, I3G_SYNC_ALL = 7, I3G_SYNC_ASYNC = 8 };
 int i3g_download(i3g_ctx *c, i3g_model *m, unsigned mask);
 int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask);
 

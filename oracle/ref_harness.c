@@ -18,6 +18,7 @@
  *   r2n PREFIX                 ronurecalc() on the loaded markers; writes PREFIX.nodes
  *   mover2n DT PREFIX          loads PREFIX.fields, movemark(), ronurecalc(); marks + nodes
  *   titerate DT PREFIX [CAP]   loads PREFIX.fields, titerate(0) (at most CAP iteration blocks); marks + nodes
+ *   steps RTOL MAXC REPS PREP HEATCAP [DT]   whole timed steps, V-cycles to RTOL (see below)
  *   step OUT.prn               one full i3mg time step (i3mg.c:80-147), wall time per phase
  */
 #include <stdio.h>
@@ -138,6 +139,7 @@ static void relres(double *mom, double *cont)
 {
     long m, e;
     double rb = 0, bb = 0, rc = 0, vv = 0, nc = 0, nv = 0, h;
+#pragma omp parallel for private(e) reduction(+ : rb, bb, rc, vv, nc, nv) schedule(static)
     for (m = 0; m < mgn[0] * 4; m++) {
         if (!num0[m]) continue;
         if (m % 4) { vv += sol0[m] * sol0[m]; nv += 1; }
@@ -254,14 +256,22 @@ static void prepare_state(void)
     timestep = ts;
 }
 
-/* Level-0 velocities from sol0 into vx, vy, vz (move3mg.c:2246-2317) and the marker time
- * step limit maxxystep / max|v| (move3mg.c:2608-2632). */
+/* Level-0 pressure and velocities from sol0 into pr, vx, vy, vz (move3mg.c:2246-2317) and the
+ * marker time step limit maxxystep / max|v| (move3mg.c:2608-2632). */
 static double sample_vmax = 0;
 
 static void velocities_and_cfl(void)
 {
     long m1, m2, m3, n;
     double vmax[3] = {0, 0, 0};
+    /* pressure shifted to pinit in the pinning cell (move3mg.c:2248-2269) */
+    const double ival = pinit - sol0[(pzinit * xynumxy + pxinit * ynumy + pyinit) * 4];
+    for (m3 = 1; m3 < znumz; m3++)
+        for (m1 = 1; m1 < xnumx; m1++)
+            for (m2 = 1; m2 < ynumy; m2++) {
+                n = m3 * xynumxy + m1 * ynumy + m2;
+                pr[n] = sol0[4 * n] + ival;
+            }
     for (m3 = 0; m3 < znumz; m3++)
         for (m1 = 0; m1 < xnumx; m1++)
             for (m2 = 0; m2 < ynumy; m2++) {
@@ -458,6 +468,78 @@ int main(int argc, char **argv)
                    "\"heat_blocks\": %ld, \"threads\": %d}\n",
                    r, t1 - t0, (t2 - t1) / (ncyc > 0 ? ncyc : 1), ncyc, t3 - t2, t4 - t3, t5 - t4, tp, timestep,
                    sample_vmax, i3g_heat_blocks + 1, omp_get_max_threads());
+            fflush(stdout);
+        }
+        return 0;
+    }
+    if (!strcmp(cmd, "steps") && argc >= 7) {
+        /* Whole time steps of the reference on all OpenMP threads, timed by wall clock:
+         * STEPS RTOL MAXC REPS PREP HEATCAP [DT].  Optionally the initial-condition passes first
+         * (PREP=1, timed apart).  Then REPS times: vpiterate's set-up (ronurestrict and row
+         * assembly, move3mg.c:1948-2159); V-cycles (move3mg.c:2170-2223), each followed by the
+         * relative residual of the level-0 rows, until momentum and continuity are <= RTOL or
+         * MAXC cycles; after the file row's multstp cycles (fl0cyc[0][2]) -- or as soon as the
+         * residual is 30 times above the best one seen, the divergence the library also
+         * reacts to -- the row's second relaxation set (move3mg.c:2585-2593); the velocities
+         * and CFL time step (or DT seconds when given), titerate (at most HEATCAP iteration
+         * blocks), movemark, ronurecalc.  One JSON line per repetition. */
+        const double rtol = atof(argv[2]);
+        const int maxc = atoi(argv[3]);
+        const int reps = atoi(argv[4]);
+        if (atol(argv[6]) > 0) i3g_heat_block_cap = atol(argv[6]);
+        const double dt_fixed = argc >= 8 ? atof(argv[7]) : 0.0;
+        double tp = 0;
+        if (atoi(argv[5])) {
+            double a = omp_get_wtime();
+            prepare_state();
+            tp = omp_get_wtime() - a;
+        }
+        fprintf(stderr, "steps: prepared in %.1f s\n", tp);
+        for (int r = 0; r < reps; r++) {
+            timestep = maxtmstep;
+            p0koef = fl0stp[0][5];
+            p1koef = fl0stp[0][6];
+            multinum = fl0cyc[0][1];
+            double t0 = omp_get_wtime();
+            stokes_assemble();
+            double t1 = omp_get_wtime();
+            double mom = 0, cont = 0, best = 1e300, rel0;
+            relres(&mom, &cont);
+            rel0 = fmax(mom, cont);
+            int ncyc = 0, switched = 0;
+            while (ncyc < maxc && !(mom <= rtol && cont <= rtol)) {
+                vcycle();
+                ncyc++;
+                relres(&mom, &cont);
+                const double cur = fmax(mom, cont);
+                if (!(cur == cur)) break;
+                if (cur < best) best = cur;
+                if (!switched && (ncyc >= fl0cyc[0][2] || cur > 30.0 * best)) {
+                    multinum = fl0cyc[0][3];
+                    p0koef = fl0stp[0][8];
+                    p1koef = fl0stp[0][9];
+                    switched = 1;
+                    best = cur;
+                }
+            }
+            double t2 = omp_get_wtime();
+            fprintf(stderr, "steps %d: set-up %.1f s, %d V-cycles %.1f s, rel %.3e\n", r, t1 - t0, ncyc, t2 - t1, fmax(mom, cont));
+            velocities_and_cfl();
+            if (dt_fixed > 0) timestep = dt_fixed;
+            i3g_heat_blocks = 0;
+            if (tempmod) titerate(0);
+            double t3 = omp_get_wtime();
+            if (markmod) movemark();
+            double t4 = omp_get_wtime();
+            if (gridmod) ronurecalc();
+            double t5 = omp_get_wtime();
+            timesum += timestep;
+            printf("{\"rep\": %d, \"step_s\": %.4f, \"assemble_s\": %.4f, \"stokes_s\": %.4f, \"ncyc\": %d, "
+                   "\"rel0\": %.3e, \"rel\": %.3e, \"switched\": %d, \"heat_s\": %.4f, \"move_s\": %.4f, "
+                   "\"r2n_s\": %.4f, \"prepare_s\": %.4f, \"timestep\": %.6e, \"vmax\": %.3e, \"heat_blocks\": %ld, "
+                   "\"threads\": %d}\n",
+                   r, t5 - t0, t1 - t0, t2 - t1, ncyc, rel0, fmax(mom, cont), switched, t3 - t2, t4 - t3, t5 - t4, tp,
+                   timestep, sample_vmax, i3g_heat_blocks + 1, omp_get_max_threads());
             fflush(stdout);
         }
         return 0;

@@ -106,3 +106,20 @@ def test_stresses_match_reference(name):
         err = float(np.abs(got.astype(np.float64) - ref).max()) / scale
         print(name, f, "differing entries", nbad, "max |diff| / max |ref|", err)
         assert err <= 1e-6, (name, f, nbad, err)
+
+
+def test_async_marker_upload_gives_the_same_step():
+    """An upload whose marker copies overlap the Stokes solve (I3G_SYNC_ASYNC) leaves the time
+    step bit-identical to a synchronous upload of the same host state."""
+    out = []
+    for mask in (abi.SYNC_NODES | abi.SYNC_MARKERS, abi.SYNC_NODES | abi.SYNC_MARKERS | abi.SYNC_ASYNC):
+        p, mode, fx, buf = marker_setup("sphere13")
+        g = lib.Context(buf, abi.make_params(mode, stokes_rtol=1e-10), abi.make_file_params(mode.files[0]))
+        runtime.time_step(g, mode, mode.files[0], 0)   # device state moves away from the host's
+        g.upload(mask)
+        runtime.time_step(g, mode, mode.files[0], 1)
+        g.download(abi.SYNC_ALL)
+        out.append({f: buf.f32[f].copy() for f in ("markx", "marky", "markk", "markv", "tk", "vx", "nu")})
+        g.close()
+    for f in out[0]:
+        np.testing.assert_array_equal(out[0][f], out[1][f], err_msg=f)
