@@ -326,7 +326,8 @@ def main():
         logs.append(runtime.time_step(ctx, mode, f, args.warmup + i))
         st = ctx.stats()
         cycles.append(st["stokes_cycles"])
-        logs[-1].update({k: st[k] for k in ("stokes_cycles", "stokes_rel", "ms_stokes", "ms_heat", "ms_move", "ms_r2n")})
+        logs[-1].update({k: st[k] for k in ("stokes_cycles", "stokes_rel", "ms_stokes", "ms_heat", "ms_move", "ms_r2n",
+                                            "heat_cycles")})
     ms = ctx.timer_stop()
     barrier()
     clk = clocks.stop()
@@ -377,19 +378,38 @@ def main():
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_value = max_over_ranks(e2e_s, world, "cuda") / world
 
-    # roofline of the dominant kernel: the multicolour Stokes relaxation of this precision
-    kind = 7 if prec == 1 else 0
-    kms, kbytes = ctx.time_kernel(kind, 20)
+    # rooflines of the step's main kernels, each timed live with an empty L2 before every launch
+    # (library's cold-cache timer) against the algorithmic bytes of SURVEY section 8(d); the
+    # dominant kernel is the one with the most device time per step
     peak, peak_src = peaks()
-    achieved = kbytes / (kms * 1e-3) / 1e9
-    traffic = None
+    traffic_tab = {}
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
             with open(tf) as fh:
-                traffic = json.load(fh).get(args.workload, {}).get("relax_vel_" + args.precision)
+                traffic_tab = json.load(fh).get(args.workload, {})
         except Exception:
-            traffic = None
+            traffic_tab = {}
+    cyc = float(np.mean(cycles[args.warmup:])) if cycles[args.warmup:] else 0.0
+    heat_cyc = float(np.mean([lg.get("heat_cycles", 0) for lg in logs])) if logs else 0.0
+    sweeps0 = mode.multinnn[0][0] + mode.multinnn[1][0]
+    specs = [("stokes_sweep_" + ("f32" if prec else "f64"), 8 if prec else 10, sweeps0 * cyc,
+              "one level-0 multicolour sweep, %s (k_relax_vel x6, k_relax_p, boundary rows)" % ("FP32" if prec else "FP64"),
+              "68 B/node FP32" if prec else "116 B/node FP64"),
+             ("k_move", 5, 1.0, "RK4 marker advection", "45 B/marker + 13 nodal FP32 fields"),
+             ("k_r2n_cells", 4, 1.0, "marker -> node sums", "25 B/marker + 48 B/node"),
+             ("k_heat_mark_cells", 9, 1.0, "marker temperature update", "42 B/marker"),
+             ("heat_sweep", 6, 4.0 * heat_cyc, "one level-0 heat sweep (k_heat_relax x2)", "32 B/node")]
+    kernels = []
+    for name, kind, per_step, what, unit_bytes in specs:
+        kms, kbytes = ctx.time_kernel(kind, 10)
+        ach = kbytes / (kms * 1e-3) / 1e9
+        tr = traffic_tab.get(name)
+        kernels.append({"kernel": name, "what": what, "algorithmic_bytes": unit_bytes, "ms_per_launch": kms,
+                        "bytes_per_launch": kbytes, "achieved": ach, "frac": ach / peak, "launches_per_step": per_step,
+                        "ms_per_step": kms * per_step, "traffic": tr})
+    dom = max(kernels, key=lambda k: k["ms_per_step"])
+    log("rooflines: " + ", ".join(f"{k['kernel']} {k['ms_per_launch']:.3f} ms {k['frac']:.2f}" for k in kernels))
     out = {
         "metric": METRIC, "value": value, "unit": "s/step", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
@@ -403,9 +423,11 @@ def main():
         "gpu_launches": int(launches),
         "fp64_multigrid": fp64_mg,
         "e2e": {"value": e2e_value, "unit": "s/step", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "kernel": "k_relax_vel<%s>" % ("float" if prec else "double"),
-                     "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "bytes_per_launch": kbytes, "ms_per_launch": kms},
+        "roofline": {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": dom["frac"], "traffic": dom["traffic"],
+                     "bytes_per_launch": dom["bytes_per_launch"], "ms_per_launch": dom["ms_per_launch"],
+                     "ms_per_step": dom["ms_per_step"], "l2": "flushed before every timed launch"},
+        "kernels": kernels,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

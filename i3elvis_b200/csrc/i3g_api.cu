@@ -270,6 +270,23 @@ int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask)
     return 0;
 }
 
+void *i3g_host_alloc(int64_t bytes)
+{
+    if (bytes <= 0) return nullptr;
+    void *p = nullptr;
+    if (cudaMallocHost(&p, (size_t)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    memset(p, 0, (size_t)bytes);
+    return p;
+}
+
+void i3g_host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+}
+
 int i3g_get_stats(const i3g_ctx *c, i3g_stats *s)
 {
     if (!c || !s) return I3G_E_ARG;

@@ -1655,13 +1655,39 @@ struct KrylovState {
     double *part = nullptr;  // partial dot products [blocks][kKryNq]
     double *hdev = nullptr;  // [3][kKryNq]: first and second projection, squared norm; then 2 weights
     double *hhost = nullptr; // pinned mirror of hdev
+    double *save = nullptr;  // FP64 preconditioner: level-0 solution and right-hand side set aside (8N)
     cudaGraphExec_t g[kKryMax] = {};
     long g_nodes[kKryMax] = {};   // kernels per captured step
-    int g_multinum = -1;
+    int g_multinum = -1, g_prec = -1;
     double g_p0 = 0, g_p1 = 0, g_v0 = 0, g_v1 = 0;
 };
 
 static KrylovState *kry(i3g_ctx *c) { return (KrylovState *)c->kry; }
+
+// FP64 preconditioner input: the vector to precondition (in the residual arrays) becomes the
+// right-hand side of the correction system, zero on boundary rows, with a zero start
+__global__ void k_corr64_in(long n, const double *r0, const double *r1, const double *r2, const double *r3, double *f0,
+                            double *f1, double *f2, double *f3, double *u0, double *u1, double *u2, double *u3,
+                            const uint8_t *bc)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint8_t b = bc[t];
+    f0[t] = (b & 1) ? 0.0 : r0[t];
+    f1[t] = (b & 2) ? 0.0 : r1[t];
+    f2[t] = (b & 4) ? 0.0 : r2[t];
+    f3[t] = (b & 8) ? 0.0 : r3[t];
+    u0[t] = 0.0; u1[t] = 0.0; u2[t] = 0.0; u3[t] = 0.0;
+}
+
+__global__ void k_kr_store64(long N, double *z, const double *e0, const double *e1, const double *e2, const double *e3)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    z[t] = e0[t]; z[N + t] = e1[t]; z[2 * N + t] = e2[t]; z[3 * N + t] = e3[t];
+}
 
 // d[0] = velocity-row weight, d[1] = pressure-row weight (device, so that the captured steps
 // stay valid when the weights change between restarts)
@@ -1840,14 +1866,8 @@ __global__ void __launch_bounds__(256) k_guess_dots(View<double> L, const double
 static int kry_alloc(i3g_ctx *c, int m)
 {
     KrylovState *K = kry(c);
-    if (K && K->m == m) return 0;
-    if (K) {
-        for (int j = 0; j < kKryMax; j++) if (K->g[j]) cudaGraphExecDestroy(K->g[j]);
-        cudaFree(K->V); cudaFree(K->Z); cudaFree(K->W); cudaFree(K->F0); cudaFree(K->part); cudaFree(K->hdev);
-        cudaFreeHost(K->hhost);
-        delete K;
-        c->kry = nullptr;
-    }
+    if (K && K->m == m && (K->save || c->p.precision != 0)) return 0;
+    if (K) kry_free(c);
     K = new KrylovState();
     c->kry = K;
     K->m = m;
@@ -1859,6 +1879,7 @@ static int kry_alloc(i3g_ctx *c, int m)
     ALLOC(K->F0, double, n4);
     ALLOC(K->part, double, (long)c->red_blocks * kKryNq);
     ALLOC(K->hdev, double, 3 * kKryNq + 2);
+    if (c->p.precision == 0) ALLOC(K->save, double, 2 * n4);
     I3G_CUDA(cudaMallocHost((void **)&K->hhost, (3 * kKryNq + 2) * sizeof(double)));
     I3G_CUDA(cudaMemsetAsync(K->W, 0, n4 * 8, c->st));
     I3G_CUDA(cudaMemsetAsync(K->F0, 0, n4 * 8, c->st));
@@ -1871,6 +1892,7 @@ static void kry_free(i3g_ctx *c)
     if (!K) return;
     for (int j = 0; j < kKryMax; j++) if (K->g[j]) cudaGraphExecDestroy(K->g[j]);
     cudaFree(K->V); cudaFree(K->Z); cudaFree(K->W); cudaFree(K->F0); cudaFree(K->part); cudaFree(K->hdev);
+    cudaFree(K->save);
     cudaFreeHost(K->hhost);
     delete K;
     c->kry = nullptr;
@@ -1895,20 +1917,39 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
     Level &L0 = c->lev[0];
     const long N = K->N, n4 = 4 * N;
     double *vj = K->V + (long)j * n4, *zj = K->Z + (long)j * n4;
-    // preconditioner: the FP32 V-cycle on the unscaled vector
+    // preconditioner: the V-cycle of this precision on the unscaled vector
     const double *d = K->hdev + 3 * kKryNq;
     LAUNCH(k_kr_to_r, nblk(N), 256, N, (const double *)vj, L0.d.r[0], L0.d.r[1], L0.d.r[2], L0.d.r[3], d);
     const int nb = c->red_blocks;
-    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], N, c->dred);
-    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], N, c->dred + nb);
-    LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], N, c->dred + 2 * nb);
-    LAUNCH(k_scale, 1, 1024, (const double *)c->dred, 3 * nb, c->h_ref, c->eta_ref, c->dscale);
-    LAUNCH(k_to_f32, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
-           (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
-           L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, (const double *)c->dscale);
-    vcycle_t<float>(c, multinum, true);
-    LAUNCH(k_kr_store, nblk(N), 256, N, zj, (const float *)L0.s.u[0], (const float *)L0.s.u[1],
-           (const float *)L0.s.u[2], (const float *)L0.s.u[3], (const double *)c->dscale);
+    if (c->p.precision == 0) {
+        // FP64 V-cycle from zero on level 0's own arrays, whose solution and right-hand side
+        // are set aside meanwhile (no scaling: the system is already FP64)
+        for (int v = 0; v < 4; v++) {
+            I3G_CUDA(cudaMemcpyAsync(K->save + v * N, L0.d.u[v], N * 8, cudaMemcpyDeviceToDevice, c->st));
+            I3G_CUDA(cudaMemcpyAsync(K->save + (4 + v) * N, L0.d.f[v], N * 8, cudaMemcpyDeviceToDevice, c->st));
+        }
+        LAUNCH(k_corr64_in, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+               (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.d.f[0], L0.d.f[1], L0.d.f[2], L0.d.f[3],
+               L0.d.u[0], L0.d.u[1], L0.d.u[2], L0.d.u[3], (const uint8_t *)L0.bc);
+        vcycle_t<double>(c, multinum, true);
+        LAUNCH(k_kr_store64, nblk(N), 256, N, zj, (const double *)L0.d.u[0], (const double *)L0.d.u[1],
+               (const double *)L0.d.u[2], (const double *)L0.d.u[3]);
+        for (int v = 0; v < 4; v++) {
+            I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], K->save + v * N, N * 8, cudaMemcpyDeviceToDevice, c->st));
+            I3G_CUDA(cudaMemcpyAsync(L0.d.f[v], K->save + (4 + v) * N, N * 8, cudaMemcpyDeviceToDevice, c->st));
+        }
+    } else {
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[1], N, c->dred);
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[2], N, c->dred + nb);
+        LAUNCH(k_max_abs, nb, 256, (const double *)L0.d.r[3], N, c->dred + 2 * nb);
+        LAUNCH(k_scale, 1, 1024, (const double *)c->dred, 3 * nb, c->h_ref, c->eta_ref, c->dscale);
+        LAUNCH(k_to_f32, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
+               (const double *)L0.d.r[2], (const double *)L0.d.r[3], L0.s.f[0], L0.s.f[1], L0.s.f[2], L0.s.f[3],
+               L0.s.u[0], L0.s.u[1], L0.s.u[2], L0.s.u[3], (const uint8_t *)L0.bc, (const double *)c->dscale);
+        vcycle_t<float>(c, multinum, true);
+        LAUNCH(k_kr_store, nblk(N), 256, N, zj, (const float *)L0.s.u[0], (const float *)L0.s.u[1],
+               (const float *)L0.s.u[2], (const float *)L0.s.u[3], (const double *)c->dscale);
+    }
     // w = D A z_j: the FP64 residual of z_j with a zero right-hand side is -A z_j
     View<double> Vz = view<double>(L0, L0.d);
     Vz.u0 = zj; Vz.u1 = zj + N; Vz.u2 = zj + 2 * N; Vz.u3 = zj + 3 * N;
@@ -1939,10 +1980,10 @@ static int kry_graph(i3g_ctx *c, int j, int multinum)
 {
     KrylovState *K = kry(c);
     if (K->g_multinum != multinum || K->g_p0 != c->p.p0koef || K->g_p1 != c->p.p1koef || K->g_v0 != c->p.v0koef ||
-        K->g_v1 != c->p.v1koef) {
+        K->g_v1 != c->p.v1koef || K->g_prec != c->p.precision) {
         for (int q = 0; q < kKryMax; q++) if (K->g[q]) { cudaGraphExecDestroy(K->g[q]); K->g[q] = nullptr; }
         K->g_multinum = multinum; K->g_p0 = c->p.p0koef; K->g_p1 = c->p.p1koef; K->g_v0 = c->p.v0koef;
-        K->g_v1 = c->p.v1koef;
+        K->g_v1 = c->p.v1koef; K->g_prec = c->p.precision;
     }
     if (K->g[j]) return 0;
     const int64_t l0 = c->launches;
@@ -2117,7 +2158,7 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     double best = std::max(mom, cont);
     bool switched = false;
     static const bool trace = getenv("I3G_TRACE") != nullptr;   // per-cycle residuals on stderr
-    if (c->p.precision == 1 && c->p.krylov > 0) {
+    if (c->p.krylov > 0) {
         if (c->p.krylov > kKryMax) return set_error(c, I3G_E_ARG, "krylov restart length %d above %d", c->p.krylov, kKryMax);
         if ((rc = kry_alloc(c, c->p.krylov))) return rc;
         if (!c->dscale) I3G_CUDA(cudaMalloc((void **)&c->dscale, 16 * sizeof(double)));

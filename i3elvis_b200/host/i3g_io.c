@@ -47,6 +47,60 @@ static int failf(char *err, const char *fmt, ...)
 
 static void *xcalloc(long n, long size) { return calloc(n > 0 ? n : 1, size); }
 
+static void *(*g_alloc)(int64_t) = NULL;
+static void (*g_release)(void *) = NULL;
+
+void prn_set_allocator(void *(*alloc)(int64_t bytes), void (*release)(void *))
+{
+    g_alloc = alloc && release ? alloc : NULL;
+    g_release = alloc && release ? release : NULL;
+}
+
+/* large arrays: the installed allocator (page-locked memory in the host loop), else calloc */
+static void *big_alloc(const prn_file *p, long n, long size)
+{
+    if (p->release != free && g_alloc) return g_alloc((int64_t)(n > 0 ? n : 1) * size);
+    return xcalloc(n, size);
+}
+
+static void big_free(const prn_file *p, void *a)
+{
+    if (a) (p->release ? p->release : free)(a);
+}
+
+/* the large arrays of an image */
+static int alloc_arrays(prn_file *p, long nn, long mn)
+{
+    p->release = g_alloc ? g_release : free;
+    p->pr = (double *)big_alloc(p, nn, 8);
+    int ok = p->pr != NULL;
+    for (int f = 0; f < 15; f++) ok &= (p->node[f] = (float *)big_alloc(p, nn, 4)) != NULL;
+    for (int f = 0; f < 12; f++) ok &= (p->stress[f] = (float *)big_alloc(p, nn, 4)) != NULL;
+    for (int f = 0; f < 12; f++) ok &= (p->mark[f] = (float *)big_alloc(p, mn, 4)) != NULL;
+    ok &= (p->markt = (int8_t *)big_alloc(p, mn, 1)) != NULL;
+    return ok ? 0 : -1;
+}
+
+/* i3g_model pointers of an image to its own arrays */
+static void bind_model(prn_file *p)
+{
+    i3g_model *m = &p->m;
+    for (int t = 0; t < 24; t++) m->rock[t] = p->rock[t];
+    m->gx = p->gxf; m->gy = p->gyf; m->gz = p->gzf;
+    m->pr = p->pr;
+    float **nf[15] = {&m->vx, &m->vy, &m->vz, &m->ro, &m->nu, &m->nxx, &m->nxy, &m->nxz, &m->nyz,
+                      &m->tk, &m->cp, &m->et, &m->kt, &m->ht, &m->rr};
+    for (int f = 0; f < 15; f++) *nf[f] = p->node[f];
+    float **sf[12] = {&m->exx, &m->eyy, &m->ezz, &m->exy, &m->exz, &m->eyz,
+                      &m->sxx, &m->syy, &m->szz, &m->sxy, &m->sxz, &m->syz};
+    for (int f = 0; f < 12; f++) *sf[f] = p->stress[f];
+    m->bond_row = p->brow; m->bond_c = p->bc; m->bond_k = p->bk; m->bond_partner1 = p->bp1;
+    float **mf[12] = {&m->markx, &m->marky, &m->markz, &m->markk, &m->markw, &m->markd, &m->markv,
+                      &m->marke, &m->markex, &m->markft, &m->markrr, &m->markrn};
+    for (int f = 0; f < 12; f++) *mf[f] = p->mark[f];
+    m->markt = p->markt;
+}
+
 int prn_read(const char *path, prn_file *p, char *err)
 {
     memset(p, 0, sizeof *p);
@@ -79,9 +133,7 @@ int prn_read(const char *path, prn_file *p, char *err)
         RD(p->rock[t], 8, rn);
         m->rock[t] = p->rock[t];
     }
-    p->pr = (double *)xcalloc(nn, 8);
-    for (int f = 0; f < 15; f++) p->node[f] = (float *)xcalloc(nn, 4);
-    for (int f = 0; f < 12; f++) p->stress[f] = (float *)xcalloc(nn, 4);
+    if (alloc_arrays(p, nn, mn)) { fclose(fl); prn_free(p); return failf(err, "%s: out of host memory", path); }
     {
         const long chunk = 1 << 16;
         float *buf = (float *)malloc(sizeof(float) * 16 * chunk);
@@ -102,8 +154,6 @@ int prn_read(const char *path, prn_file *p, char *err)
     for (long b = 0; b < bn; b++) {
         RD(&p->brow[b], 8, 1); RD(&p->bond_id[b], 8, 1); RD(&p->bc[b], 4, 1); RD(&p->bk[b], 4, 1); RD(&p->bp1[b], 8, 1);
     }
-    for (int f = 0; f < 12; f++) p->mark[f] = (float *)xcalloc(mn, 4);
-    p->markt = (int8_t *)xcalloc(mn, 1);
     {
         const long chunk = 1 << 16;
         unsigned char *buf = (unsigned char *)malloc(49 * chunk);
@@ -118,19 +168,32 @@ int prn_read(const char *path, prn_file *p, char *err)
         free(buf);
     }
     fclose(fl);
-    m->gx = p->gxf; m->gy = p->gyf; m->gz = p->gzf;
-    m->pr = p->pr;
-    float **nf[15] = {&m->vx, &m->vy, &m->vz, &m->ro, &m->nu, &m->nxx, &m->nxy, &m->nxz, &m->nyz,
-                      &m->tk, &m->cp, &m->et, &m->kt, &m->ht, &m->rr};
-    for (int f = 0; f < 15; f++) *nf[f] = p->node[f];
-    float **sf[12] = {&m->exx, &m->eyy, &m->ezz, &m->exy, &m->exz, &m->eyz,
-                      &m->sxx, &m->syy, &m->szz, &m->sxy, &m->sxz, &m->syz};
-    for (int f = 0; f < 12; f++) *sf[f] = p->stress[f];
-    m->bond_row = p->brow; m->bond_c = p->bc; m->bond_k = p->bk; m->bond_partner1 = p->bp1;
-    float **mf[12] = {&m->markx, &m->marky, &m->markz, &m->markk, &m->markw, &m->markd, &m->markv,
-                      &m->marke, &m->markex, &m->markft, &m->markrr, &m->markrn};
-    for (int f = 0; f < 12; f++) *mf[f] = p->mark[f];
-    m->markt = p->markt;
+    bind_model(p);
+    return 0;
+}
+
+int prn_alloc_like(const prn_file *src, prn_file *p, char *err)
+{
+    memset(p, 0, sizeof *p);
+    p->m = src->m;
+    p->cycle = src->cycle;
+    p->gridcur = src->gridcur;
+    p->gridtot = src->gridtot;
+    const i3g_model *m = &src->m;
+    const long rn = m->rocknum, nn = (long)(m->xnumx * m->ynumy * m->znumz), bn = (long)m->bondnum, mn = (long)m->marknum;
+    for (int t = 0; t < 24; t++) {
+        p->rock[t] = (double *)xcalloc(rn, 8);
+        memcpy(p->rock[t], src->rock[t], 8 * rn);
+    }
+    p->gxf = (float *)xcalloc(m->xnumx, 4); p->gyf = (float *)xcalloc(m->ynumy, 4); p->gzf = (float *)xcalloc(m->znumz, 4);
+    memcpy(p->gxf, src->gxf, 4 * m->xnumx); memcpy(p->gyf, src->gyf, 4 * m->ynumy); memcpy(p->gzf, src->gzf, 4 * m->znumz);
+    p->brow = (int64_t *)xcalloc(bn, 8); p->bond_id = (int64_t *)xcalloc(bn, 8); p->bp1 = (int64_t *)xcalloc(bn, 8);
+    p->bc = (float *)xcalloc(bn, 4); p->bk = (float *)xcalloc(bn, 4);
+    memcpy(p->brow, src->brow, 8 * bn); memcpy(p->bp1, src->bp1, 8 * bn);
+    memcpy(p->bc, src->bc, 4 * bn); memcpy(p->bk, src->bk, 4 * bn);
+    if (src->bond_id) memcpy(p->bond_id, src->bond_id, 8 * bn);
+    if (alloc_arrays(p, nn, mn)) { prn_free(p); return failf(err, "out of host memory for a staging image"); }
+    bind_model(p);
     return 0;
 }
 
@@ -194,13 +257,13 @@ int prn_write(const char *path, const prn_file *p, char *err)
 void prn_free(prn_file *p)
 {
     for (int t = 0; t < 24; t++) free(p->rock[t]);
-    free(p->pr);
-    for (int f = 0; f < 15; f++) free(p->node[f]);
-    for (int f = 0; f < 12; f++) free(p->stress[f]);
+    big_free(p, p->pr);
+    for (int f = 0; f < 15; f++) big_free(p, p->node[f]);
+    for (int f = 0; f < 12; f++) big_free(p, p->stress[f]);
     free(p->gxf); free(p->gyf); free(p->gzf);
     free(p->brow); free(p->bond_id); free(p->bp1); free(p->bc); free(p->bk);
-    for (int f = 0; f < 12; f++) free(p->mark[f]);
-    free(p->markt);
+    for (int f = 0; f < 12; f++) big_free(p, p->mark[f]);
+    big_free(p, p->markt);
     memset(p, 0, sizeof *p);
 }
 

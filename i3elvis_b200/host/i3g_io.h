@@ -27,11 +27,21 @@ typedef struct prn_file {
     float *mark[12];                    /* x y z k w d v e ex ft rr rn                      */
     int8_t *markt;
     double *rock[24];
+    void (*release)(void *);            /* frees the nodal and marker arrays (set by prn_read) */
 } prn_file;
+
+/* Allocator of the large arrays (nodes, stresses, markers) of the images that prn_read and
+ * prn_alloc_like make from now on; NULL restores calloc/free.  The host loop passes
+ * i3g_host_alloc / i3g_host_free so that uploads and downloads run at full bus speed from
+ * page-locked memory.  The allocator must return zeroed memory or NULL. */
+void prn_set_allocator(void *(*alloc)(int64_t bytes), void (*release)(void *));
 
 /* 0 on success; on failure -1 with a message in err[256]. */
 int prn_read(const char *path, prn_file *p, char *err);
 int prn_write(const char *path, const prn_file *p, char *err);
+/* An image with the header, grid, rocks and boundary records of src and its own (zeroed)
+ * nodal, stress and marker arrays: the staging image of an asynchronous save. */
+int prn_alloc_like(const prn_file *src, prn_file *p, char *err);
 void prn_free(prn_file *p);
 
 #define MODE_MAXFILES 1000

@@ -13,12 +13,49 @@
  *     Stokes (vpiterate) -> heat (titerate) -> markers (movemark) -> nodes (ronurecalc)
  * (i3mg.c:80-147), then saver and file.t3c.  Solver controls that the reference does not
  * have (relative stopping tolerances, precision) come from the command line.
+ *
+ * Saving overlaps the computation: the model images live in page-locked memory, each output
+ * file's state is downloaded into a staging image, and a writer thread writes the .prn file and
+ * then file.t3c (so a restart never names an incomplete file) while the GPU already runs the
+ * next file's steps.  The reference writes synchronously inside the loop (i3mg.c:150-160).
  */
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include "i3g_io.h"
+
+/* one asynchronous save: the staging image, its file name and the file.t3c index after it */
+typedef struct saver_job {
+    prn_file img;
+    char name[256];
+    int next_index;
+    int busy, rc;
+    char err[256];
+    pthread_t th;
+} saver_job;
+
+static void *saver_run(void *arg)
+{
+    saver_job *j = (saver_job *)arg;
+    j->rc = prn_write(j->name, &j->img, j->err);
+    if (!j->rc && file_t3c_write("file.t3c", j->next_index)) {
+        snprintf(j->err, sizeof j->err, "cannot write file.t3c");
+        j->rc = -1;
+    }
+    return NULL;
+}
+
+/* wait for the save in flight; non-zero if it failed */
+static int saver_wait(saver_job *j)
+{
+    if (!j->busy) return 0;
+    pthread_join(j->th, NULL);
+    j->busy = 0;
+    if (j->rc) fprintf(stderr, "i3g: %s\n", j->err);
+    return j->rc;
+}
 
 static int check(int rc, i3g_ctx *c, const char *what)
 {
@@ -98,8 +135,16 @@ int main(int argc, char **argv)
     const char *infile = md.infile;
     if (fln3 >= 0 && fln3 < md.nfiles) infile = md.files[fln3].name;
     else fln3 = -1;
+    /* page-locked images when a GPU is there (calloc otherwise: the allocator returns NULL) */
+    void *probe = i3g_host_alloc(1);
+    if (probe) {
+        i3g_host_free(probe);
+        prn_set_allocator(i3g_host_alloc, i3g_host_free);
+    }
     prn_file p;
     if (prn_read(infile, &p, err)) { fprintf(stderr, "i3g: %s\n", err); return 1; }
+    static saver_job sv;
+    if (prn_alloc_like(&p, &sv.img, err)) { fprintf(stderr, "i3g: %s\n", err); prn_free(&p); return 1; }
     md.p.stokes_rtol = rtol;
     md.p.stokes_maxcyc = maxcyc;
     md.p.heat_rtol = heat_rtol;
@@ -144,13 +189,23 @@ int main(int argc, char **argv)
             }
         }
         if (rc) break;
-        if ((rc = check(i3g_download(c, &p.m, I3G_SYNC_ALL), c, "i3g_download"))) break;
-        p.cycle = F->fp.cyc0max - 1;
-        if (prn_write(F->name, &p, err)) { fprintf(stderr, "i3g: %s\n", err); rc = 1; break; }
-        if (file_t3c_write("file.t3c", f0 + 1)) { fprintf(stderr, "i3g: cannot write file.t3c\n"); rc = 1; break; }
-        if (P->printmod) printf("\n saved %s\n", F->name);
+        /* the previous file's writer must be done with the staging image */
+        if ((rc = saver_wait(&sv))) break;
+        if ((rc = check(i3g_download(c, &sv.img.m, I3G_SYNC_ALL), c, "i3g_download"))) break;
+        sv.img.cycle = F->fp.cyc0max - 1;
+        snprintf(sv.name, sizeof sv.name, "%s", F->name);
+        sv.next_index = f0 + 1;
+        if (pthread_create(&sv.th, NULL, saver_run, &sv)) {
+            saver_run(&sv);   /* no thread: write in line */
+            if ((rc = sv.rc)) { fprintf(stderr, "i3g: %s\n", sv.err); break; }
+        } else {
+            sv.busy = 1;
+        }
+        if (P->printmod) printf("\n saving %s\n", F->name);
     }
+    if (saver_wait(&sv)) rc = 1;
     i3g_destroy(c);
+    prn_free(&sv.img);
     prn_free(&p);
     return rc ? 1 : 0;
 }

@@ -103,9 +103,11 @@ typedef struct i3g_params {
     int32_t warm_start;                 /* 0: zero start; 1: the previous step's v,P (reference behaviour);
                                          * 2: linear extrapolation in time from the last two converged
                                          * solutions (falls back to 1 until two exist; reset by i3g_upload) */
-    int32_t krylov;                     /* precision 1 only: > 0 accelerates the FP64 defect correction
-                                         * with FGMRES(krylov) preconditioned by the FP32 V-cycle (<= 16);
-                                         * 0: one V-cycle per correction, the reference's iteration */
+    int32_t krylov;                     /* > 0: restarted FGMRES(krylov) (<= 16) on the FP64 residual,
+                                         * preconditioned by one V-cycle of this precision (precision 1:
+                                         * the FP32 V-cycle on the scaled correction system; precision 0:
+                                         * the FP64 V-cycle); 0: one V-cycle per iteration, the
+                                         * reference's iteration (with FP64 defect correction for 1) */
 } i3g_params;
 
 /* ---- per output file row (load3mg.c:25-58, applied at i3mg.c:64-77) ---------------- */
@@ -180,6 +182,13 @@ int i3g_download(i3g_ctx *c, i3g_model *m, unsigned mask);
 int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask);
 
 int i3g_get_stats(const i3g_ctx *c, i3g_stats *s);
+
+/* Page-locked host memory for model images (no reference counterpart: the reference keeps
+ * its state in static arrays, head3mg.c:33-101).  Uploads and downloads from such buffers run
+ * at full bus speed and asynchronously to the host thread.  Returns zeroed memory, or NULL
+ * (also without a GPU); free with i3g_host_free. */
+void *i3g_host_alloc(int64_t bytes);
+void i3g_host_free(void *p);
 
 /* ---- kernel-level entry points (parity tests and benchmarks) ------------------------- */
 /* Level arrays addressable by i3g_get_array / i3g_set_array (element type in brackets). */

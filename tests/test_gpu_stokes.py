@@ -105,12 +105,12 @@ def _compare_to_reference(p, sol, ref, tol):
     return errs
 
 
-@pytest.mark.parametrize("precision,krylov", [(0, 0), (1, 0), (1, 8)])
+@pytest.mark.parametrize("precision,krylov", [(0, 0), (0, 8), (1, 0), (1, 8)])
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_solve_matches_reference(name, precision, krylov):
     """Converged velocity and pressure equal the reference's converged FP64 solution to
-    relative L2 1e-8 (FP64 multigrid; FP32 multigrid inside FP64 defect correction, plain and
-    FGMRES-accelerated).  Cases: sinking spheres (13^3, 17^3, the 33^3 CPU-runnable benchmark
+    relative L2 1e-8 (FP64 multigrid, plain and as the FGMRES preconditioner; FP32 multigrid
+    inside FP64 defect correction, plain and FGMRES-accelerated).  Cases: sinking spheres (13^3, 17^3, the 33^3 CPU-runnable benchmark
     configuration, whose own bar is 1e-6), Arrhenius inclusions, Drucker-Prager yielding and a
     non-uniform grid."""
     p, mode, fx = golden(name)
