@@ -189,6 +189,12 @@ int main(int argc, char **argv)
             }
         }
         if (rc) break;
+        /* ParaView output every 50th file (saver_paraview, i3mg.c:159) */
+        if ((f0 + 1) % 50 == 0) {
+            char vtr[300];
+            snprintf(vtr, sizeof vtr, "%s.vtr", F->name);
+            if ((rc = check(i3g_write_vtr(c, vtr), c, "i3g_write_vtr"))) break;
+        }
         /* the previous file's writer must be done with the staging image */
         if ((rc = saver_wait(&sv))) break;
         if ((rc = check(i3g_download(c, &sv.img.m, I3G_SYNC_ALL), c, "i3g_download"))) break;

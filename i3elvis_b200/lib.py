@@ -52,6 +52,7 @@ def load():
     L.i3g_set_array.argtypes = [P, C.c_int, C.c_int, C.c_void_p, C.c_int64]
     L.i3g_stokes_setup.argtypes = [P]
     L.i3g_stokes_stresses.argtypes = [P]
+    L.i3g_write_vtr.argtypes = [P, C.c_char_p]
     for name in ("i3g_stokes_residual", "i3g_stokes_restrict", "i3g_stokes_prolong", "i3g_stokes_vcycles"):
         getattr(L, name).argtypes = [P, C.c_int]
     L.i3g_stokes_smooth.argtypes = [P, C.c_int, C.c_int]
@@ -145,6 +146,10 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self.call("i3g_stokes_relres", C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def write_vtr(self, path: str):
+        """ParaView rectilinear-grid file of the nodal fields (``i3g_write_vtr``)."""
+        self.call("i3g_write_vtr", os.fsencode(path))
 
     def timer_start(self):
         self.call("i3g_timer", 0, None)

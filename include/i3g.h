@@ -190,6 +190,13 @@ int i3g_get_stats(const i3g_ctx *c, i3g_stats *s);
 void *i3g_host_alloc(int64_t bytes);
 void i3g_host_free(void *p);
 
+/* ParaView output of the nodal fields (saver_paraview's nodal part, i3vis_output_paraview.c:
+ * 700-792 and 887-975, called every 50th output file at i3mg.c:159): a VTK XML RectilinearGrid
+ * file with raw appended data -- Float64 grid lines, then viscosity, temperature, density, vy,
+ * vx, vz (Float32) and pressure (Float64) in VTK point order (x fastest), reordered on the GPU
+ * from the device arrays. */
+int i3g_write_vtr(i3g_ctx *c, const char *path);
+
 /* ---- kernel-level entry points (parity tests and benchmarks) ------------------------- */
 /* Level arrays addressable by i3g_get_array / i3g_set_array (element type in brackets). */
 enum {
