@@ -169,6 +169,10 @@ struct i3g_ctx {
     double *dscale = nullptr;                   // device scale factors of the FP32 correction solve
     void *flush = nullptr;                      // 256 MiB written between cold-cache timings (L2 is 126 MB)
     long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
+    long coop_nodes = 0;                        // > 0: levels up to this size run in the cooperative coarse kernel
+    int coop_blocks = 0;                        // its grid: every CTA resident at once (0: no cooperative launch)
+    unsigned *dbar = nullptr;                   // its grid barrier: arrival count, generation
+    int *dbar_err = nullptr;                    // set when a grid barrier wait timed out
     double *hist[2][4] = {};                    // last two converged level-0 solutions (warm_start 2)
     double hist_dt[2] = {0, 0};                 // time steps taken after them
     int nhist = 0;

@@ -499,98 +499,163 @@ __device__ __forceinline__ T *comp(const View<T> &L, int v)
     return v == 0 ? L.u0 : v == 1 ? L.u1 : v == 2 ? L.u2 : L.u3;
 }
 
-template <typename T>
-__device__ void tail_bc(const TailLevel<T> &TL, int v)
+// The threads that run the tail, and their barrier: one block (the one-block tail kernel) or the
+// whole co-resident grid of a cooperative launch (the coarse-level kernel).
+struct BlockTeam {
+    __device__ __forceinline__ long rank() const { return threadIdx.x; }
+    __device__ __forceinline__ long size() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident by construction).  The last CTA
+// to arrive resets the counter and advances the generation; the others wait for the generation,
+// each for at most 2 s (then the launch's error flag is set and the wait gives up, so a broken
+// launch can never hang the GPU; the host reports the flag as an error).
+struct GridTeam {
+    unsigned *count;
+    unsigned *gen;
+    int *err;
+    __device__ __forceinline__ long rank() const { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ __forceinline__ long size() const { return (long)gridDim.x * blockDim.x; }
+    __device__ void sync() const
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned *vg = gen;
+            const unsigned g = *vg;   // cannot advance before this CTA arrives
+            __threadfence();
+            if (atomicAdd(count, 1u) == gridDim.x - 1) {
+                atomicExch(count, 0u);
+                __threadfence();
+                atomicAdd(gen, 1u);
+            } else {
+                uint64_t t0;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+                while (*vg == g) {
+                    uint64_t t;
+                    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                    if (t - t0 > 2000000000ull) {
+                        atomicOr(err, 1);
+                        break;
+                    }
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+};
+
+template <typename T, typename Team>
+__device__ void tail_bc(const TailLevel<T> &TL, int v, const Team &tm)
 {
     const BcDev &B = TL.bc[v];
-    if (B.n == 0) return;   // uniform over the block
+    if (B.n == 0) return;   // uniform over the team
     T *u = comp(TL.v, v);
-    for (int t = threadIdx.x; t < B.n; t += blockDim.x) bc_apply_at<T>(u, t, B.node, B.pnode, B.depth, B.c, B.k, 0);
-    __syncthreads();
+    for (long t = tm.rank(); t < B.n; t += tm.size()) bc_apply_at<T>(u, (int)t, B.node, B.pnode, B.depth, B.c, B.k, 0);
+    tm.sync();
 }
 
-template <typename T, int V>
-__device__ void tail_colours(const TailLevel<T> &TL, T v0)
+template <typename T, int V, typename Team>
+__device__ void tail_colours(const TailLevel<T> &TL, T v0, const Team &tm)
 {
     const View<T> &L = TL.v;
     const long total = (long)((L.ny + 1) >> 1) * L.nx * L.nz;
     for (int color = 0; color < 2; color++) {
-        for (long t = threadIdx.x; t < total; t += blockDim.x) relax_vel_at<T, V>(L, t, color, v0);
-        __syncthreads();
+        for (long t = tm.rank(); t < total; t += tm.size()) relax_vel_at<T, V>(L, t, color, v0);
+        tm.sync();
     }
-    tail_bc<T>(TL, V);
+    tail_bc<T>(TL, V, tm);
 }
 
-template <typename T>
-__device__ void tail_smooth(const TailLevel<T> &TL, int nsweeps, T v0, T p0)
+template <typename T, typename Team>
+__device__ void tail_smooth(const TailLevel<T> &TL, int nsweeps, T v0, T p0, const Team &tm)
 {
     const View<T> &L = TL.v;
     const long N = L.nxy * L.nz;
     for (int s = 0; s < nsweeps; s++) {
-        tail_colours<T, 1>(TL, v0);
-        tail_colours<T, 2>(TL, v0);
-        tail_colours<T, 3>(TL, v0);
-        for (long n = threadIdx.x; n < N; n += blockDim.x) relax_p_at<T>(L, n, p0);
-        __syncthreads();
-        tail_bc<T>(TL, 0);
+        tail_colours<T, 1>(TL, v0, tm);
+        tail_colours<T, 2>(TL, v0, tm);
+        tail_colours<T, 3>(TL, v0, tm);
+        for (long n = tm.rank(); n < N; n += tm.size()) relax_p_at<T>(L, n, p0);
+        tm.sync();
+        tail_bc<T>(TL, 0, tm);
     }
 }
 
-template <typename T>
-__device__ void tail_residual(const TailLevel<T> &TL)
+template <typename T, typename Team>
+__device__ void tail_residual(const TailLevel<T> &TL, const Team &tm)
 {
     const View<T> &L = TL.v;
     const long N = L.nxy * L.nz;
-    for (long n = threadIdx.x; n < N; n += blockDim.x) residual_at<T>(L, n);
+    for (long n = tm.rank(); n < N; n += tm.size()) residual_at<T>(L, n);
     for (int v = 0; v < 4; v++) {
         const BcDev &B = TL.bc[v];
-        for (int t = threadIdx.x; t < B.n; t += blockDim.x) bc_residual_at<T>(L, v, t, B.node, B.onode, B.ocomp, B.ok);
+        for (long t = tm.rank(); t < B.n; t += tm.size()) bc_residual_at<T>(L, v, (int)t, B.node, B.onode, B.ocomp, B.ok);
     }
-    __syncthreads();
+    tm.sync();
 }
 
-template <typename T>
-__device__ void tail_restrict(const TailLevel<T> &F, const TailLevel<T> &C)
+template <typename T, typename Team>
+__device__ void tail_restrict(const TailLevel<T> &F, const TailLevel<T> &C, const Team &tm)
 {
     const long N = C.v.nxy * C.v.nz;
-    for (long n = threadIdx.x; n < N; n += blockDim.x) {
+    for (long n = tm.rank(); n < N; n += tm.size()) {
         restrict_at<T, 1>(F.v, C.v, F.tr[1][0], F.tr[1][1], F.tr[1][2], n);
         restrict_at<T, 2>(F.v, C.v, F.tr[2][0], F.tr[2][1], F.tr[2][2], n);
         restrict_at<T, 3>(F.v, C.v, F.tr[3][0], F.tr[3][1], F.tr[3][2], n);
         restrict_at<T, 0>(F.v, C.v, F.tr[0][0], F.tr[0][1], F.tr[0][2], n);
     }
-    __syncthreads();
+    tm.sync();
 }
 
-template <typename T>
-__device__ void tail_prolong(const TailLevel<T> &F, const TailLevel<T> &C, T kv, T kp)
+template <typename T, typename Team>
+__device__ void tail_prolong(const TailLevel<T> &F, const TailLevel<T> &C, T kv, T kp, const Team &tm)
 {
     const long N = F.v.nxy * F.v.nz;
-    for (long n = threadIdx.x; n < N; n += blockDim.x) {
+    for (long n = tm.rank(); n < N; n += tm.size()) {
         prolong_at<T, 1>(F.v, C.v, F.tr[1][0], F.tr[1][1], F.tr[1][2], kv, n);
         prolong_at<T, 2>(F.v, C.v, F.tr[2][0], F.tr[2][1], F.tr[2][2], kv, n);
         prolong_at<T, 3>(F.v, C.v, F.tr[3][0], F.tr[3][1], F.tr[3][2], kv, n);
         prolong_at<T, 0>(F.v, C.v, F.tr[0][0], F.tr[0][1], F.tr[0][2], kp, n);
     }
-    __syncthreads();
+    tm.sync();
 }
 
 // Levels a.L[0..nl-1] (fine to coarse) of the V-cycle schedule of move3mg.c:2173-2213, from
 // the down sweeps of a.L[0] to its up sweeps.
+template <typename T, typename Team>
+__device__ void tail_body(const TailArgs<T> &a, const Team &tm)
+{
+    for (int q = 0; q + 1 < a.nl; q++) {
+        if (a.L[q].down > 0) tail_smooth<T>(a.L[q], a.L[q].down, a.v0, a.p0, tm);
+        tail_residual<T>(a.L[q], tm);
+        tail_restrict<T>(a.L[q], a.L[q + 1], tm);
+    }
+    for (int q = a.nl - 1; q > 0; q--) {
+        if (a.L[q].up > 0) tail_smooth<T>(a.L[q], a.L[q].up, a.v0, a.p0, tm);
+        tail_prolong<T>(a.L[q - 1], a.L[q], a.kv, a.kp, tm);
+    }
+    if (a.L[0].up > 0) tail_smooth<T>(a.L[0], a.L[0].up, a.v0, a.p0, tm);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_constant__ TailArgs<T> a)
 {
     pdl_enter();
-    for (int q = 0; q + 1 < a.nl; q++) {
-        if (a.L[q].down > 0) tail_smooth<T>(a.L[q], a.L[q].down, a.v0, a.p0);
-        tail_residual<T>(a.L[q]);
-        tail_restrict<T>(a.L[q], a.L[q + 1]);
-    }
-    for (int q = a.nl - 1; q > 0; q--) {
-        if (a.L[q].up > 0) tail_smooth<T>(a.L[q], a.L[q].up, a.v0, a.p0);
-        tail_prolong<T>(a.L[q - 1], a.L[q], a.kv, a.kp);
-    }
-    if (a.L[0].up > 0) tail_smooth<T>(a.L[0], a.L[0].up, a.v0, a.p0);
+    tail_body<T>(a, BlockTeam());
+}
+
+// The same schedule over the whole grid of a cooperative launch: every phase spreads its rows
+// over all resident threads and ends at a grid barrier instead of a kernel boundary, so the
+// coarse levels run as one launch without being confined to one SM.
+constexpr int kCoopThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kCoopThreads) k_vcycle_coop(const __grid_constant__ TailArgs<T> a, GridTeam tm)
+{
+    pdl_enter();
+    tail_body<T>(a, tm);
 }
 
 // ronurestrict (move3mg.c:2642-2741): FP32 accumulator as in nu[], FP64 weights
@@ -1055,6 +1120,22 @@ int stokes_alloc(i3g_ctx *c)
 {
     // size limit of the one-block V-cycle tail (I3G_TAIL_NODES=0 turns it off)
     if (const char *e = getenv("I3G_TAIL_NODES")) c->tail_nodes = atol(e);
+    // cooperative coarse-level kernel: levels up to this size (I3G_COOP_NODES, 0 = off) run in
+    // one launch over the whole grid; its size is what every SM can hold at once
+    if (const char *e = getenv("I3G_COOP_NODES")) c->coop_nodes = atol(e);
+    {
+        int dev = 0, sms = 0, coop = 0, a = 0, b = 0;
+        I3G_CUDA(cudaGetDevice(&dev));
+        I3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        I3G_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_vcycle_coop<float>, kCoopThreads, 0));
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_vcycle_coop<double>, kCoopThreads, 0));
+        c->coop_blocks = coop ? sms * std::min(a, b) : 0;
+        I3G_CUDA(cudaMalloc((void **)&c->dbar, 2 * sizeof(unsigned)));
+        I3G_CUDA(cudaMalloc((void **)&c->dbar_err, sizeof(int)));
+        I3G_CUDA(cudaMemsetAsync(c->dbar, 0, 2 * sizeof(unsigned), c->st));
+        I3G_CUDA(cudaMemsetAsync(c->dbar_err, 0, sizeof(int), c->st));
+    }
     // level geometry (gridcheck, load3mg.c:1220-1282)
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
@@ -1134,6 +1215,10 @@ static void kry_free(i3g_ctx *c);
 
 void stokes_free(i3g_ctx *c)
 {
+    cudaFree(c->dbar);
+    cudaFree(c->dbar_err);
+    c->dbar = nullptr;
+    c->dbar_err = nullptr;
     stokes_graph_free(c);
     kry_free(c);
     for (int h = 0; h < 2; h++)
@@ -1297,12 +1382,15 @@ static void prolong_t(i3g_ctx *c, int l)
 }
 
 // First level of the one-block tail: the coarsest levels (>= 1) with at most tail_nodes nodes;
-// multinum + 1 when none qualifies.
+// multinum + 1 when none qualifies.  With the cooperative coarse-level kernel enabled
+// (coop_nodes > 0) the same rule applies with its larger size limit, and all those levels run in
+// that kernel instead.
 static int tail_start(const i3g_ctx *c, int multinum)
 {
+    const long lim = c->coop_nodes > 0 && c->coop_blocks > 0 ? c->coop_nodes : c->tail_nodes;
     int lc = multinum + 1;
     for (int l = multinum; l >= 1 && l > multinum - kTailMax; l--) {
-        if (c->lev[l].n > c->tail_nodes) break;
+        if (c->lev[l].n > lim) break;
         lc = l;
     }
     return lc;
@@ -1327,6 +1415,22 @@ static void tail_launch(i3g_ctx *c, int lc, int multinum)
         }
         TL.down = c->p.multinnn[0][lc + q];
         TL.up = c->p.multinnn[1][lc + q];
+    }
+    if (c->coop_nodes > 0 && c->coop_blocks > 0) {
+        // one cooperative launch over all resident CTAs; the barrier counter starts at zero
+        cudaMemsetAsync(c->dbar, 0, 2 * sizeof(unsigned), c->st);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)c->coop_blocks);
+        cfg.blockDim = dim3(kCoopThreads);
+        cfg.stream = c->st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_vcycle_coop<T>, a, GridTeam{c->dbar, c->dbar + 1, c->dbar_err});
+        c->launches++;
+        return;
     }
     LAUNCH(k_vcycle_tail<T>, 1, kTailThreads, a);
 }
@@ -2232,6 +2336,11 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     c->st_.ms_stokes = ms;
+    if (c->dbar_err && c->coop_nodes > 0) {
+        int berr = 0;
+        I3G_CUDA(cudaMemcpy(&berr, c->dbar_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (berr) return set_error(c, I3G_E_CUDA, "Stokes: a grid barrier of the coarse-level kernel timed out");
+    }
     if (!conv) return set_error(c, I3G_E_NOCONV, "Stokes: %d V-cycles without reaching relative residual %g (mom %.3e cont %.3e)", cycles, rtol, mom, cont);
     return 0;
 }

@@ -72,12 +72,16 @@ def test_residual_smooth_transfer_bit_exact(name):
         assert np.array_equal(g.get(abi.A_SOL, l - 1, 4 * sizes[l - 1]), o.get(abi.A_SOL, l - 1, 4 * sizes[l - 1])), ("prolong", l)
 
 
-@pytest.mark.parametrize("tail", ["12000", "2000", "0"])
+@pytest.mark.parametrize("tail", ["12000", "2000", "0", "coop"])
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_vcycles_bit_exact(name, tail, monkeypatch):
     """V-cycles equal the oracle's bit for bit, with the small levels in the one-block tail
-    kernel (default) and with one kernel per phase on every level (I3G_TAIL_NODES=0)."""
-    monkeypatch.setenv("I3G_TAIL_NODES", tail)
+    kernel (default), with one kernel per phase on every level (I3G_TAIL_NODES=0), and with
+    every coarse level in the cooperative grid-wide kernel (I3G_COOP_NODES)."""
+    if tail == "coop":
+        monkeypatch.setenv("I3G_COOP_NODES", "1000000")
+    else:
+        monkeypatch.setenv("I3G_TAIL_NODES", tail)
     p, mode, fx, g, o = pair(name)
     g.call("i3g_stokes_setup")
     o.call("orc_stokes_setup")
