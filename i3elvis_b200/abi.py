@@ -52,6 +52,40 @@ class Model(C.Structure):
     ]
 
 
+class Body(C.Structure):
+    """``i3g_body``: a rock body of init.t3c (in3mg.c:548-797), coordinates relative to the box."""
+    _fields_ = [("rock", C.c_int32), ("shape", C.c_int32), ("x", C.c_double * 8), ("y", C.c_double * 8),
+                ("z", C.c_double * 8), ("ex", C.c_double), ("e", C.c_double)]
+
+
+class Init(C.Structure):
+    """``i3g_init``: initial markers of in3mg.c:131-797 (jitter, background rock, bodies, T)."""
+    _fields_ = [("nonstab", C.c_int32), ("xnonstab", C.c_double), ("ynonstab", C.c_double),
+                ("znonstab", C.c_double), ("seed", C.c_uint64), ("background", C.c_int32),
+                ("t_top", C.c_double), ("t_bottom", C.c_double), ("nbodies", C.c_int32),
+                ("bodies", C.POINTER(Body))]
+
+
+def box_body(rock, lo, hi, ex=0.0, e=0.0):
+    """An axis-aligned box body from relative corners lo = (x, y, z), hi (shape 0)."""
+    b = Body(rock=rock, shape=0, ex=ex, e=e)
+    for n in range(8):
+        b.x[n] = hi[0] if n & 2 else lo[0]
+        b.y[n] = hi[1] if n & 1 else lo[1]
+        b.z[n] = hi[2] if n & 4 else lo[2]
+    return b
+
+
+def sphere_body(rock, centre, scale, r0=0.0, r1=1.0, cylinder=False, ex=0.0, e=0.0):
+    """Ellipsoid shell (or cylinder along y) body: centre and axis scales relative to the box,
+    scaled radius between r0 and r1 (shapes 1 and 2)."""
+    b = Body(rock=rock, shape=2 if cylinder else 1, ex=ex, e=e)
+    b.x[0], b.y[0], b.z[0] = centre
+    b.x[7], b.y[7], b.z[7] = scale
+    b.x[2], b.x[5] = r0, r1
+    return b
+
+
 class Params(C.Structure):
     _fields_ = [
         ("printmod", C.c_int32), ("movemod", C.c_int32), ("tempmod", C.c_int32), ("markmod", C.c_int32),

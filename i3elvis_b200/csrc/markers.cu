@@ -1180,6 +1180,78 @@ __global__ void k_unsort(Marks A, Marks B, long n)
 }
 
 // ------------------------------------------------------------------------------------
+// initial markers (in3mg.c:131-797)
+// ------------------------------------------------------------------------------------
+// SplitMix64 (Steele, Lea & Flood 2014) of (seed, counter): the jitter's random integers.  The
+// reference draws them from the C library's rand() in marker order (in3mg.c:177-186); a
+// counter-based generator gives every marker its own numbers independently of the others.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long seed, unsigned long long k)
+{
+    unsigned long long z = seed + (k + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// one marker: the position of in3mg.c:147-175 (sub-grid per cell, built by repeated addition
+// of the marker spacing), the jitter of in3mg.c:177-186 with 31-bit random integers, the rock
+// bodies of in3mg.c:548-797 in file order (later bodies win) and a linear temperature in y
+__global__ void k_init_markers(Marks M, long n, Grid Gg, InitDev d)
+{
+    const long mm1 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (mm1 >= n) return;
+    const int mpc = d.mx * d.my * d.mz;
+    const long cell = mm1 / mpc;
+    const int q = (int)(mm1 - cell * mpc);
+    const int m5 = q / (d.mx * d.my), m6 = (q / d.my) % d.mx, m7 = q % d.my;
+    const long ny1 = Gg.ny - 1, nxy1 = (long)(Gg.nx - 1) * ny1;
+    const long m3 = cell / nxy1, m1 = (cell / ny1) % (Gg.nx - 1), m2 = cell % ny1;
+    const double dx = d.st[0] / (double)d.mx, dy = d.st[1] / (double)d.my, dz = d.st[2] / (double)d.mz;
+    double x = (double)m1 * d.st[0] + dx / 2.0, y = (double)m2 * d.st[1] + dy / 2.0, z = (double)m3 * d.st[2] + dz / 2.0;
+    for (int k = 0; k < m6; k++) x += dx;
+    for (int k = 0; k < m7; k++) y += dy;
+    for (int k = 0; k < m5; k++) z += dz;
+    float fx = (float)x, fy = (float)y, fz = (float)z;
+    if (d.nonstab) {
+        const int span = 2 * d.nonstab + 1;
+        const float nf = (float)d.nonstab;
+        const int rx = (int)(splitmix64(d.seed, 3 * (unsigned long long)mm1) >> 33);
+        const int ry = (int)(splitmix64(d.seed, 3 * (unsigned long long)mm1 + 1) >> 33);
+        const int rz = (int)(splitmix64(d.seed, 3 * (unsigned long long)mm1 + 2) >> 33);
+        fx = __fadd_rn(fx, __fmul_rn(__fdiv_rn((float)(rx % span - d.nonstab), nf), d.jit[0]));
+        fy = __fadd_rn(fy, __fmul_rn(__fdiv_rn((float)(ry % span - d.nonstab), nf), d.jit[1]));
+        fz = __fadd_rn(fz, __fmul_rn(__fdiv_rn((float)(rz % span - d.nonstab), nf), d.jit[2]));
+    }
+    int t = d.background;
+    float ex = 0.f, e = 0.f;
+    const double rx = (double)fx / Gg.xsize, ry = (double)fy / Gg.ysize, rz = (double)fz / Gg.zsize;
+    for (int b = 0; b < d.nbodies; b++) {
+        const BodyDev &B = d.bodies[b];
+        bool in;
+        if (B.shape == 0) {
+            const double (*k)[4] = B.k;
+            in = rx >= k[0][0] + k[0][1] * ry + k[0][2] * rz + k[0][3] * ry * rz &&
+                 rx <= k[1][0] + k[1][1] * ry + k[1][2] * rz + k[1][3] * ry * rz &&
+                 ry >= k[2][0] + k[2][1] * rx + k[2][2] * rz + k[2][3] * rx * rz &&
+                 ry <= k[3][0] + k[3][1] * rx + k[3][2] * rz + k[3][3] * rx * rz &&
+                 rz >= k[4][0] + k[4][1] * ry + k[4][2] * rx + k[4][3] * ry * rx &&
+                 rz <= k[5][0] + k[5][1] * ry + k[5][2] * rx + k[5][3] * ry * rx;
+        } else {
+            const double ux = (rx - B.c[0]) / B.s[0], uy = (ry - B.c[1]) / B.s[1], uz = (rz - B.c[2]) / B.s[2];
+            const double r = B.shape == 1 ? sqrt(ux * ux + uy * uy + uz * uz) : sqrt(ux * ux + uz * uz);
+            in = r >= B.r0 && r <= B.r1 && (B.shape == 1 || fabs(uy) <= 1.0);
+        }
+        if (in) { t = B.rock; ex = B.ex; e = B.e; }
+    }
+    M.x[mm1] = fx; M.y[mm1] = fy; M.z[mm1] = fz;
+    M.t[mm1] = (int8_t)t;
+    M.ex[mm1] = ex; M.e[mm1] = e;
+    M.k[mm1] = (float)(d.ttop + (d.tbot - d.ttop) * (double)fy / Gg.ysize);
+    M.w[mm1] = 0.f; M.d[mm1] = 0.f; M.v[mm1] = 0.f; M.ft[mm1] = 0.f; M.rr[mm1] = 0.f; M.rn[mm1] = 0.f;
+    M.id[mm1] = (int)mm1;
+}
+
+// ------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------
 static inline unsigned nb(long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
@@ -1390,6 +1462,17 @@ int markers_upload(i3g_ctx *c, const i3g_model *m, bool async)
         I3G_CUDA(cudaEventRecord(S->up_ev, c->cst));
         S->up_pending = true;
     }
+    S->sorted = false;
+    return 0;
+}
+
+int markers_init(i3g_ctx *c, const InitDev &d)
+{
+    MarkerState *S = ms(c);
+    if (!S || !S->n) return 0;
+    if (int rc = markers_wait(c)) return rc;
+    LAUNCH(k_init_markers, nb(S->n), 256, 0, S->a, S->n, grid_of(c), d);
+    I3G_CUDA(cudaGetLastError());
     S->sorted = false;
     return 0;
 }

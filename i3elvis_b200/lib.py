@@ -53,6 +53,8 @@ def load():
     L.i3g_stokes_setup.argtypes = [P]
     L.i3g_stokes_stresses.argtypes = [P]
     L.i3g_write_vtr.argtypes = [P, C.c_char_p]
+    L.i3g_init_markers.argtypes = [P, C.POINTER(abi.Init)]
+    L.i3g_prepare.argtypes = [P]
     for name in ("i3g_stokes_residual", "i3g_stokes_restrict", "i3g_stokes_prolong", "i3g_stokes_vcycles"):
         getattr(L, name).argtypes = [P, C.c_int]
     L.i3g_stokes_smooth.argtypes = [P, C.c_int, C.c_int]
@@ -146,6 +148,17 @@ class Context:
         a, b = C.c_double(), C.c_double()
         self.call("i3g_stokes_relres", C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def init_markers(self, init: abi.Init, bodies=()):
+        """Replace the markers by in3mg's initial markers (``i3g_init_markers``)."""
+        arr = (abi.Body * max(len(bodies), 1))(*bodies)
+        init.nbodies = len(bodies)
+        init.bodies = C.cast(arr, C.POINTER(abi.Body))
+        self.call("i3g_init_markers", C.byref(init))
+
+    def prepare(self):
+        """Initial-condition passes on the device (``i3g_prepare``, in3mg.c:990-1031)."""
+        self.call("i3g_prepare")
 
     def write_vtr(self, path: str):
         """ParaView rectilinear-grid file of the nodal fields (``i3g_write_vtr``)."""

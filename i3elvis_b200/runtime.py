@@ -35,12 +35,9 @@ def hydrostatic_pressure(buf: abi.ModelBuffers) -> None:
 
 
 def prepare(ctx: lib.Context) -> None:
-    """Node fields from markers, hydrostatic pressure, node fields again (``in3mg.c:990-1031``)."""
-    ctx.markers_to_nodes(0.0)
-    ctx.download(abi.SYNC_NODES)
-    hydrostatic_pressure(ctx.buf)
-    ctx.upload(abi.SYNC_NODES)
-    ctx.markers_to_nodes(0.0)
+    """Node fields from markers, hydrostatic pressure, node fields again (``in3mg.c:990-1031``),
+    on the device (``i3g_prepare``); the host buffers receive the result."""
+    ctx.prepare()
     ctx.download(abi.SYNC_ALL)
 
 

@@ -197,6 +197,36 @@ void i3g_host_free(void *p);
  * from the device arrays. */
 int i3g_write_vtr(i3g_ctx *c, const char *path);
 
+/* ---- initial conditions on the GPU (in3mg.c, the reference's separate generator) ------- */
+/* A rock body of init.t3c (in3mg.c:548-797); coordinates relative to the box size.
+ * shape 0: a box whose six faces are bilinear surfaces through its corners 0..7 (corner bits:
+ *          1 larger y, 2 larger x, 4 larger z);
+ * shape 1: an ellipsoid shell, centre = point 0, axis scales = point 7, scaled radius between
+ *          x[2] and x[5];  shape 2: the same as a cylinder along y, |y - y0| <= scale y. */
+#define I3G_INIT_MAX_BODIES 256
+typedef struct i3g_body {
+    int32_t rock, shape;
+    double x[8], y[8], z[8];
+    double ex, e;                       /* markex and marke of the body's markers          */
+} i3g_body;
+typedef struct i3g_init {
+    int32_t nonstab;                    /* jitter resolution n (0: none), in3mg.c:177-186  */
+    double xnonstab, ynonstab, znonstab;/* jitter amplitude, fraction of the marker spacing */
+    uint64_t seed;                      /* of the counter-based jitter generator            */
+    int32_t background;                 /* rock type of markers outside every body          */
+    double t_top, t_bottom;             /* marker temperature, linear in y between these    */
+    int32_t nbodies;
+    const i3g_body *bodies;             /* applied in order: later bodies win               */
+} i3g_init;
+/* Replace c's markers by in3mg's initial markers: mnumx x mnumy x mnumz per cell on the
+ * placement grid size/(n-1) (in3mg.c:131-175), jittered by (r mod (2n+1) - n)/n x amplitude with
+ * r 31-bit numbers from SplitMix64(seed, 3 * marker + axis) (the reference uses rand()), then
+ * the bodies.  Rock types >= 50 (fluid, immobile) are rejected as I3G_E_UNSUPPORTED. */
+int i3g_init_markers(i3g_ctx *c, const i3g_init *s);
+/* The initial-condition passes of in3mg.c:990-1031 on the device: nodes from markers,
+ * hydrostatic pressure (in3mg.c:1010-1021), nodes from markers again. */
+int i3g_prepare(i3g_ctx *c);
+
 /* ---- kernel-level entry points (parity tests and benchmarks) ------------------------- */
 /* Level arrays addressable by i3g_get_array / i3g_set_array (element type in brackets). */
 enum {
