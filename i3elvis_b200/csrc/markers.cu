@@ -52,6 +52,9 @@ struct MarkerState {
     int *tbc_node = nullptr, *tbc_p = nullptr;
     double *tbc_c = nullptr, *tbc_k = nullptr;
     bool sorted = false;
+    // register caps of the FP64-latency-bound marker kernels (resident CTAs per SM they allow)
+    int move_minb = 2;              // k_move: 2 (128 registers), 3 or 4 (I3G_MOVE_OCC)
+    int heat_minb = 1;              // k_heat_mark_cells: 1 (128 registers) or 2 (I3G_HEAT_OCC)
     unsigned move_blocks = 1;       // persistent grid of k_move: resident CTAs on all SMs
     unsigned key_blocks = 1;        // the same for k_tile_key and k_heat_mark_anti
     cudaEvent_t up_ev = nullptr;    // end of an asynchronous upload on the copy stream
@@ -577,7 +580,8 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
 // Persistent grid-stride launch (a few CTAs per SM): the grid lines are staged in shared memory
 // once per CTA instead of once per 256 markers.  Markers are in (tile, cell) order from the last
 // sort, so a warp's interpolation corners hit the same L1 lines.
-__global__ void __launch_bounds__(256, 2) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
 {
     extern __shared__ double shg[];
     Grid G;
@@ -969,7 +973,8 @@ __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, dou
 // change; stage 2 sums them per node (lane = 2 * node + quantity) without atomics.
 constexpr int kHmStage = 9;   // wi[0..7], dtk1
 
-__global__ void __launch_bounds__(32 * kR2nWarps) k_heat_mark_cells(Marks M, const int *coff, Grid Gg, TkF T, TileGeo TG,
+template <int MINB>
+__global__ void __launch_bounds__(32 * kR2nWarps, MINB) k_heat_mark_cells(Marks M, const int *coff, Grid Gg, TkF T, TileGeo TG,
                                                                     double timestep, double heatdif, double zdeep,
                                                                     double tdeep, double *stage)
 {
@@ -1327,6 +1332,26 @@ static Phys phys_of(i3g_ctx *c)
 }
 
 static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
+
+static void launch_move(i3g_ctx *c, unsigned grid, const Marks &M, long n, const Grid &G, const NodeF &F, const Phys &P,
+                        double dt)
+{
+    switch (ms(c)->move_minb) {
+    case 3: LAUNCH(k_move<3>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    case 4: LAUNCH(k_move<4>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    default: LAUNCH(k_move<2>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    }
+}
+
+static int move_occupancy(i3g_ctx *c, int *per_sm)
+{
+    switch (ms(c)->move_minb) {
+    case 3: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<3>, 256, grid_smem(c))); break;
+    case 4: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<4>, 256, grid_smem(c))); break;
+    default: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<2>, 256, grid_smem(c))); break;
+    }
+    return 0;
+}
 static size_t r2n_smem(i3g_ctx *c) { return sizeof(double) * (NACC * NBOX + kR2nWarps * 32 * kStage) + grid_smem(c) + sizeof(int) * kR2nWarps * 32; }
 static size_t heat_mark_smem(i3g_ctx *c) { return sizeof(double) * (2 * NBOX + kR2nWarps * 32 * kHmStage) + grid_smem(c); }
 
@@ -1388,7 +1413,9 @@ int markers_alloc(i3g_ctx *c)
         int dev = 0, sms = 0, per_sm = 0;
         I3G_CUDA(cudaGetDevice(&dev));
         I3G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move, 256, grid_smem(c)));
+        if (const char *e = getenv("I3G_MOVE_OCC")) S->move_minb = std::min(4, std::max(2, atoi(e)));
+        if (const char *e = getenv("I3G_HEAT_OCC")) S->heat_minb = std::min(2, std::max(1, atoi(e)));
+        if (int rc = move_occupancy(c, &per_sm)) return rc;
         S->move_blocks = (unsigned)std::max(1, sms * std::max(per_sm, 1));
         int a = 0, b = 0;
         I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tile_key, 256, grid_smem(c)));
@@ -1396,7 +1423,8 @@ int markers_alloc(i3g_ctx *c)
         S->key_blocks = (unsigned)std::max(1, sms * std::max(std::min(a, b), 1));
     }
     I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
-    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
     I3G_CUDA(cudaStreamSynchronize(c->st));
     // upload the host markers
     return markers_upload(c, &c->m);
@@ -1518,8 +1546,7 @@ int markers_move(i3g_ctx *c, double timestep)
     cudaEvent_t e0 = ev.a, e1 = ev.b;
     I3G_CUDA(cudaEventRecord(e0, c->st));
     I3G_CUDA(cudaMemsetAsync(S->err, 0, sizeof(int), c->st));
-    LAUNCH(k_move, std::min(nb(S->n), S->move_blocks), 256, grid_smem(c), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c),
-           timestep);
+    launch_move(c, std::min(nb(S->n), S->move_blocks), S->a, S->n, grid_of(c), nodes_of(c), phys_of(c), timestep);
     I3G_CUDA(cudaGetLastError());
     I3G_CUDA(cudaEventRecord(e1, c->st));
     int rc = check_err(c, "movemark");
@@ -1596,7 +1623,9 @@ int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const flo
     }
     TkF T{tk0, tk1, c->tk, tk2, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
     TileGeo TG{S->ntx, S->nty, S->ntz, S->ntiles};
-    LAUNCH(k_heat_mark_cells, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
+    if (S->heat_minb == 2) LAUNCH(k_heat_mark_cells<2>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
+           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
+        else LAUNCH(k_heat_mark_cells<1>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
            T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
     if (c->p.heatdif != 0) {
         LAUNCH(k_heat_mark_gather, nb(N), 256, 0, (const double *)S->stage, TG, (int)c->m.xnumx, (int)c->m.ynumy,
@@ -1625,11 +1654,12 @@ int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *
             LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff,
                    grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->stage);
         else if (kind == 9)
-            LAUNCH(k_heat_mark_cells, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
+            if (S->heat_minb == 2) LAUNCH(k_heat_mark_cells<2>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
+                   TK, T, 1e10, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
+        else LAUNCH(k_heat_mark_cells<1>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
                    TK, T, 1e10, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
         else
-            LAUNCH(k_move, std::min(nb(n), S->move_blocks), 256, grid_smem(c), S->a, n, grid_of(c), nodes_of(c), phys_of(c),
-                   0.0);
+            launch_move(c, std::min(nb(n), S->move_blocks), S->a, n, grid_of(c), nodes_of(c), phys_of(c), 0.0);
         return 0;
     };
     launch();   // warm-up
