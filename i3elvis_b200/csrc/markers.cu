@@ -54,7 +54,9 @@ struct MarkerState {
     bool sorted = false;
     // register caps of the FP64-latency-bound marker kernels (resident CTAs per SM they allow)
     int move_minb = 2;              // k_move: 2 (128 registers), 3 or 4 (I3G_MOVE_OCC)
-    int heat_minb = 1;              // k_heat_mark_cells: 1 (128 registers) or 2 (I3G_HEAT_OCC)
+    // k_heat_mark_cells: 2 CTAs per SM (64 registers; 4.5 ms instead of 6.6 ms at 129^3 with 56.6 M
+    // markers on B200, its FP64 dependency chains need the extra warps), 1 with I3G_HEAT_OCC=1
+    int heat_minb = 2;
     unsigned move_blocks = 1;       // persistent grid of k_move: resident CTAs on all SMs
     unsigned key_blocks = 1;        // the same for k_tile_key and k_heat_mark_anti
     cudaEvent_t up_ev = nullptr;    // end of an asynchronous upload on the copy stream
@@ -508,9 +510,11 @@ __device__ __forceinline__ void load_grid(const Grid &Gg, double *sh, Grid &G)
     G.gx = sh; G.gy = sh + Gg.nx; G.gz = sh + Gg.nx + Gg.ny;
 }
 
+// second invariant (mark3mg.c:73-74 computes it as pow(., 0.5)): the correctly rounded square
+// root of the same sum, which a pow of exponent 0.5 approximates to within its own error bound
 __device__ __forceinline__ double inv2(const double *e)
 {
-    return pow(0.5 * (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]) + e[3] * e[3] + e[4] * e[4] + e[5] * e[5], 0.5);
+    return sqrt(0.5 * (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]) + e[3] * e[3] + e[4] * e[4] + e[5] * e[5]);
 }
 
 // ------------------------------------------------------------------------------------
