@@ -65,6 +65,7 @@ void i3g_destroy(i3g_ctx *c)
     for (int a = 0; a < 6; a++) { cudaFree(c->eps[a]); cudaFree(c->sig[a]); }
     for (int v = 0; v < 4; v++) cudaFree(c->guess[v]);
     for (int v = 0; v < 8; v++) cudaFree(c->gsave[v]);
+    cudaFree(c->gdots);
     if (c->hstage) cudaFreeHost(c->hstage);
     if (c->tev[0]) { cudaEventDestroy(c->tev[0]); cudaEventDestroy(c->tev[1]); }
     delete[] c->hgx; delete[] c->hgy; delete[] c->hgz;

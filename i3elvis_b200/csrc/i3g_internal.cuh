@@ -179,11 +179,12 @@ struct i3g_ctx {
     // staged start for the next Stokes solve (i3g_unet_predict); kept only when its relative
     // residual is below the default start's
     double *guess[4] = {};
-    double *gsave[8] = {};                      // default start (0..3) and the state one iteration later (4..7)
+    double *gsave[8] = {};                      // default start (0..3) and its residual (4..7)
+    double *gdots = nullptr;                    // 2 device doubles: weighted <r0,dr>, <dr,dr>
     int guess_pending = 0;
     int guess_used = -1;                        // last solve: -1 none staged, 0 rejected, 1 used
-    double guess_rel[2] = {0, 0};               // relative residual one iteration after the staged / default start
-    double guess_alpha = 0;                     // 1 when the staged start was kept, else 0
+    double guess_rel[2] = {0, 0};               // relative residual of the staged / default start
+    double guess_alpha = 0;                     // factor applied to the staged correction
     void *kry = nullptr;       // FGMRES state of the mixed-precision Stokes solve
     void *heat = nullptr;      // heat-solver state
     void *mk = nullptr;        // marker state

@@ -54,9 +54,6 @@ struct MarkerState {
     bool sorted = false;
     // register caps of the FP64-latency-bound marker kernels (resident CTAs per SM they allow)
     int move_minb = 2;              // k_move: 2 (128 registers), 3 or 4 (I3G_MOVE_OCC)
-    int move_split = 0;             // 1: the step as k_move_rheology + k_move_advect (I3G_MOVE_SPLIT)
-    double *v1s = nullptr;          // their first RK velocity per marker (3 n doubles)
-    unsigned rheo_blocks = 1, adv_blocks = 1;
     // k_heat_mark_cells: 2 CTAs per SM (64 registers; 4.5 ms instead of 6.6 ms at 129^3 with 56.6 M
     // markers on B200, its FP64 dependency chains need the extra warps), 1 with I3G_HEAT_OCC=1
     int heat_minb = 2;
@@ -582,111 +579,6 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
     }
     M.x[i] = nx_; M.y[i] = ny_; M.z[i] = nz_;
     M.k[i] = mk; M.v[i] = mv; M.e[i] = me; M.ft[i] = mft; M.w[i] = mw; M.t[i] = (int8_t)t;
-}
-
-// The same step in two launches that each keep fewer values live (so more warps hide the FP64
-// latency): the rheology half ends after the strain update and stores the first RK velocity,
-// the advection half reads it back.  Every operation and its order is move_one's; markers that
-// move_one leaves untouched are flagged with a NaN first velocity and left untouched again.
-__device__ __forceinline__ void move_rheology(const Marks &M, long i, const Grid &G, const NodeF &F, const Phys &P,
-                                              double timestep, double *v1s, long n)
-{
-    const int t = M.t[i];
-    const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
-    const bool inbox = fx >= 0 && fy >= 0 && fz >= 0 && (double)fx <= G.xsize && (double)fy <= G.ysize && (double)fz <= G.zsize;
-    if (!(inbox || (P.outgrid != 1 && (t < 50 || t >= 100)))) { v1s[i] = nan(""); return; }
-    if (t >= 50) { atomicOr(P.err, ERR_TYPE); v1s[i] = nan(""); return; }
-    double v1[3], e[7], s[6], dis;
-    int wn[3];
-    VStencil S0;
-    vxyz(G, F, fx, fy, fz, v1, wn, &S0);
-    eps_from(G, F, fx, fy, fz, wn, S0, e, s, &dis);
-    const double eii = inv2(e), sii = inv2(s);
-    const double mpb = e[6] * 1e-5;
-    float mv = M.v[i], me = M.e[i], mft = M.ft[i];
-    const double mtk = M.k[i];
-    if (t < 50 && mtk > 0) {
-        double rii = 1.0;
-        if (mv > 0 && fx > G.gx[3] && fx < G.gx[G.nx - 4] && fy > G.gy[3] && fy < G.gy[G.ny - 4] && fz > G.gz[3] && fz < G.gz[G.nz - 4])
-            rii *= pow(0.5 * sii / eii / mv, 0.87);
-        const double mnu = visc(P, mtk, mpb, t, eii, rii, me, mft);
-        if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); v1s[i] = nan(""); return; }
-        mv = (float)mnu;
-        if (me > 0) me += timestep * eii;
-        if (me > 0) { me -= timestep * P.healrate; if (me < 0) me = 0; }
-        else { me += timestep * P.healrate; if (me > 0) me = 0; }
-    }
-    M.v[i] = mv; M.e[i] = me; M.ft[i] = mft;
-    v1s[i] = v1[0]; v1s[n + i] = v1[1]; v1s[2 * n + i] = v1[2];
-}
-
-__device__ __forceinline__ void move_advect(const Marks &M, long i, const Grid &G, const NodeF &F, const Phys &P,
-                                            double timestep, const double *v1s, long n)
-{
-    const double v10 = v1s[i];
-    if (isnan(v10)) return;
-    const double v1[3] = {v10, v1s[n + i], v1s[2 * n + i]};
-    int t = M.t[i];
-    const float fx = M.x[i], fy = M.y[i], fz = M.z[i];
-    const double yold = fy;
-    float mk = M.k[i], mw = M.w[i];
-    int wn[3];
-    double v[3];
-    if (P.markmod == 1) { v[0] = v1[0]; v[1] = v1[1]; v[2] = v1[2]; }
-    else {
-        // (v1 + 2 v2 + 2 v3 + v4) / 6 summed left to right as the stages arrive, so only one
-        // stage velocity and the partial sum are live at a time
-        double w[3];
-        vxyz(G, F, fx + v1[0] * timestep / 2.0, fy + v1[1] * timestep / 2.0, fz + v1[2] * timestep / 2.0, w, wn);
-        for (int k = 0; k < 3; k++) v[k] = v1[k] + 2.0 * w[k];
-        vxyz(G, F, fx + w[0] * timestep / 2.0, fy + w[1] * timestep / 2.0, fz + w[2] * timestep / 2.0, w, wn);
-        for (int k = 0; k < 3; k++) v[k] = v[k] + 2.0 * w[k];
-        vxyz(G, F, fx + w[0] * timestep, fy + w[1] * timestep, fz + w[2] * timestep, w, wn);
-        for (int k = 0; k < 3; k++) v[k] = (v[k] + w[k]) / 6.0;
-    }
-    if (P.outgrid == 2) {
-        if (fx < 0 || (double)fx > G.xsize) v[1] = v[2] = 0;
-        if (fy < 0 || (double)fy > G.ysize) v[0] = v[2] = 0;
-        if (fz < 0 || (double)fz > G.zsize) v[0] = v[1] = 0;
-    }
-    if (fy > P.zdeep && v[1] < 0 && mk < P.tdeep && t == 10) mk = (float)P.tdeep;
-    if (fy > P.zdeep && v[1] < 0 && t != 10) { t = 10; mw = 0; }
-    if (fy > P.zdeep && t != 10 && t != 9) { t = 9; mw = 0; }
-    const float nx_ = (float)(fx + (timestep * v[0] - 0.0));
-    const float ny_ = (float)(fy + timestep * v[1]);
-    const float nz_ = (float)(fz + timestep * v[2]);
-    if ((yold > P.vdeep && ny_ < P.vdeep) || (yold > P.zdeep && ny_ < P.zdeep)) {
-        if (mk < P.tdeep) mk = (float)P.tdeep;
-        t = 10;
-    }
-    if (nx_ < 0 || ny_ < 0 || nz_ < 0 || (double)nx_ > G.xsize || (double)ny_ > G.ysize || (double)nz_ > G.zsize) {
-        mk = 0;
-        M.v[i] = 0;
-    }
-    M.x[i] = nx_; M.y[i] = ny_; M.z[i] = nz_;
-    M.k[i] = mk; M.w[i] = mw; M.t[i] = (int8_t)t;
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_move_rheology(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep,
-                                                             double *v1s)
-{
-    extern __shared__ double shg[];
-    Grid G;
-    load_grid(Gg, shg, G);
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        move_rheology(M, i, G, F, P, timestep, v1s, n);
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_move_advect(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep,
-                                                           const double *v1s)
-{
-    extern __shared__ double shg[];
-    Grid G;
-    load_grid(Gg, shg, G);
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        move_advect(M, i, G, F, P, timestep, v1s, n);
 }
 
 // Persistent grid-stride launch (a few CTAs per SM): the grid lines are staged in shared memory
@@ -1445,20 +1337,10 @@ static Phys phys_of(i3g_ctx *c)
 
 static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
 
-
 static void launch_move(i3g_ctx *c, unsigned grid, const Marks &M, long n, const Grid &G, const NodeF &F, const Phys &P,
                         double dt)
 {
-    MarkerState *S = ms(c);
-    if (S->move_split) {
-        LAUNCH(k_move_rheology<2>, std::min(grid, S->rheo_blocks), 256, grid_smem(c), M, n, G, F, P, dt, S->v1s);
-        if (S->move_split == 3)
-            LAUNCH(k_move_advect<3>, std::min(nb(n), S->adv_blocks), 256, grid_smem(c), M, n, G, F, P, dt, (const double *)S->v1s);
-        else
-            LAUNCH(k_move_advect<2>, std::min(nb(n), S->adv_blocks), 256, grid_smem(c), M, n, G, F, P, dt, (const double *)S->v1s);
-        return;
-    }
-    switch (S->move_minb) {
+    switch (ms(c)->move_minb) {
     case 3: LAUNCH(k_move<3>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
     case 4: LAUNCH(k_move<4>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
     default: LAUNCH(k_move<2>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
@@ -1538,19 +1420,6 @@ int markers_alloc(i3g_ctx *c)
         if (const char *e = getenv("I3G_MOVE_OCC")) S->move_minb = std::min(4, std::max(2, atoi(e)));
         if (const char *e = getenv("I3G_HEAT_OCC")) S->heat_minb = std::min(2, std::max(1, atoi(e)));
         if (int rc = move_occupancy(c, &per_sm)) return rc;
-        // I3G_MOVE_SPLIT = 2 or 3: the two-launch step, advection half at that many CTAs per SM
-        if (const char *e = getenv("I3G_MOVE_SPLIT")) S->move_split = atoi(e) == 3 ? 3 : atoi(e) ? 2 : 0;
-        if (S->move_split) {
-            int r = 0, a = 0;
-            I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_move_rheology<2>, 256, grid_smem(c)));
-            if (S->move_split == 3)
-                I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_move_advect<3>, 256, grid_smem(c)));
-            else
-                I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_move_advect<2>, 256, grid_smem(c)));
-            S->rheo_blocks = (unsigned)std::max(1, sms * std::max(r, 1));
-            S->adv_blocks = (unsigned)std::max(1, sms * std::max(a, 1));
-            I3G_CUDA(cudaMalloc((void **)&S->v1s, sizeof(double) * 3 * (n > 0 ? n : 1)));
-        }
         S->move_blocks = (unsigned)std::max(1, sms * std::max(per_sm, 1));
         int a = 0, b = 0;
         I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tile_key, 256, grid_smem(c)));
@@ -1572,7 +1441,7 @@ void markers_free(i3g_ctx *c)
     if (c->cst) cudaStreamSynchronize(c->cst);   // no upload may still target the buffers freed here
     free_marks(S->a);
     free_marks(S->b);
-    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->coff); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->bsum); cudaFree(S->acc); cudaFree(S->stage); cudaFree(S->tk1); cudaFree(S->v1s);
+    cudaFree(S->key); cudaFree(S->cnt); cudaFree(S->coff); cudaFree(S->off); cudaFree(S->cur); cudaFree(S->bsum); cudaFree(S->acc); cudaFree(S->stage); cudaFree(S->tk1);
     cudaFree(S->rock); cudaFree(S->err);
     if (S->herr) cudaFreeHost(S->herr);
     if (S->up_ev) cudaEventDestroy(S->up_ev);

@@ -1935,6 +1935,37 @@ __global__ void k_extrapolate(long n, double *u, const double *a, const double *
     u[t] = a[t] + r * (a[t] - b[t]);
 }
 
+// Row-weighted dots of a staged start's residual change dr = r0 - r (r0: the default start's
+// residual, r = L.r: the staged start's) over the rows of the stopping test: out[0] += <r0, dr>,
+// out[1] += <dr, dr>, weight wm on non-boundary velocity rows and wc on pressure rows.
+__global__ void __launch_bounds__(256) k_guess_dots(View<double> L, const double *a0, const double *a1, const double *a2,
+                                                    const double *a3, double wm, double wc, double *out)
+{
+    pdl_enter();
+    __shared__ double sh[2][8];
+    double x = 0, y = 0;
+    const long N = L.nxy * L.nz;
+    for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
+        const int j = (int)(n % L.ny);
+        const long rest = n / L.ny;
+        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        const uint8_t b = L.bc[n];
+        if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) { const double d = a0[n] - L.r0[n]; x += wc * a0[n] * d; y += wc * d * d; }
+        if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(b & 2)) { const double d = a1[n] - L.r1[n]; x += wm * a1[n] * d; y += wm * d * d; }
+        if (row_exists(2, i, j, k, L.nx, L.ny, L.nz) && !(b & 4)) { const double d = a2[n] - L.r2[n]; x += wm * a2[n] * d; y += wm * d * d; }
+        if (row_exists(3, i, j, k, L.nx, L.ny, L.nz) && !(b & 8)) { const double d = a3[n] - L.r3[n]; x += wm * a3[n] * d; y += wm * d * d; }
+    }
+    x = warp_sum(x);
+    y = warp_sum(y);
+    const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (ln == 0) { sh[0][w] = x; sh[1][w] = y; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); q++) { x += sh[0][q]; y += sh[1][q]; }
+        atomicAdd(out, x);
+        atomicAdd(out + 1, y);
+    }
+}
 
 static int kry_alloc(i3g_ctx *c, int m)
 {
@@ -2174,52 +2205,57 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     double mom, cont;
     if ((rc = stokes_relres(c, &mom, &cont))) return rc;
     c->guess_used = -1;
-    int trial_cycles = 0;
-    const double rel_start = std::max(mom, cont);
     if (c->guess_pending) {
-        // A staged (learned) start g competes with the default start d.  Their raw residuals say
-        // little: a start whose error is mostly smooth -- what the network gets right -- can have
-        // a larger residual than d and still be much closer to the solution.  So each start gets
-        // one solver iteration (one V-cycle; with precision 1 inside the FP64 defect correction),
-        // which removes the high-frequency part of its error, and the solve continues from the
-        // one with the lower relative residual after it.  Both iterations count as cycles.
+        // A staged (learned) start g competes with the default start d.  The correction g - d is
+        // first scaled by the factor that minimises the stopping test's row-weighted residual
+        // along it: r(d + a (g - d)) = r0 - a dr with dr = r0 - r(g), a = <r0,dr> / <dr,dr>.
+        // The scaled start is kept only if its relative residual is below the default start's.
         c->guess_pending = 0;
-        double *const *sd = c->gsave, *const *sd1 = c->gsave + 4;
-        for (int v = 0; v < 4; v++) I3G_CUDA(cudaMemcpyAsync(sd[v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
-        if ((rc = iteration_graph(c, multinum))) return rc;
-        I3G_CUDA(cudaGraphLaunch(c->sgraph, c->st));
-        c->launches += c->sg_nodes;
-        I3G_CUDA(cudaStreamSynchronize(c->st));
-        double dm, dc;
-        relres_read(c, &dm, &dc);
+        const double q1 = c->hred[1], q3 = c->hred[3];   // sum b_mom^2 and sum v^2 of the default start
+        double *const *su = c->gsave, *const *sr = c->gsave + 4;
+        residual_t<double>(c, 0);
         for (int v = 0; v < 4; v++) {
-            I3G_CUDA(cudaMemcpyAsync(sd1[v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+            I3G_CUDA(cudaMemcpyAsync(sr[v], L0.d.r[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+            I3G_CUDA(cudaMemcpyAsync(su[v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
             I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], c->guess[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
         }
         for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
-        I3G_CUDA(cudaGraphLaunch(c->sgraph, c->st));
-        c->launches += c->sg_nodes;
+        residual_t<double>(c, 0);
+        const double wm = q1 > 0 ? 1.0 / q1 : 1.0;
+        const double wc = (c->ncont > 0 && q3 > 0) ? c->h_ref * c->h_ref * c->nvel / (c->ncont * q3) : 1.0;
+        I3G_CUDA(cudaMemsetAsync(c->gdots, 0, 2 * sizeof(double), c->st));
+        LAUNCH(k_guess_dots, c->red_blocks, 256, view<double>(L0, L0.d), (const double *)sr[0], (const double *)sr[1],
+               (const double *)sr[2], (const double *)sr[3], wm, wc, c->gdots);
+        double dots[2] = {0, 0};
+        I3G_CUDA(cudaMemcpyAsync(dots, c->gdots, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
         I3G_CUDA(cudaStreamSynchronize(c->st));
+        double alpha = dots[1] > 0 ? dots[0] / dots[1] : 0.0;
+        if (!(alpha > 0)) alpha = 0.0;   // also for NaN
+        alpha = std::min(alpha, 4.0);
+        c->guess_alpha = alpha;
+        // u = d + alpha (g - d)
+        for (int v = 0; v < 4; v++)
+            LAUNCH(k_extrapolate, nblk(L0.n), 256, L0.n, L0.d.u[v], (const double *)su[v], (const double *)c->guess[v], -alpha);
+        for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
         double gm, gc;
-        relres_read(c, &gm, &gc);
-        trial_cycles = 2;
-        const double rg = std::max(gm, gc), rdef = std::max(dm, dc);
+        if ((rc = stokes_relres(c, &gm, &gc))) return rc;
+        const double rg = std::max(gm, gc), rdef = std::max(mom, cont);
         c->guess_rel[0] = rg;
         c->guess_rel[1] = rdef;
-        c->guess_used = rg < rdef ? 1 : 0;   // false for a NaN residual too
-        c->guess_alpha = c->guess_used ? 1.0 : 0.0;
+        c->guess_used = (alpha > 0 && rg < rdef) ? 1 : 0;   // false for a NaN residual too
         if (c->guess_used) {
             mom = gm;
             cont = gc;
         } else {
+            // back to the default start; the norms are recomputed so that everything derived from
+            // them (the FGMRES row scaling) is the default start's again
             for (int v = 0; v < 4; v++)
-                I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], sd1[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
-            // norms of the kept state: everything derived from them (the FGMRES row scaling) is its own
+                I3G_CUDA(cudaMemcpyAsync(L0.d.u[v], su[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
             if ((rc = stokes_relres(c, &mom, &cont))) return rc;
         }
     }
-    c->st_.stokes_rel0 = rel_start;
-    int cycles = trial_cycles, outer = 0;
+    c->st_.stokes_rel0 = std::max(mom, cont);
+    int cycles = 0, outer = 0;
     bool conv = mom <= rtol && cont <= rtol;
     const double p0_save = c->p.p0koef, p1_save = c->p.p1koef;
     const int ncyc = c->p.multicyc > 0 ? c->p.multicyc : 1;

@@ -1246,11 +1246,13 @@ int i3g_unet_predict(i3g_unet *u, i3g_ctx *c)
     const long n = u->L[0].n;
     if (!c->guess[0]) {
         // all or nothing: a partial set would be taken as complete by the next call
-        bool ok = true;
+        bool ok = cudaMalloc((void **)&c->gdots, 2 * sizeof(double)) == cudaSuccess;
         for (int v = 0; v < 4 && ok; v++) ok = cudaMalloc((void **)&c->guess[v], n * sizeof(double)) == cudaSuccess;
         for (int v = 0; v < 8 && ok; v++) ok = cudaMalloc((void **)&c->gsave[v], n * sizeof(double)) == cudaSuccess;
         if (!ok) {
             cudaGetLastError();
+            cudaFree(c->gdots);
+            c->gdots = nullptr;
             for (int v = 0; v < 4; v++) { cudaFree(c->guess[v]); c->guess[v] = nullptr; }
             for (int v = 0; v < 8; v++) { cudaFree(c->gsave[v]); c->gsave[v] = nullptr; }
             return set_global_error(I3G_E_NOMEM, "U-Net: guess buffers");

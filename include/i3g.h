@@ -277,9 +277,8 @@ int i3g_timer(i3g_ctx *c, int op, double *ms);
 /* The reference starts every Stokes solve from the previous step's v, P
  * (move3mg.c:1969-2019).  The network maps log10 viscosity, density and that previous
  * velocity on the level-0 node grid to a correction (dP, dVx, dVy, dVz) of that start; the
- * solver runs one iteration from each start, continues from the one with the lower relative
- * residual after it and iterates to the same tolerance, so the network changes the cycle count,
- * never the converged answer.
+ * solver keeps the corrected start only when its relative residual is lower and then iterates
+ * to the same tolerance, so the network changes the cycle count, never the converged answer.
  * 4 levels of 16/32/64/128 channels, 15 convolutions of 3x3x3 on tcgen05 tensor cores (BF16
  * operands, FP32 accumulation), Adam on FP32 master weights.  Every grid axis needs n >= 9
  * and n-1 divisible by 8.  Host arrays of nodal data are planar in the solver's node order
@@ -308,9 +307,9 @@ int i3g_unet_loss(i3g_unet *u, const int *slots, int nslots, double *loss);
 /* Host data in and out: out4 = correction for in5; with tg4, *loss and (grads != NULL) the
  * parameter gradients of that one sample's loss. */
 int i3g_unet_eval_host(i3g_unet *u, const float *in5, const float *tg4, float *out4, float *grads, double *loss);
-/* Stage previous v, P + correction as the start of c's next i3g_stokes, which runs one
- * iteration from it and one from the default start and continues from the better of the two
- * (see i3g_stokes_guess_info). */
+/* Stage previous v, P + correction as the start of c's next i3g_stokes, which scales the
+ * correction by the residual-minimising factor and keeps the result only when its relative
+ * residual is lower than the default start's (see i3g_stokes_guess_info). */
 int i3g_unet_predict(i3g_unet *u, i3g_ctx *c);
 /* Mean device time of one training step on sample slot 0 and of one forward pass. */
 int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward);
@@ -322,10 +321,9 @@ int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *byt
  * [rows][cout], interior rows only.  cin, cout in {16, 32, 64, 128} as the network pairs them. */
 int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *in, const uint16_t *w,
                        const float *bias, const uint16_t *add, int relu, float *out);
-/* Last i3g_stokes: used = -1 no staged start, 0 rejected, 1 used; relative residuals one
- * iteration after the staged start and after the default start (the raw residual of a start
- * weighs its high-frequency error, which the first iteration removes); alpha = 1 when the
- * staged start was kept, 0 otherwise.  Both trial iterations count in stokes_cycles. */
+/* Last i3g_stokes: used = -1 no staged start, 0 rejected, 1 used; relative residuals of the
+ * staged start (after scaling its correction by alpha) and of the default start; alpha is the
+ * factor a >= 0 minimising the row-weighted residual of default + a (staged - default). */
 int i3g_stokes_guess_info(const i3g_ctx *c, int *used, double *rel_guess, double *rel_default, double *alpha);
 
 /* ---- allocation-free stopping test (no counterpart in the reference) --------------- */

@@ -1,7 +1,7 @@
 """Learned warm start on the GPU, through the C ABI (i3g_unet_*), against the CPU oracle
 oracle/unet_ref.py: the tcgen05 convolution, the network's output and its parameter
-gradients; then a small training run that must lower the loss, after which a held-out Stokes
-solve continues from the better of its two trial iterates and needs at most two more cycles."""
+gradients; then a small training run that must lower the loss and must never make a
+held-out Stokes solve start from a worse residual than the default start."""
 import numpy as np
 import pytest
 
@@ -98,10 +98,11 @@ def test_network_output_and_gradients_match_oracle():
 
 def test_training_lowers_loss_and_never_worsens_the_start():
     """A short training run on library solves of seeded 17^3 inclusion models lowers the loss;
-    on held-out models the solve continues from the better of the two starts after one
-    iteration each, so it never continues from a worse state than the default start's, and it
-    still meets the tolerance in about as many V-cycles.  The gain itself is printed (and
-    measured at larger sizes by ``python -m i3elvis_b200.learned``)."""
+    on held-out models the learned start (its correction scaled by the residual-minimising
+    factor, kept only when its residual is lower) never starts the solve from a higher
+    residual than the default start, and the solve still meets the tolerance in about as
+    many V-cycles.  The gain itself is printed (and measured at larger sizes by
+    ``python -m i3elvis_b200.learned``)."""
     from i3elvis_b200 import learned
     from i3elvis_b200.warmstart import UNet
     case = learned.Case(n=17, mnum=2, count=8, r_km=(15.0, 35.0))
@@ -116,9 +117,12 @@ def test_training_lowers_loss_and_never_worsens_the_start():
     print("learned warm start, 17^3 held-out models:", learned.summarize(rows))
     for r in rows:
         assert r["guess_used"] in (0, 1), r
-        # the solve continues from the better of the two states one iteration after each start
-        assert (r["guess_used"] == 1) == (r["rel_guess"] < r["rel_default"]), r
-        assert r["alpha"] == float(r["guess_used"]), r
+        # the solve starts from the better of the two starts of its own state
+        assert r["learned_rel0"] <= r["rel_default"] * (1 + 1e-9), r
+        # ... and never from a worse one than the separate default-start context on the same
+        # state (one step per seed: both contexts hold identical models)
+        assert r["learned_rel0"] <= r["default_rel0"] * (1 + 1e-9), r
+        assert r["alpha"] >= 0.0, r
     print("guess accepted on", sum(r["guess_used"] == 1 for r in rows), "of", len(rows), "held-out solves")
     d = float(np.mean([r["default_cycles"] for r in rows]))
     g = float(np.mean([r["learned_cycles"] for r in rows]))
