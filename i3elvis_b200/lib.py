@@ -105,9 +105,14 @@ class Context:
         self.call("i3g_set_params", C.byref(p))
 
     # the four time-step calls of the host loop (i3mg.c:98-137)
-    def stokes(self, n0: int, timestep: float) -> float:
+    def stokes(self, n0: int, timestep: float, allow_noconv: bool = False) -> float:
+        """``i3g_stokes``; with ``allow_noconv`` an iteration cap reached before the tolerance is
+        not an error (the solution reached, its stresses and the CFL step are kept, as the
+        library writes them before returning I3G_E_NOCONV)."""
         t = C.c_double(timestep)
-        self.call("i3g_stokes", n0, C.byref(t))
+        rc = load().i3g_stokes(self.h, n0, C.byref(t))
+        if not (allow_noconv and rc == -5):
+            self._check(rc)
         return t.value
 
     def heat(self, n0: int, timestep: float) -> float:

@@ -41,13 +41,14 @@ def prepare(ctx: lib.Context) -> None:
     ctx.download(abi.SYNC_ALL)
 
 
-def time_step(ctx: lib.Context, mode: config.Mode, f: config.OutFile, n0: int) -> dict:
-    """One reference time step (``i3mg.c:80-147``); returns the step size and phase times."""
+def time_step(ctx: lib.Context, mode: config.Mode, f: config.OutFile, n0: int, allow_noconv: bool = False) -> dict:
+    """One reference time step (``i3mg.c:80-147``); returns the step size and phase times.
+    ``allow_noconv``: a Stokes solve that stops at its cycle cap does not end the step."""
     timestep = f.maxtmstep_yr * YEAR
     t = {}
     if mode.movemod:
         t0 = time.perf_counter()
-        timestep = ctx.stokes(n0, timestep)
+        timestep = ctx.stokes(n0, timestep, allow_noconv)
         t["stokes_s"] = time.perf_counter() - t0
     if mode.tempmod and timestep:
         t0 = time.perf_counter()
