@@ -170,6 +170,7 @@ struct i3g_ctx {
     void *flush = nullptr;                      // 256 MiB written between cold-cache timings (L2 is 126 MB)
     long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
     long coop_nodes = 0;                        // > 0: levels up to this size run in the cooperative coarse kernel
+    int tail_cluster = 1;                       // CTAs of the V-cycle tail (> 1: one thread-block cluster)
     int coop_blocks = 0;                        // its grid: every CTA resident at once (0: no cooperative launch)
     unsigned *dbar = nullptr;                   // its grid barrier: arrival count, generation
     int *dbar_err = nullptr;                    // set when a grid barrier wait timed out

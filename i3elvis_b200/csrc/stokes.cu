@@ -507,6 +507,28 @@ struct BlockTeam {
     __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
+// The CTAs of one thread-block cluster (up to 16, on distinct SMs of one GPC) and the hardware
+// cluster barrier, whose release/acquire orders the global-memory writes of one phase before the
+// reads of the next across the cluster.
+struct ClusterTeam {
+    __device__ __forceinline__ long rank() const
+    {
+        unsigned r;
+        asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+        return (long)r * blockDim.x + threadIdx.x;
+    }
+    __device__ __forceinline__ long size() const
+    {
+        unsigned n;
+        asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+        return (long)n * blockDim.x;
+    }
+    __device__ __forceinline__ void sync() const
+    {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+};
+
 // Grid-wide barrier of a cooperative launch (all CTAs resident by construction).  The last CTA
 // to arrive resets the counter and advances the generation; the others wait for the generation,
 // each for at most 2 s (then the launch's error flag is set and the wait gives up, so a broken
@@ -656,6 +678,15 @@ __global__ void __launch_bounds__(kCoopThreads) k_vcycle_coop(const __grid_const
 {
     pdl_enter();
     tail_body<T>(a, tm);
+}
+
+// The same schedule on one cluster of CTAs: the small coarse levels run on several SMs with a
+// hardware barrier between phases instead of on one SM (the one-block tail) or the whole grid.
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_cluster(const __grid_constant__ TailArgs<T> a)
+{
+    pdl_enter();
+    tail_body<T>(a, ClusterTeam());
 }
 
 // ronurestrict (move3mg.c:2642-2741): FP32 accumulator as in nu[], FP64 weights
@@ -1123,6 +1154,12 @@ int stokes_alloc(i3g_ctx *c)
     // cooperative coarse-level kernel: levels up to this size (I3G_COOP_NODES, 0 = off) run in
     // one launch over the whole grid; its size is what every SM can hold at once
     if (const char *e = getenv("I3G_COOP_NODES")) c->coop_nodes = atol(e);
+    // CTAs of the tail (I3G_TAIL_CLUSTER, 1: the one-block kernel; 2..16: one thread-block cluster)
+    if (const char *e = getenv("I3G_TAIL_CLUSTER")) c->tail_cluster = std::max(1, std::min(16, atoi(e)));
+    if (c->tail_cluster > 8) {
+        I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
     {
         int dev = 0, sms = 0, coop = 0, a = 0, b = 0;
         I3G_CUDA(cudaGetDevice(&dev));
@@ -1429,6 +1466,25 @@ static void tail_launch(i3g_ctx *c, int lc, int multinum)
         cfg.attrs = at;
         cfg.numAttrs = 1;
         cudaLaunchKernelEx(&cfg, k_vcycle_coop<T>, a, GridTeam{c->dbar, c->dbar + 1, c->dbar_err});
+        c->launches++;
+        return;
+    }
+    if (c->tail_cluster > 1) {
+        // one cluster of tail_cluster CTAs (non-portable sizes above 8 are enabled at set-up)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)c->tail_cluster);
+        cfg.blockDim = dim3(kTailThreads);
+        cfg.stream = c->st;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)c->tail_cluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl_enabled() ? 2 : 1;
+        cudaLaunchKernelEx(&cfg, k_vcycle_cluster<T>, a);
         c->launches++;
         return;
     }
