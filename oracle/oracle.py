@@ -147,7 +147,7 @@ def run_reference(workdir, *args, threads=1, timeout=3600):
         i = line.find("{\"")
         if i >= 0:
             try:
-                return json.loads(line[i:])
+                return json.loads(_c_numbers(line[i:]))
             except json.JSONDecodeError:
                 continue
     return None
@@ -169,10 +169,17 @@ def run_reference_lines(workdir, *args, threads=1, timeout=3600):
         i = line.find("{\"")
         if i >= 0:
             try:
-                out.append(json.loads(line[i:]))
+                out.append(json.loads(_c_numbers(line[i:])))
             except json.JSONDecodeError:
                 continue
     return out
+
+
+def _c_numbers(line):
+    """printf's nan / inf tokens as the JSON parser's NaN / Infinity."""
+    import re
+    line = re.sub(r"(?<![A-Za-z])-?nan(?![A-Za-z])", "NaN", line)
+    return re.sub(r"(?<![A-Za-z])(-?)inf(?![A-Za-z])", r"\1Infinity", line)
 
 
 def read_csr(path):
