@@ -124,7 +124,7 @@ class Stats(C.Structure):
         ("stokes_mom_rel", C.c_double), ("stokes_cont_rel", C.c_double),
         ("heat_cycles", C.c_int32), ("heat_substeps", C.c_int32), ("heat_rel", C.c_double),
         ("ms_stokes", C.c_double), ("ms_heat", C.c_double), ("ms_move", C.c_double), ("ms_r2n", C.c_double),
-        ("kernel_launches", C.c_int64),
+        ("kernel_launches", C.c_int64), ("stokes_start", C.c_int32),
     ]
 
     def as_dict(self):

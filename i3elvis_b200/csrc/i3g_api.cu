@@ -248,13 +248,15 @@ int i3g_upload(i3g_ctx *c, const i3g_model *m, unsigned mask)
     if (!c || !m) return I3G_E_ARG;
     const long N = c->nodenum;
     if (mask & I3G_SYNC_NODES) {
-        c->nhist = 0;   // new state: no extrapolation across it
         H2D(c->pr, m->pr, N, 8);
         H2D(c->vx, m->vx, N, 4); H2D(c->vy, m->vy, N, 4); H2D(c->vz, m->vz, N, 4);
         H2D(c->ro, m->ro, N, 4); H2D(c->lev[0].nu, m->nu, N, 4);
         H2D(c->nxx, m->nxx, N, 4); H2D(c->nxy, m->nxy, N, 4); H2D(c->nxz, m->nxz, N, 4); H2D(c->nyz, m->nyz, N, 4);
         H2D(c->tk, m->tk, N, 4); H2D(c->cp, m->cp, N, 4); H2D(c->et, m->et, N, 4);
         H2D(c->kt, m->kt, N, 4); H2D(c->ht, m->ht, N, 4); H2D(c->rr, m->rr, N, 4);
+        // the extrapolation history survives only an upload of the library's own last solution
+        int rc = i3g::stokes_upload_check(c);
+        if (rc) return rc;
     }
     if (mask & I3G_SYNC_STRESS) {
         const float *he[6] = {m->exx, m->eyy, m->ezz, m->exy, m->exz, m->eyz};

@@ -65,6 +65,14 @@ struct BcList {
     int *onode = nullptr;       // original partner node (unflattened), -1: none
     int *ocomp = nullptr;       // original partner component
     double *oc = nullptr, *ok = nullptr;   // original constant and factor (level 0 residual)
+    // Rows written inside the relaxation kernel that finalises the component in a sweep
+    // (na >= 0): entries [0, na) are sorted by their writer, a row of that kernel, and written by
+    // the writer's thread right after its own update (bit 4 + v of the level's bc byte marks
+    // writers, first[node] is a writer's first entry); entries [na, n) run on extra blocks of
+    // that kernel.  na = -1: a separate boundary pass after the kernel.
+    int na = -1;
+    int *first = nullptr;
+    int *writer = nullptr;
 };
 
 template <typename T>
@@ -100,7 +108,8 @@ struct Level {
     long n = 0;
     double *gx = nullptr, *gy = nullptr, *gz = nullptr;   // level coordinates (host)
     float *nu = nullptr;               // nodal viscosity of this level
-    uint8_t *bc = nullptr;             // bit v: row v (0 P, 1 Vx, 2 Vy, 3 Vz) is a boundary row
+    uint8_t *bc = nullptr;             // bit v: row v (0 P, 1 Vx, 2 Vy, 3 Vz) is a boundary row;
+                                       // bit 4 + v: partner of in-kernel boundary rows of v (BcList::na)
     Fields<double> d;
     Fields<float> s;                    // scaled FP32 copy for the mixed-precision solver
     BcList bcl[4];
@@ -171,10 +180,15 @@ struct i3g_ctx {
     long tail_nodes = 2000;                     // levels up to this size run in the one-block V-cycle tail
     long coop_nodes = 0;                        // > 0: levels up to this size run in the cooperative coarse kernel
     int tail_cluster = 1;                       // CTAs of the V-cycle tail (> 1: one thread-block cluster)
+    int fuse = 1;                               // boundary rows inside the relaxation kernels of levels >= 1
+                                                // (3: level 0 too), residual and four-component transfer
+                                                // launches (0: one launch per pass)
     int coop_blocks = 0;                        // its grid: every CTA resident at once (0: no cooperative launch)
     unsigned *dbar = nullptr;                   // its grid barrier: arrival count, generation
     int *dbar_err = nullptr;                    // set when a grid barrier wait timed out
     double *hist[2][4] = {};                    // last two converged level-0 solutions (warm_start 2)
+    int hist_check = 0;                         // an upload is being compared with the last solution
+    int *dflag = nullptr, *hflag = nullptr;     // its result: device flag and pinned host mirror
     double hist_dt[2] = {0, 0};                 // time steps taken after them
     int nhist = 0;
     // staged start for the next Stokes solve (i3g_unet_predict); kept only when its relative
@@ -242,6 +256,7 @@ void stokes_free(i3g_ctx *c);
 void stokes_graph_free(i3g_ctx *c);
 void stokes_params_changed(i3g_ctx *c);
 int stokes_setup(i3g_ctx *c);
+int stokes_upload_check(i3g_ctx *c);
 int stokes_residual(i3g_ctx *c, int level);
 int stokes_smooth(i3g_ctx *c, int level, int nsweeps);
 int stokes_restrict(i3g_ctx *c, int level);

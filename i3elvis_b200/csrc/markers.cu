@@ -166,9 +166,11 @@ __device__ __forceinline__ Ax ax_cent(const double *g, int n, int m, double x)
 
 __device__ __forceinline__ Ax clamped(Ax a) { return Ax{a.i, clamp01(a.w0), clamp01(a.w1)}; }
 
-// sum over the 8 corners of f * ((ddx * ddy) * ddz) in the reference's loop order z, x, y
-__device__ __forceinline__ double tri(const float *__restrict__ f, long NY, long NXY, const Ax &X, const Ax &Y, const Ax &Z)
+// sum over the 8 corners of f * ((ddx * ddy) * ddz) in the reference's loop order z, x, y; node
+// offsets in 32 bits (a level-0 grid has fewer than 2^31 nodes)
+__device__ __forceinline__ double tri(const float *__restrict__ f, int NY, int NXY, const Ax &X, const Ax &Y, const Ax &Z)
 {
+    const float *p = f + (Z.i * NXY + X.i * NY + Y.i);
     double s = 0;
 #pragma unroll
     for (int k3 = 0; k3 < 2; k3++) {
@@ -176,11 +178,11 @@ __device__ __forceinline__ double tri(const float *__restrict__ f, long NY, long
 #pragma unroll
         for (int k1 = 0; k1 < 2; k1++) {
             const double ddx = k1 ? X.w1 : X.w0;
-            const long base = (long)(Z.i + k3) * NXY + (long)(X.i + k1) * NY + Y.i;
+            const int base = k3 * NXY + k1 * NY;
 #pragma unroll
             for (int k2 = 0; k2 < 2; k2++) {
                 const double ddy = k2 ? Y.w1 : Y.w0;
-                s += (double)__ldg(f + base + k2) * (ddx * ddy * ddz);
+                s += (double)__ldg(p + base + k2) * (ddx * ddy * ddz);
             }
         }
     }
@@ -210,16 +212,18 @@ __device__ __forceinline__ void vxyz(const Grid &G, const NodeF &F, double x, do
     S.mx = ax_mid(gx, X, m1, x);
     S.my = ax_mid(gy, Y, m2, y);
     S.mz = ax_mid(gz, Z, m3, z);
-    v[0] = tri(F.vx, F.NY, F.NXY, S.lx, S.my, S.mz);
-    v[1] = tri(F.vy, F.NY, F.NXY, S.mx, S.ly, S.mz);
-    v[2] = tri(F.vz, F.NY, F.NXY, S.mx, S.my, S.lz);
+    const int NY = (int)F.NY, NXY = (int)F.NXY;
+    v[0] = tri(F.vx, NY, NXY, S.lx, S.my, S.mz);
+    v[1] = tri(F.vy, NY, NXY, S.mx, S.ly, S.mz);
+    v[2] = tri(F.vz, NY, NXY, S.mx, S.my, S.lz);
     if (out) *out = S;
 }
 
 // one shear group of epscalc1: strain rate, stress and the dissipation term 2 s e w
-__device__ __forceinline__ void edge_group(const float *__restrict__ fe, const float *__restrict__ fs, long NY, long NXY,
+__device__ __forceinline__ void edge_group(const float *__restrict__ fe, const float *__restrict__ fs, int NY, int NXY,
                                            const Ax &AX, const Ax &AY, const Ax &AZ, double &e, double &s, double &d)
 {
+    const int n0 = AZ.i * NXY + AX.i * NY + AY.i;
 #pragma unroll
     for (int k3 = 0; k3 < 2; k3++) {
         const double ddz = k3 ? AZ.w1 : AZ.w0;
@@ -229,7 +233,7 @@ __device__ __forceinline__ void edge_group(const float *__restrict__ fe, const f
 #pragma unroll
             for (int k2 = 0; k2 < 2; k2++) {
                 const double ddy = k2 ? AY.w1 : AY.w0;
-                const long n = (long)(AZ.i + k3) * NXY + (long)(AX.i + k1) * NY + (AY.i + k2);
+                const int n = n0 + k3 * NXY + k1 * NY + k2;
                 const double w = ddx * ddy * ddz;
                 const float ev = __ldg(fe + n), sv = __ldg(fs + n);
                 e += ev * w;
@@ -251,12 +255,13 @@ __device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x
     if (x < 0) x = 0; if (x > G.xsize) x = G.xsize;
     if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
-    const long NY = F.NY, NXY = F.NXY;
+    const int NY = (int)F.NY, NXY = (int)F.NXY;
     for (int i = 0; i < 7; i++) e[i] = 0;
     for (int i = 0; i < 6; i++) s[i] = 0;
     double d = 0;
     {
         const Ax cx = ax_cent(gx, X, wn[0], x), cy = ax_cent(gy, Y, wn[1], y), cz = ax_cent(gz, Z, wn[2], z);
+        const int n0 = cz.i * NXY + cx.i * NY + cy.i;
 #pragma unroll
         for (int k3 = 0; k3 < 2; k3++) {
             const double ddz = k3 ? cz.w1 : cz.w0;
@@ -266,7 +271,7 @@ __device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x
 #pragma unroll
                 for (int k2 = 0; k2 < 2; k2++) {
                     const double ddy = k2 ? cy.w1 : cy.w0;
-                    const long n = (long)(cz.i + k3) * NXY + (long)(cx.i + k1) * NY + (cy.i + k2);
+                    const int n = n0 + k3 * NXY + k1 * NY + k2;
                     const double w = ddx * ddy * ddz;
                     const float exx = __ldg(F.e[0] + n), eyy = __ldg(F.e[1] + n), ezz = __ldg(F.e[2] + n);
                     const float sxx = __ldg(F.s[0] + n), syy = __ldg(F.s[1] + n), szz = __ldg(F.s[2] + n);
@@ -391,17 +396,18 @@ __device__ double pr_at(const Grid &G, const double *pr, long NY, long NXY, doub
     if (y > (gy[b] + gy[b + 1]) / 2.0) b += 1; if (b < 1) b = 1; if (b > Y - 2) b = Y - 2;
     if (z > (gz[c] + gz[c + 1]) / 2.0) c += 1; if (c < 1) c = 1; if (c > Z - 2) c = Z - 2;
     const double dx = (gx[a + 1] - gx[a - 1]) / 2.0, dy = (gy[b + 1] - gy[b - 1]) / 2.0, dz = (gz[c + 1] - gz[c - 1]) / 2.0;
-    double p = 0, ddx, ddy, ddz;
-    for (int k3 = c; k3 <= c + 1; k3++) {
-        ddz = ((gz[k3 - 1] + gz[k3]) / 2.0 - z) / dz; if (k3 == c) ddz = -ddz; ddz = 1.0 - ddz;
-        for (int k1 = a; k1 <= a + 1; k1++) {
-            ddx = ((gx[k1 - 1] + gx[k1]) / 2.0 - x) / dx; if (k1 == a) ddx = -ddx; ddx = 1.0 - ddx;
-            for (int k2 = b; k2 <= b + 1; k2++) {
-                ddy = ((gy[k2 - 1] + gy[k2]) / 2.0 - y) / dy; if (k2 == b) ddy = -ddy; ddy = 1.0 - ddy;
-                p += pr[k3 * NXY + (long)k1 * NY + k2] * (ddx * ddy * ddz);
-            }
-        }
-    }
+    // prcalc1's per-corner weights, computed once per axis (1 - (-q) = 1 + q exactly)
+    const double wx[2] = {1.0 + ((gx[a - 1] + gx[a]) / 2.0 - x) / dx, 1.0 - ((gx[a] + gx[a + 1]) / 2.0 - x) / dx};
+    const double wy[2] = {1.0 + ((gy[b - 1] + gy[b]) / 2.0 - y) / dy, 1.0 - ((gy[b] + gy[b + 1]) / 2.0 - y) / dy};
+    const double wz[2] = {1.0 + ((gz[c - 1] + gz[c]) / 2.0 - z) / dz, 1.0 - ((gz[c] + gz[c + 1]) / 2.0 - z) / dz};
+    const double *p0 = pr + ((int)(c * NXY) + a * (int)NY + b);
+    double p = 0;
+#pragma unroll
+    for (int k3 = 0; k3 < 2; k3++)
+#pragma unroll
+        for (int k1 = 0; k1 < 2; k1++)
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) p += p0[k3 * (int)NXY + k1 * (int)NY + k2] * (wx[k1] * wy[k2] * wz[k3]);
     return p;
 }
 

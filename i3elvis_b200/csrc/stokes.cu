@@ -40,11 +40,29 @@ struct Ar<float> {
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
 };
 
+// floor(n / d) for 0 <= n < 2^31 by one multiply-high and a shift (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, Theorem 4.2 with N = 31):
+// l = ceil(log2 d), m = ceil(2^(31+l) / d) < 2^32, q = umulhi(n, m) >> (l - 1); d = 1: m = 0.
+struct FastDiv {
+    unsigned m = 0, s = 0;
+    static FastDiv of(unsigned d)
+    {
+        FastDiv f;
+        if (d <= 1) return f;
+        const unsigned l = 32u - (unsigned)__builtin_clz(d - 1u);
+        f.m = (unsigned)((((unsigned long long)1 << (31 + l)) + d - 1) / d);
+        f.s = l - 1;
+        return f;
+    }
+    __device__ __forceinline__ unsigned div(unsigned n) const { return m ? __umulhi(n, m) >> s : n; }
+};
+
 // Level view passed by value to kernels.
 template <typename T>
 struct View {
     int nx, ny, nz;
     long nxy;
+    FastDiv dnx, dny, dhy;          // division by nx, ny and (ny + 1) / 2 for index decomposition
     const uint8_t *bc;
     T *u0, *u1, *u2, *u3;
     T *f0, *f1, *f2, *f3;
@@ -54,11 +72,24 @@ struct View {
     const float *nd;
 };
 
+// (i, j, k) of node n = (k * nx + i) * ny + j of a level (n < 2^31)
+template <typename T>
+__device__ __forceinline__ void node_ijk(const View<T> &L, long n, int &i, int &j, int &k)
+{
+    const unsigned u = (unsigned)n;
+    const unsigned r = L.dny.div(u);
+    j = (int)(u - r * (unsigned)L.ny);
+    const unsigned q = L.dnx.div(r);
+    i = (int)(r - q * (unsigned)L.nx);
+    k = (int)q;
+}
+
 template <typename T>
 static View<T> view(Level &L, Fields<T> &F)
 {
     View<T> v;
     v.nx = L.nx; v.ny = L.ny; v.nz = L.nz; v.nxy = (long)L.nx * L.ny;
+    v.dnx = FastDiv::of((unsigned)L.nx); v.dny = FastDiv::of((unsigned)L.ny); v.dhy = FastDiv::of((unsigned)((L.ny + 1) / 2));
     v.bc = L.bc;
     v.u0 = F.u[0]; v.u1 = F.u[1]; v.u2 = F.u[2]; v.u3 = F.u[3];
     v.f0 = F.f[0]; v.f1 = F.f[1]; v.f2 = F.f[2]; v.f3 = F.f[3];
@@ -229,22 +260,40 @@ __device__ __forceinline__ void crow(const View<T> &L, int i, int j, int k, long
 // ------------------------------------------------------------------------------------
 // One colour of one velocity component: thread t handles the row of colour `color` in the
 // y-pair (2*jh, 2*jh+1) of line (i,k), so a warp covers 64 consecutive y.
+// Node of thread t's row of colour `color` (the y-pair (2*jh, 2*jh+1) of line (i,k)); -1 when
+// the row does not exist.
+template <int V, typename T>
+__device__ __forceinline__ long vel_row_node(const View<T> &L, long t, int color, int &i, int &j, int &k)
+{
+    const unsigned hy = (unsigned)((L.ny + 1) >> 1), u = (unsigned)t;
+    const unsigned rest = L.dhy.div(u);
+    const int jh = (int)(u - rest * hy);
+    const unsigned q = L.dnx.div(rest);
+    i = (int)(rest - q * (unsigned)L.nx); k = (int)q;
+    j = 2 * jh + ((i + k + color) & 1);
+    if (j >= L.ny || !row_exists(V, i, j, k, L.nx, L.ny, L.nz)) return -1;
+    return (long)k * L.nxy + (long)i * L.ny + j;
+}
+
+// the relaxation update of velocity row n; returns the new value
+template <typename T, int V>
+__device__ __forceinline__ T relax_vel_row(const View<T> &L, int i, int j, int k, long n, T koef)
+{
+    using A = Ar<T>;
+    T s, d, u;
+    if (V == 1) { s = -L.f1[n]; d = xrow<T, false>(L, i, j, k, n, s); u = L.u1[n] = A::sub(L.u1[n], A::mul(A::div(s, d), koef)); }
+    if (V == 2) { s = -L.f2[n]; d = yrow<T, false>(L, i, j, k, n, s); u = L.u2[n] = A::sub(L.u2[n], A::mul(A::div(s, d), koef)); }
+    if (V == 3) { s = -L.f3[n]; d = zrow<T, false>(L, i, j, k, n, s); u = L.u3[n] = A::sub(L.u3[n], A::mul(A::div(s, d), koef)); }
+    return u;
+}
+
 template <typename T, int V>
 __device__ __forceinline__ void relax_vel_at(const View<T> &L, long t, int color, T koef)
 {
-    using A = Ar<T>;
-    const int hy = (L.ny + 1) >> 1;
-    const int jh = (int)(t % hy);
-    const long rest = t / hy;
-    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
-    const int j = 2 * jh + ((i + k + color) & 1);
-    if (j >= L.ny || !row_exists(V, i, j, k, L.nx, L.ny, L.nz)) return;
-    const long n = (long)k * L.nxy + (long)i * L.ny + j;
-    if (L.bc[n] & (1 << V)) return;
-    T s, d;
-    if (V == 1) { s = -L.f1[n]; d = xrow<T, false>(L, i, j, k, n, s); L.u1[n] = A::sub(L.u1[n], A::mul(A::div(s, d), koef)); }
-    if (V == 2) { s = -L.f2[n]; d = yrow<T, false>(L, i, j, k, n, s); L.u2[n] = A::sub(L.u2[n], A::mul(A::div(s, d), koef)); }
-    if (V == 3) { s = -L.f3[n]; d = zrow<T, false>(L, i, j, k, n, s); L.u3[n] = A::sub(L.u3[n], A::mul(A::div(s, d), koef)); }
+    int i, j, k;
+    const long n = vel_row_node<V>(L, t, color, i, j, k);
+    if (n < 0 || (L.bc[n] & (1 << V))) return;
+    relax_vel_row<T, V>(L, i, j, k, n, koef);
 }
 
 template <typename T, int V>
@@ -257,17 +306,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_relax_vel(View<
 }
 
 // All interior pressure rows: p -= (div v - f) * nd * p0koef (move3mg.c:3105-3116)
+// Relaxes pressure row n if it exists; *b receives its bc byte, *u the new value.
 template <typename T>
-__device__ __forceinline__ void relax_p_at(const View<T> &L, long n, T koef)
+__device__ __forceinline__ bool relax_p_at(const View<T> &L, long n, T koef, uint8_t *b = nullptr, T *u = nullptr)
 {
     using A = Ar<T>;
-    const int j = (int)(n % L.ny);
-    const long rest = n / L.ny;
-    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
-    if (!(i > 0 && j > 0 && k > 0) || (L.bc[n] & 1)) return;
+    int i, j, k;
+    node_ijk(L, n, i, j, k);
+    const uint8_t bb = L.bc[n];
+    if (!(i > 0 && j > 0 && k > 0) || (bb & 1)) return false;
     T s = -L.f0[n];
     crow<T, false>(L, i, j, k, n, s);
-    L.u0[n] = A::sub(L.u0[n], A::mul(A::mul(s, (T)L.nd[n]), koef));
+    const T un = L.u0[n] = A::sub(L.u0[n], A::mul(A::mul(s, (T)L.nd[n]), koef));
+    if (b) *b = bb;
+    if (u) *u = un;
+    return true;
 }
 
 template <typename T>
@@ -305,15 +358,93 @@ __global__ void k_bc_apply(T *u, int n, const int *node, const int *pnode, const
     bc_apply_at<T>(u, t, node, pnode, depth, cc, kk, use_c);
 }
 
+// Device view of a component's boundary rows (BcList).
+struct BcDev {
+    int n, na;
+    const int *node, *pnode, *depth, *onode, *ocomp, *first, *writer;
+    const double *c, *k, *ok;
+};
+
+// In-kernel boundary rows (BcList::na >= 0).  A sweep's separate boundary pass writes each
+// boundary node from its interior partner after the kernel that finalises the component.  Here
+// the same values are written inside that kernel, by one of its rows' threads right after that
+// row's update (entries [0, na), sorted by writer) or by extra blocks (entries [na, n)).  The
+// writer is the partner when the kernel updates the partner; otherwise the one row of the
+// kernel that reads the boundary node, if there is one.  Set-up admits a component only if
+// every boundary node is read by no row of the kernel other than its writer, whose read comes
+// before its write, so all rows see the values the separate pass would leave and the results
+// are bit-identical.
+//
+// The writer's entries are fetched through the read-only path before its own update (e0 =
+// first entry), so their loads overlap the row's; a partner that is the writer itself takes the
+// value just computed (un), any other partner is final in this kernel.
+template <typename T>
+__device__ __forceinline__ void bc_writer_rows(T *u, const BcDev &B, int e0, long n, T un, int use_c)
+{
+    using A = Ar<T>;
+    for (int e = e0; e < B.na && __ldg(B.writer + e) == (int)n; e++) {
+        const int p = __ldg(B.pnode + e);
+        T val = p < 0 ? T(0) : p == (int)n ? un : __ldg(u + p);
+        for (int d = __ldg(B.depth + e) - 1; d >= 0; d--) {
+            const T c0 = use_c ? (T)__ldg(B.c + e * kMaxBcDepth + d) : T(0);
+            val = A::add(c0, A::mul((T)__ldg(B.k + e * kMaxBcDepth + d), val));
+        }
+        u[__ldg(B.node + e)] = val;
+    }
+}
+
+// Colour 1 of velocity component V with the component's boundary rows; blocks from rowblocks on
+// write entries [na, n).
+template <typename T, int V>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_relax_vel_bc(View<T> L, T koef, BcDev B, int use_c,
+                                                                               unsigned rowblocks)
+{
+    pdl_enter();
+    T *u = V == 1 ? L.u1 : V == 2 ? L.u2 : L.u3;
+    if (blockIdx.x >= rowblocks) {
+        const int e = B.na + (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
+        if (e < B.n) bc_apply_at<T>(u, e, B.node, B.pnode, B.depth, B.c, B.k, use_c);
+        return;
+    }
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)((L.ny + 1) >> 1) * L.nx * L.nz) return;
+    int i, j, k;
+    const long n = vel_row_node<V>(L, t, 1, i, j, k);
+    if (n < 0) return;
+    const uint8_t b = L.bc[n];
+    if (b & (1 << V)) return;
+    const int e0 = (b & (16 << V)) ? __ldg(B.first + n) : B.na;
+    const T un = relax_vel_row<T, V>(L, i, j, k, n, koef);
+    if (e0 < B.na) bc_writer_rows<T>(u, B, e0, n, un, use_c);
+}
+
+// All pressure rows with the pressure boundary rows (no pressure row reads another pressure).
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_relax_p_bc(View<T> L, T koef, BcDev B, int use_c,
+                                                                             unsigned rowblocks)
+{
+    pdl_enter();
+    if (blockIdx.x >= rowblocks) {
+        const int e = B.na + (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
+        if (e < B.n) bc_apply_at<T>(L.u0, e, B.node, B.pnode, B.depth, B.c, B.k, use_c);
+        return;
+    }
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.nxy * L.nz) return;
+    const int e0 = (L.bc[n] & 16) ? __ldg(B.first + n) : B.na;
+    uint8_t b = 0;
+    T un = 0;
+    if (relax_p_at<T>(L, n, koef, &b, &un) && e0 < B.na) bc_writer_rows<T>(L.u0, B, e0, n, un, use_c);
+}
+
 // ------------------------------------------------------------------------------------
 // residual (gausmat4 residual pass, move3mg.c:3136-3157)
 // ------------------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void residual_at(const View<T> &L, long n)
 {
-    const int j = (int)(n % L.ny);
-    const long rest = n / L.ny;
-    const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+    int i, j, k;
+    node_ijk(L, n, i, j, k);
     const uint8_t b = L.bc[n];
     if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) { T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); L.r0[n] = s; }
     if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(b & 2)) { T s = L.f1[n]; xrow<T, true>(L, i, j, k, n, s); L.r1[n] = s; }
@@ -356,6 +487,32 @@ __global__ void k_bc_residual(View<T> L, int V, int n, const int *node, const in
     bc_residual_at<T>(L, V, t, node, onode, ocomp, ok);
 }
 
+// Residual of all rows; blocks from rowblocks on take the boundary rows of the four components
+// (they write only boundary nodes, which the row threads skip, and read no residual).
+struct BcDev4 {
+    BcDev b[4];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_residual_bc(View<T> L, BcDev4 B, unsigned rowblocks)
+{
+    pdl_enter();
+    if (blockIdx.x >= rowblocks) {
+        int t = (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
+        for (int v = 0; v < 4; v++) {
+            if (t < B.b[v].n) {
+                bc_residual_at<T>(L, v, t, B.b[v].node, B.b[v].onode, B.b[v].ocomp, B.b[v].ok);
+                return;
+            }
+            t -= B.b[v].n;
+        }
+        return;
+    }
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.nxy * L.nz) return;
+    residual_at<T>(L, n);
+}
+
 // ------------------------------------------------------------------------------------
 // grid transfers in gather form
 // ------------------------------------------------------------------------------------
@@ -380,9 +537,8 @@ __device__ __forceinline__ void restrict_at(const View<T> &F, const View<T> &Cc,
                                             const TrView &tz, long n)
 {
     using A = Ar<T>;
-    const int j = (int)(n % Cc.ny);
-    const long rest = n / Cc.ny;
-    const int i = (int)(rest % Cc.nx), k = (int)(rest / Cc.nx);
+    int i, j, k;
+    node_ijk(Cc, n, i, j, k);
     T *cu = V == 0 ? Cc.u0 : V == 1 ? Cc.u1 : V == 2 ? Cc.u2 : Cc.u3;
     T *cf_ = V == 0 ? Cc.f0 : V == 1 ? Cc.f1 : V == 2 ? Cc.f2 : Cc.f3;
     const T *fr = V == 0 ? F.r0 : V == 1 ? F.r1 : V == 2 ? F.r2 : F.r3;
@@ -428,9 +584,8 @@ __device__ __forceinline__ void prolong_at(const View<T> &F, const View<T> &Cc, 
                                            const TrView &tz, T koef, long n)
 {
     using A = Ar<T>;
-    const int j = (int)(n % F.ny);
-    const long rest = n / F.ny;
-    const int i = (int)(rest % F.nx), k = (int)(rest / F.nx);
+    int i, j, k;
+    node_ijk(F, n, i, j, k);
     if (!row_exists(V, i, j, k, F.nx, F.ny, F.nz)) return;
     T *fu = V == 0 ? F.u0 : V == 1 ? F.u1 : V == 2 ? F.u2 : F.u3;
     const T *cu = V == 0 ? Cc.u0 : V == 1 ? Cc.u1 : V == 2 ? Cc.u2 : Cc.u3;
@@ -458,6 +613,40 @@ __global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView t
     prolong_at<T, V>(F, Cc, tx, ty, tz, koef, n);
 }
 
+// The four components' transfers in one launch (blockIdx.y = component); the components read
+// and write disjoint arrays.
+struct Tr4 {
+    TrView t[4][3];      // [component][axis]
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict4(View<T> F, View<T> Cc, Tr4 R)
+{
+    pdl_enter();
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Cc.nxy * Cc.nz) return;
+    switch (blockIdx.y) {
+    case 0: restrict_at<T, 0>(F, Cc, R.t[0][0], R.t[0][1], R.t[0][2], n); break;
+    case 1: restrict_at<T, 1>(F, Cc, R.t[1][0], R.t[1][1], R.t[1][2], n); break;
+    case 2: restrict_at<T, 2>(F, Cc, R.t[2][0], R.t[2][1], R.t[2][2], n); break;
+    default: restrict_at<T, 3>(F, Cc, R.t[3][0], R.t[3][1], R.t[3][2], n); break;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong4(View<T> F, View<T> Cc, Tr4 R, T kv, T kp)
+{
+    pdl_enter();
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= F.nxy * F.nz) return;
+    switch (blockIdx.y) {
+    case 0: prolong_at<T, 0>(F, Cc, R.t[0][0], R.t[0][1], R.t[0][2], kp, n); break;
+    case 1: prolong_at<T, 1>(F, Cc, R.t[1][0], R.t[1][1], R.t[1][2], kv, n); break;
+    case 2: prolong_at<T, 2>(F, Cc, R.t[2][0], R.t[2][1], R.t[2][2], kv, n); break;
+    default: prolong_at<T, 3>(F, Cc, R.t[3][0], R.t[3][1], R.t[3][2], kv, n); break;
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // coarse tail of a V-cycle in one thread block
 // ------------------------------------------------------------------------------------
@@ -471,12 +660,6 @@ __global__ void __launch_bounds__(256) k_prolong(View<T> F, View<T> Cc, TrView t
 // The small levels stay resident in L1/L2.
 constexpr int kTailMax = 6;
 constexpr int kTailThreads = 512;
-
-struct BcDev {
-    int n;
-    const int *node, *pnode, *depth, *onode, *ocomp;
-    const double *c, *k, *ok;
-};
 
 template <typename T>
 struct TailLevel {
@@ -891,9 +1074,8 @@ __global__ void __launch_bounds__(kRedThreads) k_relres_part(View<T> L, double *
     double q[kRedQ] = {0, 0, 0, 0};
     const long N = L.nxy * L.nz;
     for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
-        const int j = (int)(n % L.ny);
-        const long rest = n / L.ny;
-        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        int i, j, k;
+        node_ijk(L, n, i, j, k);
         const uint8_t b = L.bc[n];
         if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) {
             T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); q[2] += (double)s * (double)s;
@@ -1132,11 +1314,88 @@ static int build_bc(i3g_ctx *c)
                 }
             }
         }
+        // In-kernel boundary rows (k_relax_vel_bc, k_relax_p_bc).  The finalising kernel of a
+        // velocity component updates its colour-1 rows (i + j + k odd), which read only their even
+        // neighbours; the pressure kernel updates every pressure row and reads no pressure.  Per
+        // boundary row b with partner p, R = the kernel's rows that read b:
+        //   p updated by the kernel: writer p, admitted if R is within {p};
+        //   otherwise (p final or constant): no reader -> extra blocks; one reader r -> writer r;
+        // two or more readers: the component keeps the separate pass.
+        int na[4] = {-1, -1, -1, -1};
+        std::vector<int> first[4], writer[4];
+        auto is_row = [&](long q, int v) {
+            const int j = (int)(q % L.ny), i = (int)((q / L.ny) % L.nx), k = (int)(q / ((long)L.ny * L.nx));
+            return row_exists(v, i, j, k, L.nx, L.ny, L.nz) && !(mask[q] & (1 << v));
+        };
+        auto odd = [&](long q) {
+            const int j = (int)(q % L.ny), i = (int)((q / L.ny) % L.nx), k = (int)(q / ((long)L.ny * L.nx));
+            return ((i + j + k) & 1) != 0;
+        };
+        for (int v = 0; c->fuse && v < 4; v++) {
+            const int nb = (int)node[v].size();
+            std::vector<int> A, Bo, wr(nb, -1);
+            bool admit = true;
+            for (int e = 0; e < nb && admit; e++) {
+                const int p = pnode[v][e];
+                int R[6], nr = 0;
+                if (v > 0) {
+                    const long q = node[v][e];
+                    const int j = (int)(q % L.ny), i = (int)((q / L.ny) % L.nx), k = (int)(q / ((long)L.ny * L.nx));
+                    const int di[6] = {-1, 1, 0, 0, 0, 0}, dj[6] = {0, 0, -1, 1, 0, 0}, dk[6] = {0, 0, 0, 0, -1, 1};
+                    for (int d = 0; d < 6; d++) {
+                        const int i2 = i + di[d], j2 = j + dj[d], k2 = k + dk[d];
+                        if (i2 < 0 || j2 < 0 || k2 < 0 || i2 >= L.nx || j2 >= L.ny || k2 >= L.nz) continue;
+                        const long r = ((long)k2 * L.nx + i2) * L.ny + j2;
+                        if (is_row(r, v) && odd(r)) R[nr++] = (int)r;
+                    }
+                }
+                if (p >= 0 && is_row(p, v) && (v == 0 || odd(p))) {
+                    for (int q = 0; q < nr; q++)
+                        if (R[q] != p) admit = false;
+                    wr[e] = p;
+                    A.push_back(e);
+                } else if (nr == 0) {
+                    Bo.push_back(e);
+                } else if (nr == 1) {
+                    wr[e] = R[0];
+                    A.push_back(e);
+                } else {
+                    admit = false;
+                }
+            }
+            if (!admit) continue;
+            std::stable_sort(A.begin(), A.end(), [&](int x, int y) { return wr[x] < wr[y]; });
+            std::vector<int> perm(A);
+            perm.insert(perm.end(), Bo.begin(), Bo.end());
+            auto permute = [&](auto &vec, int width) {
+                auto old = vec;
+                for (size_t e = 0; e < perm.size(); e++)
+                    for (int w = 0; w < width; w++) vec[e * width + w] = old[(size_t)perm[e] * width + w];
+            };
+            permute(node[v], 1); permute(pnode[v], 1); permute(depth[v], 1); permute(onode[v], 1);
+            permute(ocomp[v], 1); permute(oc[v], 1); permute(ok[v], 1); permute(wr, 1);
+            permute(cc[v], kMaxBcDepth); permute(kk[v], kMaxBcDepth);
+            na[v] = (int)A.size();
+            if (na[v] > 0) {
+                writer[v].assign(wr.begin(), wr.begin() + na[v]);
+                first[v].assign(L.n, -1);
+                for (int e = na[v] - 1; e >= 0; e--) {
+                    first[v][wr[e]] = e;
+                    mask[wr[e]] |= (uint8_t)(16 << v);
+                }
+            }
+        }
+        if (getenv("I3G_TRACE"))
+            for (int v = 0; v < 4; v++)
+                fprintf(stderr, "i3g: level %d component %d: %zu boundary rows, %s (%d by a row's thread)\n", l, v,
+                        node[v].size(), na[v] >= 0 ? "in-kernel" : "separate pass", na[v]);
         int rc = upload(c, L.bc, mask);
         if (rc) return rc;
         for (int v = 0; v < 4; v++) {
             BcList &B = L.bcl[v];
             B.n = (int)node[v].size();
+            B.na = na[v];
+            if (na[v] > 0 && ((rc = upload(c, B.first, first[v])) || (rc = upload(c, B.writer, writer[v])))) return rc;
             if ((rc = upload(c, B.node, node[v])) || (rc = upload(c, B.pnode, pnode[v])) ||
                 (rc = upload(c, B.depth, depth[v])) || (rc = upload(c, B.c, cc[v])) || (rc = upload(c, B.k, kk[v])) ||
                 (rc = upload(c, B.onode, onode[v])) || (rc = upload(c, B.ocomp, ocomp[v])) ||
@@ -1156,6 +1415,9 @@ int stokes_alloc(i3g_ctx *c)
     if (const char *e = getenv("I3G_COOP_NODES")) c->coop_nodes = atol(e);
     // CTAs of the tail (I3G_TAIL_CLUSTER, 1: the one-block kernel; 2..16: one thread-block cluster)
     if (const char *e = getenv("I3G_TAIL_CLUSTER")) c->tail_cluster = std::max(1, std::min(16, atoi(e)));
+    // I3G_FUSE: 0 one launch per boundary pass, residual part and transfer component; 1 boundary
+    // rows in-kernel on levels >= 1 (default); 3 on level 0 too
+    if (const char *e = getenv("I3G_FUSE")) c->fuse = atoi(e);
     if (c->tail_cluster > 8) {
         I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1271,7 +1533,7 @@ void stokes_free(i3g_ctx *c)
             cudaFree(L.s.u[v]); cudaFree(L.s.f[v]); cudaFree(L.s.r[v]);
             BcList &B = L.bcl[v];
             cudaFree(B.node); cudaFree(B.pnode); cudaFree(B.depth); cudaFree(B.c); cudaFree(B.k);
-            cudaFree(B.onode); cudaFree(B.ocomp); cudaFree(B.oc); cudaFree(B.ok);
+            cudaFree(B.onode); cudaFree(B.ocomp); cudaFree(B.oc); cudaFree(B.ok); cudaFree(B.first); cudaFree(B.writer);
         }
         cudaFree(L.d.etac); cudaFree(L.d.etaxy); cudaFree(L.d.etaxz); cudaFree(L.d.etayz); cudaFree(L.d.nd);
         cudaFree(L.s.etac); cudaFree(L.s.etaxy); cudaFree(L.s.etaxz); cudaFree(L.s.etayz); cudaFree(L.s.nd);
@@ -1357,11 +1619,24 @@ static void bc_apply(i3g_ctx *c, int l, int v, bool use_c)
            (const int *)B.depth, (const double *)B.c, (const double *)B.k, (int)use_c);
 }
 
+static BcDev bcdev(const BcList &B)
+{
+    return BcDev{B.n, B.na, B.node, B.pnode, B.depth, B.onode, B.ocomp, B.first, B.writer, B.c, B.k, B.ok};
+}
+
 template <typename T>
 static void residual_t(i3g_ctx *c, int l)
 {
     Level &L = c->lev[l];
     View<T> V = view<T>(L, fields<T>(L));
+    if (c->fuse) {
+        BcDev4 B;
+        long nb = 0;
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L.bcl[v]); nb += L.bcl[v].n; }
+        const unsigned rows = nblk(L.n);
+        LAUNCH(k_residual_bc<T>, rows + nblk(nb), 256, V, B, rows);
+        return;
+    }
     LAUNCH(k_residual<T>, nblk(L.n), 256, V);
     for (int v = 0; v < 4; v++) {
         BcList &B = L.bcl[v];
@@ -1379,19 +1654,37 @@ static void smooth_t(i3g_ctx *c, int l, int nsweeps, bool homogeneous, bool with
     const long total = (long)((L.ny + 1) / 2) * L.nx * L.nz;
     const T v0 = (T)c->p.v0koef, p0 = (T)c->p.p0koef;
     const bool use_c = l == 0 && !homogeneous;
+    const unsigned rows = nblk(total), prows = nblk(L.n);
+    // in-kernel boundary rows: coarse levels always (latency-bound launches), level 0 with
+    // I3G_FUSE=3 (its launches are bandwidth-bound and the writers' loads lengthen them)
+    const bool inkernel = c->fuse && (l > 0 || c->fuse >= 3);
+    // colour 1 of a component, with its boundary rows when set-up admitted them in-kernel
+#define LAST_COLOUR(V_)                                                                                 \
+    do {                                                                                                \
+        const BcList &B = L.bcl[V_];                                                                    \
+        if (inkernel && B.na >= 0)                                                                      \
+            LAUNCH((k_relax_vel_bc<T, V_>), rows + nblk(B.n - B.na), 256, V, v0, bcdev(B), (int)use_c, rows); \
+        else {                                                                                          \
+            LAUNCH((k_relax_vel<T, V_>), rows, 256, V, 1, v0);                                          \
+            bc_apply<T>(c, l, V_, use_c);                                                               \
+        }                                                                                               \
+    } while (0)
     for (int s = 0; s < nsweeps; s++) {
-        LAUNCH((k_relax_vel<T, 1>), nblk(total), 256, V, 0, v0);
-        LAUNCH((k_relax_vel<T, 1>), nblk(total), 256, V, 1, v0);
-        bc_apply<T>(c, l, 1, use_c);
-        LAUNCH((k_relax_vel<T, 2>), nblk(total), 256, V, 0, v0);
-        LAUNCH((k_relax_vel<T, 2>), nblk(total), 256, V, 1, v0);
-        bc_apply<T>(c, l, 2, use_c);
-        LAUNCH((k_relax_vel<T, 3>), nblk(total), 256, V, 0, v0);
-        LAUNCH((k_relax_vel<T, 3>), nblk(total), 256, V, 1, v0);
-        bc_apply<T>(c, l, 3, use_c);
-        LAUNCH(k_relax_p<T>, nblk(L.n), 256, V, p0);
-        bc_apply<T>(c, l, 0, use_c);
+        LAUNCH((k_relax_vel<T, 1>), rows, 256, V, 0, v0);
+        LAST_COLOUR(1);
+        LAUNCH((k_relax_vel<T, 2>), rows, 256, V, 0, v0);
+        LAST_COLOUR(2);
+        LAUNCH((k_relax_vel<T, 3>), rows, 256, V, 0, v0);
+        LAST_COLOUR(3);
+        const BcList &B = L.bcl[0];
+        if (inkernel && B.na >= 0)
+            LAUNCH(k_relax_p_bc<T>, prows + nblk(B.n - B.na), 256, V, p0, bcdev(B), (int)use_c, prows);
+        else {
+            LAUNCH(k_relax_p<T>, prows, 256, V, p0);
+            bc_apply<T>(c, l, 0, use_c);
+        }
     }
+#undef LAST_COLOUR
     if (with_residual) residual_t<T>(c, l);
 }
 
@@ -1400,6 +1693,13 @@ static void restrict_t(i3g_ctx *c, int l)
 {
     Level &F = c->lev[l - 1], &Cc = c->lev[l];
     View<T> VF = view<T>(F, fields<T>(F)), VC = view<T>(Cc, fields<T>(Cc));
+    if (c->fuse) {
+        Tr4 R;
+        for (int v = 0; v < 4; v++)
+            for (int ax = 0; ax < 3; ax++) R.t[v][ax] = trview(F.tr[ax][kStag[v][ax]]);
+        LAUNCH(k_restrict4<T>, dim3(nblk(Cc.n), 4), 256, VF, VC, R);
+        return;
+    }
 #define RST(V_) LAUNCH((k_restrict<T, V_>), nblk(Cc.n), 256, VF, VC, trview(F.tr[0][kStag[V_][0]]), \
                        trview(F.tr[1][kStag[V_][1]]), trview(F.tr[2][kStag[V_][2]]))
     RST(1); RST(2); RST(3); RST(0);
@@ -1412,6 +1712,13 @@ static void prolong_t(i3g_ctx *c, int l)
     Level &F = c->lev[l - 1], &Cc = c->lev[l];
     View<T> VF = view<T>(F, fields<T>(F)), VC = view<T>(Cc, fields<T>(Cc));
     const T kv = (T)c->p.v1koef, kp = (T)c->p.p1koef;
+    if (c->fuse) {
+        Tr4 R;
+        for (int v = 0; v < 4; v++)
+            for (int ax = 0; ax < 3; ax++) R.t[v][ax] = trview(F.tr[ax][kStag[v][ax]]);
+        LAUNCH(k_prolong4<T>, dim3(nblk(F.n), 4), 256, VF, VC, R, kv, kp);
+        return;
+    }
 #define PRL(V_, K_) LAUNCH((k_prolong<T, V_>), nblk(F.n), 256, VF, VC, trview(F.tr[0][kStag[V_][0]]), \
                            trview(F.tr[1][kStag[V_][1]]), trview(F.tr[2][kStag[V_][2]]), K_)
     PRL(1, kv); PRL(2, kv); PRL(3, kv); PRL(0, kp);
@@ -1446,7 +1753,7 @@ static void tail_launch(i3g_ctx *c, int lc, int multinum)
         TL.v = view<T>(L, fields<T>(L));
         for (int v = 0; v < 4; v++) {
             const BcList &B = L.bcl[v];
-            TL.bc[v] = BcDev{B.n, B.node, B.pnode, B.depth, B.onode, B.ocomp, B.c, B.k, B.ok};
+            TL.bc[v] = bcdev(B);
             if (q + 1 < a.nl)
                 for (int ax = 0; ax < 3; ax++) TL.tr[v][ax] = trview(L.tr[ax][kStag[v][ax]]);
         }
@@ -1630,9 +1937,8 @@ __global__ void k_copy_back(View<double> L, long pin, double pinit, double *pr, 
     const long N = L.nxy * L.nz;
     const double shift = pinit - L.u0[pin];
     for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
-        const int j = (int)(n % L.ny);
-        const long rest = n / L.ny;
-        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        int i, j, k;
+        node_ijk(L, n, i, j, k);
         if (row_exists(0, i, j, k, L.nx, L.ny, L.nz)) { pr[n] = L.u0[n] + shift; m[3] = fmax(m[3], pr[n]); }
         if (row_exists(1, i, j, k, L.nx, L.ny, L.nz)) { vx[n] = (float)L.u1[n]; m[0] = fmax(m[0], fabs((double)vx[n])); }
         if (row_exists(2, i, j, k, L.nx, L.ny, L.nz)) { vy[n] = (float)L.u2[n]; m[1] = fmax(m[1], fabs((double)vy[n])); }
@@ -1649,6 +1955,50 @@ __global__ void k_copy_back(View<double> L, long pin, double pinit, double *pr, 
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sh[threadIdx.x][w]);
         part[(long)blockIdx.x * 4 + threadIdx.x] = v;
     }
+}
+
+// *flag = 1 where the node arrays differ from what k_copy_back writes for the level-0
+// solution x (pinned pressure shift included): the uploaded state is not the last solution.
+__global__ void k_same_solution(View<double> L, long pin, double pinit, const double *x0, const double *x1,
+                                const double *x2, const double *x3, const double *pr, const float *vx, const float *vy,
+                                const float *vz, int *flag)
+{
+    const long N = L.nxy * L.nz;
+    const double shift = pinit - x0[pin];
+    bool diff = false;
+    for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        node_ijk(L, n, i, j, k);
+        if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(pr[n] == x0[n] + shift)) diff = true;
+        if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(vx[n] == (float)x1[n])) diff = true;
+        if (row_exists(2, i, j, k, L.nx, L.ny, L.nz) && !(vy[n] == (float)x2[n])) diff = true;
+        if (row_exists(3, i, j, k, L.nx, L.ny, L.nz) && !(vz[n] == (float)x3[n])) diff = true;
+    }
+    if (__any_sync(0xffffffffu, diff) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
+// After an upload of nodal fields: keep the extrapolation history only if the uploaded v, P are
+// exactly the last converged solution as the library returned it (a host loop that downloads
+// and re-uploads the state every step); the comparison's result is read at the next solve.
+int stokes_upload_check(i3g_ctx *c)
+{
+    c->hist_check = 0;
+    if (c->nhist == 0 || !c->hist[1][0]) { c->nhist = 0; return 0; }
+    if (!c->dflag) {
+        I3G_CUDA(cudaMalloc((void **)&c->dflag, sizeof(int)));
+        I3G_CUDA(cudaMallocHost((void **)&c->hflag, sizeof(int)));
+    }
+    Level &L0 = c->lev[0];
+    const long pin = ((long)c->m.pzinit * L0.nx + c->m.pxinit) * L0.ny + c->m.pyinit;
+    I3G_CUDA(cudaMemsetAsync(c->dflag, 0, sizeof(int), c->st));
+    k_same_solution<<<std::min<long>(nblk(L0.n), 4L * 148), 256, 0, c->st>>>(
+        view<double>(L0, L0.d), pin, c->m.pinit, c->hist[1][0], c->hist[1][1], c->hist[1][2], c->hist[1][3], c->pr,
+        c->vx, c->vy, c->vz, c->dflag);
+    c->launches++;
+    I3G_CUDA(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    c->hist_check = 1;
+    I3G_CUDA(cudaGetLastError());
+    return 0;
 }
 
 // strain rates and stresses from the FP32 velocities (sxxcalc..syzcalc with ynval = 0)
@@ -2002,9 +2352,8 @@ __global__ void __launch_bounds__(256) k_guess_dots(View<double> L, const double
     double x = 0, y = 0;
     const long N = L.nxy * L.nz;
     for (long n = (long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x) {
-        const int j = (int)(n % L.ny);
-        const long rest = n / L.ny;
-        const int i = (int)(rest % L.nx), k = (int)(rest / L.nx);
+        int i, j, k;
+        node_ijk(L, n, i, j, k);
         const uint8_t b = L.bc[n];
         if (row_exists(0, i, j, k, L.nx, L.ny, L.nz) && !(b & 1)) { const double d = a0[n] - L.r0[n]; x += wc * a0[n] * d; y += wc * d * d; }
         if (row_exists(1, i, j, k, L.nx, L.ny, L.nz) && !(b & 2)) { const double d = a1[n] - L.r1[n]; x += wm * a1[n] * d; y += wm * d * d; }
@@ -2115,11 +2464,18 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
     Vz.u0 = zj; Vz.u1 = zj + N; Vz.u2 = zj + 2 * N; Vz.u3 = zj + 3 * N;
     Vz.f0 = K->F0; Vz.f1 = K->F0 + N; Vz.f2 = K->F0 + 2 * N; Vz.f3 = K->F0 + 3 * N;
     Vz.r0 = K->W; Vz.r1 = K->W + N; Vz.r2 = K->W + 2 * N; Vz.r3 = K->W + 3 * N;
-    LAUNCH(k_residual<double>, nblk(N), 256, Vz);
-    for (int v = 0; v < 4; v++) {
-        BcList &B = L0.bcl[v];
-        if (B.n) LAUNCH(k_bc_residual<double>, nblk(B.n), 256, Vz, v, B.n, (const int *)B.node, (const int *)B.onode,
-                        (const int *)B.ocomp, (const double *)B.ok);
+    if (c->fuse) {
+        BcDev4 B;
+        long nb = 0;
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L0.bcl[v]); nb += L0.bcl[v].n; }
+        LAUNCH(k_residual_bc<double>, nblk(N) + nblk(nb), 256, Vz, B, nblk(N));
+    } else {
+        LAUNCH(k_residual<double>, nblk(N), 256, Vz);
+        for (int v = 0; v < 4; v++) {
+            BcList &B = L0.bcl[v];
+            if (B.n) LAUNCH(k_bc_residual<double>, nblk(B.n), 256, Vz, v, B.n, (const int *)B.node, (const int *)B.onode,
+                            (const int *)B.ocomp, (const double *)B.ok);
+        }
     }
     LAUNCH(k_kr_negscale, nblk(N), 256, N, K->W, d);
     // classical Gram-Schmidt, twice; the second projection's pass also yields w.w, from which the
@@ -2246,7 +2602,15 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     Level &L0 = c->lev[0];
     if (!c->p.warm_start)
         for (int v = 0; v < 4; v++) I3G_CUDA(cudaMemsetAsync(L0.d.u[v], 0, L0.n * 8, c->st));
+    if (c->hist_check) {
+        // the upload comparison was enqueued before this solve: its flag is ready after a sync
+        I3G_CUDA(cudaStreamSynchronize(c->st));
+        if (*c->hflag) c->nhist = 0;
+        c->hist_check = 0;
+    }
+    c->st_.stokes_start = 0;
     if (c->p.warm_start == 2 && c->nhist == 2 && c->hist_dt[0] > 0) {
+        c->st_.stokes_start = 1;
         // linear extrapolation in time from the last two converged solutions
         const double r = c->hist_dt[1] / c->hist_dt[0];
         for (int v = 0; v < 4; v++)
@@ -2300,6 +2664,7 @@ int stokes_solve(i3g_ctx *c, double *timestep)
         c->guess_rel[1] = rdef;
         c->guess_used = (alpha > 0 && rg < rdef) ? 1 : 0;   // false for a NaN residual too
         if (c->guess_used) {
+            c->st_.stokes_start = 2;
             mom = gm;
             cont = gc;
         } else {
@@ -2408,6 +2773,8 @@ int stokes_solve(i3g_ctx *c, double *timestep)
 //   8 / 10 one full sweep (FP32 / FP64: Vx, Vy, Vz red and black, boundary rows, pressure):
 //          4 unknowns read and written, 4 right-hand sides read, 5 FP32 viscosities: 68 / 116 B;
 //   1      FP64 residual: 116 B;  2  restriction: 4 s (1 + 1/8) B;  3  prolongation: 4 s (2 + 1/8) B.
+constexpr int kMaxLevWarm = 6;
+
 int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes)
 {
     if (!c->stokes_ready) {
@@ -2434,6 +2801,32 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
         r++;
         return 0;
     };
+    // warm-cache kinds (the coarse levels of a V-cycle stay in L2): 11 one FP32 V-cycle of the
+    // solver's schedule, 12 its coarse tail kernel alone, 13 + l - 1 one FP32 sweep of level l
+    if (kind >= 11 && kind <= 12 + kMaxLevWarm) {
+        const int mn = c->f.multinum > 0 ? std::min(c->f.multinum, c->nlev - 1) : std::min(c->p.multimax, c->nlev - 1);
+        const int lc = tail_start(c, mn);
+        const int l = kind - 12;
+        if (kind >= 13 && l >= c->nlev) return set_error(c, I3G_E_ARG, "level %d does not exist", l);
+        auto warm = [&]() {
+            if (kind == 11) vcycle_t<float>(c, mn, true);
+            else if (kind == 12) { if (lc <= mn) tail_launch<float>(c, lc, mn); }
+            else smooth_t<float>(c, l, 1, true, false);
+        };
+        for (int w = 0; w < 2; w++) warm();
+        EventPair e;
+        I3G_CUDA(e.create());
+        I3G_CUDA(cudaEventRecord(e.a, c->st));
+        for (int q = 0; q < reps; q++) warm();
+        I3G_CUDA(cudaEventRecord(e.b, c->st));
+        I3G_CUDA(cudaEventSynchronize(e.b));
+        float t = 0;
+        I3G_CUDA(cudaEventElapsedTime(&t, e.a, e.b));
+        *ms = t / reps;
+        *bytes = kind >= 13 ? 68.0 * (double)c->lev[l].n : 0.0;
+        I3G_CUDA(cudaGetLastError());
+        return 0;
+    }
     for (int w = 0; w < 2; w++) launch();   // warm-up (instruction caches, first-touch)
     int rc = cold_time(c, reps, launch, ms);
     if (rc) return rc;

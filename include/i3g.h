@@ -102,7 +102,9 @@ typedef struct i3g_params {
     int32_t precision;                  /* 0: FP64 multigrid, 1: FP32 MG inside FP64 defect correction */
     int32_t warm_start;                 /* 0: zero start; 1: the previous step's v,P (reference behaviour);
                                          * 2: linear extrapolation in time from the last two converged
-                                         * solutions (falls back to 1 until two exist; reset by i3g_upload) */
+                                         * solutions (falls back to 1 until two exist; an upload of nodal
+                                         * fields whose v, P differ from the last solution as downloaded
+                                         * resets it, an upload of exactly that state keeps it) */
     int32_t krylov;                     /* > 0: restarted FGMRES(krylov) (<= 16) on the FP64 residual,
                                          * preconditioned by one V-cycle of this precision (precision 1:
                                          * the FP32 V-cycle on the scaled correction system; precision 0:
@@ -130,6 +132,10 @@ typedef struct i3g_stats {
     double heat_rel;
     double ms_stokes, ms_heat, ms_move, ms_r2n;   /* device time of the last calls        */
     int64_t kernel_launches;            /* kernels launched by this context so far        */
+    int32_t stokes_start;               /* start of the last i3g_stokes: 0 the nodal v, P
+                                           (uploaded or the last solution), 1 extrapolated
+                                           from the last two solutions (warm_start 2), 2 the
+                                           staged guess (i3g_unet_predict)                */
 } i3g_stats;
 
 typedef struct i3g_ctx i3g_ctx;
@@ -265,7 +271,10 @@ int i3g_stokes_stresses(i3g_ctx *c);
 /* Time reps launches of one kernel class on the level-0 data with CUDA events on the
  * context stream; returns the mean duration per launch and the algorithmic bytes that one
  * launch must move.  kind: 0 smoother sweep, 1 residual, 2 restriction, 3 prolongation,
- * 4 marker->node, 5 RK4 advection, 6 heat sweep. */
+ * 4 marker->node, 5 RK4 advection, 6 heat sweep, 7 one FP32 velocity colour, 8 one FP32
+ * level-0 sweep, 9 marker temperatures, 10 one FP64 level-0 sweep (kinds 0-10 with L2
+ * flushed before every launch); with warm caches: 11 one FP32 V-cycle of the solver's schedule,
+ * 12 its coarse tail kernel, 13 + l - 1 one FP32 sweep of level l >= 1. */
 int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, double *bytes_per_launch);
 
 /* Device-side stopwatch on the context stream (no reference counterpart: the reference

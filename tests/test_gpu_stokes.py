@@ -72,14 +72,19 @@ def test_residual_smooth_transfer_bit_exact(name):
         assert np.array_equal(g.get(abi.A_SOL, l - 1, 4 * sizes[l - 1]), o.get(abi.A_SOL, l - 1, 4 * sizes[l - 1])), ("prolong", l)
 
 
-@pytest.mark.parametrize("tail", ["12000", "2000", "0", "coop", "cluster"])
+@pytest.mark.parametrize("tail", ["12000", "2000", "0", "0-separate", "0-level0", "coop", "cluster"])
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_vcycles_bit_exact(name, tail, monkeypatch):
     """V-cycles equal the oracle's bit for bit, with the small levels in the one-block tail
-    kernel (default), with one kernel per phase on every level (I3G_TAIL_NODES=0), with every
-    coarse level in the cooperative grid-wide kernel (I3G_COOP_NODES), and with the tail on a
-    16-CTA thread-block cluster (I3G_TAIL_CLUSTER)."""
-    if tail == "coop":
+    kernel (default), with one kernel per phase on every level (I3G_TAIL_NODES=0), the same
+    with separate boundary, residual and transfer launches (I3G_FUSE=0) and with in-kernel
+    boundary rows on level 0 too (I3G_FUSE=3), with every coarse
+    level in the cooperative grid-wide kernel (I3G_COOP_NODES), and with the tail on a 16-CTA
+    thread-block cluster (I3G_TAIL_CLUSTER)."""
+    if tail in ("0-separate", "0-level0"):
+        monkeypatch.setenv("I3G_TAIL_NODES", "0")
+        monkeypatch.setenv("I3G_FUSE", "0" if tail == "0-separate" else "3")
+    elif tail == "coop":
         monkeypatch.setenv("I3G_COOP_NODES", "1000000")
     elif tail == "cluster":
         monkeypatch.setenv("I3G_TAIL_NODES", "12000")
