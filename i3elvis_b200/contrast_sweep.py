@@ -1,6 +1,7 @@
 """Viscosity-contrast sweep: mixed precision against FP64 on the 129^3 inclusion model.
 
-    python -m i3elvis_b200.contrast_sweep [--n 129] [--contrasts 1e2,1e4,1e6]
+    python -m i3elvis_b200.contrast_sweep [--n 129] [--contrasts 1e2,1e4,1e6] [--krylov 12]
+                                          [--maxcyc 3000] [--solvers fp64,fp64k,mixed]
 
 For each contrast C the 100 seeded inclusions get viscosity contrasts log-uniform in [1, C]
 against the Arrhenius matrix (binned into rock types as ``model.random_inclusions`` does).
@@ -70,7 +71,7 @@ def _rel(a, b):
     return float(d / n) if n > 0 else float(d)
 
 
-def run(n=129, contrasts=(1e2, 1e4, 1e6), mnum=3, multinum=4, seed=7):
+def run(n=129, contrasts=(1e2, 1e4, 1e6), mnum=3, multinum=4, seed=7, krylov=12, maxcyc=3000, solvers=None):
     out = []
     for C in contrasts:
         prn, _ = model.random_inclusions(n=n, mnum=mnum, multinum=multinum, seed=seed, count=100, contrast=C)
@@ -82,18 +83,20 @@ def run(n=129, contrasts=(1e2, 1e4, 1e6), mnum=3, multinum=4, seed=7):
         light = copy.deepcopy(mode)
         light.multinnn = _sweeps(multinum, True)
         runs = {
-            "ref": (light, dict(stokes_rtol=1e-11, stokes_maxcyc=1500, precision=0, krylov=12)),
+            "ref": (light, dict(stokes_rtol=1e-11, stokes_maxcyc=1500, precision=0, krylov=krylov)),
             "fp64": (mode, dict(stokes_rtol=1e-8, precision=0, krylov=0)),
-            "fp64k": (light, dict(stokes_rtol=1e-8, precision=0, krylov=12)),
-            "mixed": (light, dict(stokes_rtol=1e-8, precision=1, krylov=12)),
+            "fp64k": (light, dict(stokes_rtol=1e-8, precision=0, krylov=krylov)),
+            "mixed": (light, dict(stokes_rtol=1e-8, precision=1, krylov=krylov)),
         }
+        if solvers:
+            runs = {k: v for k, v in runs.items() if k == "ref" or k in solvers}
         ctx = lib.Context(abi.ModelBuffers(prn, pinned=True), abi.make_params(mode), abi.make_file_params(f))
         runtime.prepare(ctx)
         s0 = _state(ctx)
         res = {}
         for name, (md, solver) in runs.items():
             _restore(ctx, s0)
-            ctx.set_params(abi.make_params(md, heat_rtol=1e-10, **{"stokes_maxcyc": 3000, **solver}))
+            ctx.set_params(abi.make_params(md, heat_rtol=1e-10, **{"stokes_maxcyc": maxcyc, **solver}))
             conv = True
             try:
                 dt = ctx.stokes(0, f.maxtmstep_yr * YEAR)
@@ -117,7 +120,10 @@ def run(n=129, contrasts=(1e2, 1e4, 1e6), mnum=3, multinum=4, seed=7):
         ctx.close()
         ref = res["ref"]
         line = {"contrast": C, "n": n, "markers": prn.marknum, "ref_cycles": ref["cycles"], "ref_rel": ref["rel"]}
+        line["krylov"] = krylov
         for name in ("fp64", "fp64k", "mixed"):
+            if name not in res:
+                continue
             r = res[name]
             line[name] = {"cycles": r["cycles"], "rel": r["rel"], "converged": r["converged"],
                           "ms_stokes": r["ms_stokes"], "ms_heat": r["ms_heat"],
@@ -132,8 +138,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=129)
     ap.add_argument("--contrasts", default="1e2,1e4,1e6")
+    ap.add_argument("--krylov", type=int, default=12, help="FGMRES restart length (<= 16)")
+    ap.add_argument("--maxcyc", type=int, default=3000, help="V-cycle cap of the 1e-8 solves")
+    ap.add_argument("--solvers", default="fp64,fp64k,mixed", help="solvers besides the FP64 reference solve")
     a = ap.parse_args()
-    run(n=a.n, contrasts=tuple(float(x) for x in a.contrasts.split(",")))
+    run(n=a.n, contrasts=tuple(float(x) for x in a.contrasts.split(",")), krylov=a.krylov, maxcyc=a.maxcyc,
+        solvers=tuple(a.solvers.split(",")))
 
 
 if __name__ == "__main__":

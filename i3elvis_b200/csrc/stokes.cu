@@ -2774,6 +2774,7 @@ int stokes_solve(i3g_ctx *c, double *timestep)
 //          4 unknowns read and written, 4 right-hand sides read, 5 FP32 viscosities: 68 / 116 B;
 //   1      FP64 residual: 116 B;  2  restriction: 4 s (1 + 1/8) B;  3  prolongation: 4 s (2 + 1/8) B.
 constexpr int kMaxLevWarm = 6;
+constexpr int kWarmLevel0 = 19;
 
 int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes)
 {
@@ -2803,10 +2804,10 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
     };
     // warm-cache kinds (the coarse levels of a V-cycle stay in L2): 11 one FP32 V-cycle of the
     // solver's schedule, 12 its coarse tail kernel alone, 13 + l - 1 one FP32 sweep of level l
-    if (kind >= 11 && kind <= 12 + kMaxLevWarm) {
+    if ((kind >= 11 && kind <= 12 + kMaxLevWarm) || kind == kWarmLevel0) {
         const int mn = c->f.multinum > 0 ? std::min(c->f.multinum, c->nlev - 1) : std::min(c->p.multimax, c->nlev - 1);
         const int lc = tail_start(c, mn);
-        const int l = kind - 12;
+        const int l = kind == kWarmLevel0 ? 0 : kind - 12;
         if (kind >= 13 && l >= c->nlev) return set_error(c, I3G_E_ARG, "level %d does not exist", l);
         auto warm = [&]() {
             if (kind == 11) vcycle_t<float>(c, mn, true);
@@ -2823,7 +2824,7 @@ int stokes_time_kernel(i3g_ctx *c, int kind, int reps, double *ms, double *bytes
         float t = 0;
         I3G_CUDA(cudaEventElapsedTime(&t, e.a, e.b));
         *ms = t / reps;
-        *bytes = kind >= 13 ? 68.0 * (double)c->lev[l].n : 0.0;
+        *bytes = kind >= 13 || kind == kWarmLevel0 ? 68.0 * (double)c->lev[l].n : 0.0;
         I3G_CUDA(cudaGetLastError());
         return 0;
     }

@@ -274,7 +274,8 @@ int i3g_stokes_stresses(i3g_ctx *c);
  * 4 marker->node, 5 RK4 advection, 6 heat sweep, 7 one FP32 velocity colour, 8 one FP32
  * level-0 sweep, 9 marker temperatures, 10 one FP64 level-0 sweep (kinds 0-10 with L2
  * flushed before every launch); with warm caches: 11 one FP32 V-cycle of the solver's schedule,
- * 12 its coarse tail kernel, 13 + l - 1 one FP32 sweep of level l >= 1. */
+ * 12 its coarse tail kernel, 13 + l - 1 one FP32 sweep of level l >= 1, 19 one FP32 sweep of
+ * level 0. */
 int i3g_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_per_launch, double *bytes_per_launch);
 
 /* Device-side stopwatch on the context stream (no reference counterpart: the reference
