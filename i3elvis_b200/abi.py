@@ -103,7 +103,7 @@ class Params(C.Structure):
         ("timebeg", C.c_double), ("timeend", C.c_double), ("tempend", C.c_double),
         ("stokes_rtol", C.c_double), ("stokes_maxcyc", C.c_int32), ("heat_rtol", C.c_double),
         ("heat_maxcyc", C.c_int32), ("precision", C.c_int32), ("warm_start", C.c_int32),
-        ("krylov", C.c_int32),
+        ("krylov", C.c_int32), ("marker_exact", C.c_int32),
     ]
 
 
@@ -236,6 +236,7 @@ def make_params(mode: Mode, **solver) -> Params:
     p.precision = solver.get("precision", 0)
     p.warm_start = solver.get("warm_start", 1)
     p.krylov = solver.get("krylov", 0)
+    p.marker_exact = solver.get("marker_exact", 0)
     return p
 
 

@@ -73,7 +73,27 @@ struct Grid {
     double xsize, ysize, zsize;
     const double *gx, *gy, *gz;     // shared-memory copies inside kernels
     double ux, uy, uz;              // 1 / spacing of a uniform axis, 0 when not uniform
+    // per-axis tables of the fast arithmetic (shared memory, filled by load_grid<false>), index
+    // 0 = x, 1 = y, 2 = z: mid-points (g[i] + g[i+1]) / 2, 1 / (g[i+1] - g[i]) and
+    // 1 / ((g[i+2] - g[i]) / 2)
+    const double *gm[3], *rl[3], *rm[3];
 };
+
+// Interpolation arithmetic of the marker kernels, chosen per launch by the template flag EX:
+//  * EX = true: the reference's expressions in its operation order -- one correctly rounded
+//    division per weight, separate multiply and add (this file is compiled with -fmad=false),
+//    sums over the 8 corners in the reference's loop order.  Marker positions, strains and
+//    types come out bit-identical to the reference's movemark.
+//  * EX = false: the same weights from per-interval reciprocal tables, written as the distance
+//    to the other node times 1 / spacing (so a point on a node gets exactly zero weight for the
+//    other one, like the reference: a marker on a wall keeps its exactly zero wall velocity),
+//    fused multiply-adds and factorised trilinear sums (y, then x, then z).  Each interpolated
+//    value differs from the exact one by a few units in the last place of FP64 times the sum of
+//    |node value x weight|; the new FP32 positions x + dt v differ only when that double lies
+//    within ~1e-12 m of an FP32 rounding boundary.  Node averages and marker temperatures are
+//    compared with tolerances either way.
+template <bool EX>
+__device__ __forceinline__ double quot(double a, double b, double rb) { return EX ? a / b : a * rb; }
 
 __device__ __forceinline__ int bsearch_g(const double *g, int n, double x)
 {
@@ -123,13 +143,24 @@ struct Ax {
     double w0, w1;
 };
 
+__device__ __forceinline__ Ax clamped(Ax a) { return Ax{a.i, clamp01(a.w0), clamp01(a.w1)}; }
+
 // node-line stencil of a component along its own axis (vxyzcalc1, e.g. Vx in x,
 // mark3mg.c:2370-2395): i = cell clamped to [lo, n - 2 - hi_off]
-__device__ __forceinline__ Ax ax_line(const double *g, int n, int m, double x, int lo, int hi)
+// (axis q: 0 = x, 1 = y, 2 = z; the fast tables of that axis)
+template <bool EX>
+__device__ __forceinline__ Ax ax_line(const Grid &G, int q, const double *g, int n, int m, double x, int lo, int hi)
 {
     int a = m;
     if (a < lo) a = lo;
     if (a > n - hi) a = n - hi;
+    if (!EX) {
+        // each weight is the distance to the other node times 1 / spacing: a point on a node
+        // gets exactly 0 for the other one, as in the reference (a wall node's zero velocity
+        // then stays exactly zero)
+        const double r = G.rl[q][a];
+        return Ax{a, (g[a + 1] - x) * r, (x - g[a]) * r};
+    }
     const double d = g[a + 1] - g[a];
     double t0 = (g[a] - x) / d, t1 = (g[a + 1] - x) / d;
     t0 = -t0;
@@ -138,9 +169,18 @@ __device__ __forceinline__ Ax ax_line(const double *g, int n, int m, double x, i
 
 // mid-point stencil across a staggered axis (vxyzcalc1, e.g. Vx in y): i = cell, minus one below
 // the cell's mid-point, clamped to [0, n - 3]; nodes are the mid-points (g[k] + g[k+1]) / 2
-__device__ __forceinline__ Ax ax_mid(const double *g, int n, int m, double x)
+template <bool EX>
+__device__ __forceinline__ Ax ax_mid(const Grid &G, int q, const double *g, int n, int m, double x)
 {
     int b = m;
+    if (!EX) {
+        const double *gm = G.gm[q];   // the same mid-point values, bit for bit
+        if (x < gm[b]) b -= 1;
+        if (b < 0) b = 0;
+        if (b > n - 3) b = n - 3;
+        const double r = G.rm[q][b];
+        return Ax{b, (gm[b + 1] - x) * r, (x - gm[b]) * r};
+    }
     if (x < (g[b] + g[b + 1]) / 2.0) b -= 1;
     if (b < 0) b = 0;
     if (b > n - 3) b = n - 3;
@@ -152,8 +192,21 @@ __device__ __forceinline__ Ax ax_mid(const double *g, int n, int m, double x)
 
 // cell-centre stencil of epscalc1's normal components (mark3mg.c:2562-2600): i = cell, plus one
 // above the mid-point, clamped to [1, n - 2]; nodes are (g[k-1] + g[k]) / 2; weights in [0, 1]
-__device__ __forceinline__ Ax ax_cent(const double *g, int n, int m, double x)
+__device__ __forceinline__ Ax ax_cent_raw(const Grid &G, int q, int n, int m, double x)
 {
+    const double *gm = G.gm[q];
+    int a = m;
+    if (x > gm[a]) a += 1;
+    if (a < 1) a = 1;
+    if (a > n - 2) a = n - 2;
+    const double r = G.rm[q][a - 1];   // 1 / ((g[a+1] - g[a-1]) / 2)
+    return Ax{a, (gm[a] - x) * r, (x - gm[a - 1]) * r};
+}
+
+template <bool EX>
+__device__ __forceinline__ Ax ax_cent(const Grid &G, int q, const double *g, int n, int m, double x)
+{
+    if (!EX) return clamped(ax_cent_raw(G, q, n, m, x));
     int a = m;
     if (x > (g[a] + g[a + 1]) / 2.0) a += 1;
     if (a < 1) a = 1;
@@ -164,13 +217,30 @@ __device__ __forceinline__ Ax ax_cent(const double *g, int n, int m, double x)
     return Ax{a, clamp01(1.0 - t0), clamp01(1.0 - t1)};
 }
 
-__device__ __forceinline__ Ax clamped(Ax a) { return Ax{a.i, clamp01(a.w0), clamp01(a.w1)}; }
+// factorised trilinear sum of val(node) from node n0 (fast arithmetic): pairs along y, then x,
+// then z, 14 FP64 operations instead of 28
+template <class Fn>
+__device__ __forceinline__ double tri_fact(int n0, int NY, int NXY, const Ax &X, const Ax &Y, const Ax &Z, Fn val)
+{
+    double u[2];
+#pragma unroll
+    for (int k3 = 0; k3 < 2; k3++) {
+        const int b = n0 + k3 * NXY;
+        const double a0 = fma(val(b + 1), Y.w1, val(b) * Y.w0);
+        const double a1 = fma(val(b + NY + 1), Y.w1, val(b + NY) * Y.w0);
+        u[k3] = fma(a1, X.w1, a0 * X.w0);
+    }
+    return fma(u[1], Z.w1, u[0] * Z.w0);
+}
 
-// sum over the 8 corners of f * ((ddx * ddy) * ddz) in the reference's loop order z, x, y; node
-// offsets in 32 bits (a level-0 grid has fewer than 2^31 nodes)
+// sum over the 8 corners of f * ((ddx * ddy) * ddz) in the reference's loop order z, x, y (EX)
+// or factorised (fast); node offsets in 32 bits (a level-0 grid has fewer than 2^31 nodes)
+template <bool EX>
 __device__ __forceinline__ double tri(const float *__restrict__ f, int NY, int NXY, const Ax &X, const Ax &Y, const Ax &Z)
 {
-    const float *p = f + (Z.i * NXY + X.i * NY + Y.i);
+    const int n0 = Z.i * NXY + X.i * NY + Y.i;
+    if (!EX) return tri_fact(n0, NY, NXY, X, Y, Z, [&](int n) { return (double)__ldg(f + n); });
+    const float *p = f + n0;
     double s = 0;
 #pragma unroll
     for (int k3 = 0; k3 < 2; k3++) {
@@ -196,6 +266,7 @@ struct VStencil {
 
 // vxyzcalc1 (mark3mg.c:2347-2530): staggered trilinear velocity at a point.  Vx uses
 // (line x, mid y, mid z), Vy (mid x, line y, mid z), Vz (mid x, mid y, line z).
+template <bool EX>
 __device__ __forceinline__ void vxyz(const Grid &G, const NodeF &F, double x, double y, double z, double *v, int *wn,
                                      VStencil *out = nullptr)
 {
@@ -206,24 +277,31 @@ __device__ __forceinline__ void vxyz(const Grid &G, const NodeF &F, double x, do
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
     const int m1 = wn[0] = locate(gx, X, x, G.ux), m2 = wn[1] = locate(gy, Y, y, G.uy), m3 = wn[2] = locate(gz, Z, z, G.uz);
     VStencil S;
-    S.lx = ax_line(gx, X, m1, x, 0, 2);
-    S.ly = ax_line(gy, Y, m2, y, 0, 2);
-    S.lz = ax_line(gz, Z, m3, z, 0, 2);
-    S.mx = ax_mid(gx, X, m1, x);
-    S.my = ax_mid(gy, Y, m2, y);
-    S.mz = ax_mid(gz, Z, m3, z);
+    S.lx = ax_line<EX>(G, 0, gx, X, m1, x, 0, 2);
+    S.ly = ax_line<EX>(G, 1, gy, Y, m2, y, 0, 2);
+    S.lz = ax_line<EX>(G, 2, gz, Z, m3, z, 0, 2);
+    S.mx = ax_mid<EX>(G, 0, gx, X, m1, x);
+    S.my = ax_mid<EX>(G, 1, gy, Y, m2, y);
+    S.mz = ax_mid<EX>(G, 2, gz, Z, m3, z);
     const int NY = (int)F.NY, NXY = (int)F.NXY;
-    v[0] = tri(F.vx, NY, NXY, S.lx, S.my, S.mz);
-    v[1] = tri(F.vy, NY, NXY, S.mx, S.ly, S.mz);
-    v[2] = tri(F.vz, NY, NXY, S.mx, S.my, S.lz);
+    v[0] = tri<EX>(F.vx, NY, NXY, S.lx, S.my, S.mz);
+    v[1] = tri<EX>(F.vy, NY, NXY, S.mx, S.ly, S.mz);
+    v[2] = tri<EX>(F.vz, NY, NXY, S.mx, S.my, S.lz);
     if (out) *out = S;
 }
 
 // one shear group of epscalc1: strain rate, stress and the dissipation term 2 s e w
+template <bool EX>
 __device__ __forceinline__ void edge_group(const float *__restrict__ fe, const float *__restrict__ fs, int NY, int NXY,
                                            const Ax &AX, const Ax &AY, const Ax &AZ, double &e, double &s, double &d)
 {
     const int n0 = AZ.i * NXY + AX.i * NY + AY.i;
+    if (!EX) {
+        e += tri_fact(n0, NY, NXY, AX, AY, AZ, [&](int n) { return (double)__ldg(fe + n); });
+        s += tri_fact(n0, NY, NXY, AX, AY, AZ, [&](int n) { return (double)__ldg(fs + n); });
+        d += tri_fact(n0, NY, NXY, AX, AY, AZ, [&](int n) { return 2.0 * (double)__ldg(fs + n) * (double)__ldg(fe + n); });
+        return;
+    }
 #pragma unroll
     for (int k3 = 0; k3 < 2; k3++) {
         const double ddz = k3 ? AZ.w1 : AZ.w0;
@@ -247,6 +325,7 @@ __device__ __forceinline__ void edge_group(const float *__restrict__ fe, const f
 // epscalc1 (mark3mg.c:2535-2838) at the point of the first vxyz call, from its cell and
 // mid-point stencils: normal strain rates, stresses and pressure at cell centres, the three
 // shear groups on their edges, and the dissipation sum, each with weights clamped to [0, 1].
+template <bool EX>
 __device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x, double y, double z, const int *wn,
                                          const VStencil &S, double *e, double *s, double *dis)
 {
@@ -259,8 +338,34 @@ __device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x
     for (int i = 0; i < 7; i++) e[i] = 0;
     for (int i = 0; i < 6; i++) s[i] = 0;
     double d = 0;
+    if (!EX) {
+        const Ax cx = ax_cent<false>(G, 0, gx, X, wn[0], x), cy = ax_cent<false>(G, 1, gy, Y, wn[1], y),
+                 cz = ax_cent<false>(G, 2, gz, Z, wn[2], z);
+        const int n0 = cz.i * NXY + cx.i * NY + cy.i;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            e[q] = tri_fact(n0, NY, NXY, cx, cy, cz, [&](int n) { return (double)__ldg(F.e[q] + n); });
+            s[q] = tri_fact(n0, NY, NXY, cx, cy, cz, [&](int n) { return (double)__ldg(F.s[q] + n); });
+        }
+        e[6] = tri_fact(n0, NY, NXY, cx, cy, cz, [&](int n) { return __ldg(F.pr + n); });
+        // the dissipation of the normal components: the FP32 sum of the three products per corner
+        d = tri_fact(n0, NY, NXY, cx, cy, cz, [&](int n) {
+            return (double)__fadd_rn(__fadd_rn(__fmul_rn(__ldg(F.s[0] + n), __ldg(F.e[0] + n)),
+                                               __fmul_rn(__ldg(F.s[1] + n), __ldg(F.e[1] + n))),
+                                     __fmul_rn(__ldg(F.s[2] + n), __ldg(F.e[2] + n)));
+        });
+        const Ax ix = clamped(ax_line<false>(G, 0, gx, X, wn[0], x, 1, 3)), iy = clamped(ax_line<false>(G, 1, gy, Y, wn[1], y, 1, 3)),
+                 iz = clamped(ax_line<false>(G, 2, gz, Z, wn[2], z, 1, 3));
+        const Ax qx = clamped(S.mx), qy = clamped(S.my), qz = clamped(S.mz);
+        edge_group<false>(F.e[3], F.s[3], NY, NXY, ix, iy, qz, e[3], s[3], d);   // exy
+        edge_group<false>(F.e[4], F.s[4], NY, NXY, ix, qy, iz, e[4], s[4], d);   // exz
+        edge_group<false>(F.e[5], F.s[5], NY, NXY, qx, iy, iz, e[5], s[5], d);   // eyz
+        *dis = d;
+        return;
+    }
     {
-        const Ax cx = ax_cent(gx, X, wn[0], x), cy = ax_cent(gy, Y, wn[1], y), cz = ax_cent(gz, Z, wn[2], z);
+        const Ax cx = ax_cent<true>(G, 0, gx, X, wn[0], x), cy = ax_cent<true>(G, 1, gy, Y, wn[1], y),
+                 cz = ax_cent<true>(G, 2, gz, Z, wn[2], z);
         const int n0 = cz.i * NXY + cx.i * NY + cy.i;
 #pragma unroll
         for (int k3 = 0; k3 < 2; k3++) {
@@ -284,12 +389,12 @@ __device__ __forceinline__ void eps_from(const Grid &G, const NodeF &F, double x
         }
     }
     // edge groups: node lines clamped to [1, n - 3] and the mid-point stencils, weights in [0, 1]
-    const Ax ix = clamped(ax_line(gx, X, wn[0], x, 1, 3)), iy = clamped(ax_line(gy, Y, wn[1], y, 1, 3)),
-             iz = clamped(ax_line(gz, Z, wn[2], z, 1, 3));
+    const Ax ix = clamped(ax_line<true>(G, 0, gx, X, wn[0], x, 1, 3)), iy = clamped(ax_line<true>(G, 1, gy, Y, wn[1], y, 1, 3)),
+             iz = clamped(ax_line<true>(G, 2, gz, Z, wn[2], z, 1, 3));
     const Ax qx = clamped(S.mx), qy = clamped(S.my), qz = clamped(S.mz);
-    edge_group(F.e[3], F.s[3], NY, NXY, ix, iy, qz, e[3], s[3], d);   // exy
-    edge_group(F.e[4], F.s[4], NY, NXY, ix, qy, iz, e[4], s[4], d);   // exz
-    edge_group(F.e[5], F.s[5], NY, NXY, qx, iy, iz, e[5], s[5], d);   // eyz
+    edge_group<true>(F.e[3], F.s[3], NY, NXY, ix, iy, qz, e[3], s[3], d);   // exy
+    edge_group<true>(F.e[4], F.s[4], NY, NXY, ix, qy, iz, e[4], s[4], d);   // exz
+    edge_group<true>(F.e[5], F.s[5], NY, NXY, qx, iy, iz, e[5], s[5], d);   // eyz
     *dis = d;
 }
 
@@ -383,6 +488,7 @@ __device__ void eps_at(const Grid &G, const NodeF &F, double x, double y, double
 }
 
 // prcalc1 (mark3mg.c:2917-3001)
+template <bool EX>
 __device__ double pr_at(const Grid &G, const double *pr, long NY, long NXY, double x, double y, double z, int *wn)
 {
     const double *gx = G.gx, *gy = G.gy, *gz = G.gz;
@@ -391,6 +497,10 @@ __device__ double pr_at(const Grid &G, const double *pr, long NY, long NXY, doub
     if (y < 0) y = 0; if (y > G.ysize) y = G.ysize;
     if (z < 0) z = 0; if (z > G.zsize) z = G.zsize;
     const int m1 = wn[0] = locate(gx, X, x, G.ux), m2 = wn[1] = locate(gy, Y, y, G.uy), m3 = wn[2] = locate(gz, Z, z, G.uz);
+    if (!EX) {   // prcalc1's cell-centre stencil: ax_cent without the clamp of the weights
+        const Ax A = ax_cent_raw(G, 0, X, m1, x), B = ax_cent_raw(G, 1, Y, m2, y), C = ax_cent_raw(G, 2, Z, m3, z);
+        return tri_fact(C.i * (int)NXY + A.i * (int)NY + B.i, (int)NY, (int)NXY, A, B, C, [&](int n) { return __ldg(pr + n); });
+    }
     int a = m1, b = m2, c = m3;
     if (x > (gx[a] + gx[a + 1]) / 2.0) a += 1; if (a < 1) a = 1; if (a > X - 2) a = X - 2;
     if (y > (gy[b] + gy[b + 1]) / 2.0) b += 1; if (b < 1) b = 1; if (b > Y - 2) b = Y - 2;
@@ -506,14 +616,36 @@ __device__ double visc(const Phys &P, double mtk, double mpb, int mm2, double ep
     return nueff;
 }
 
+// Grid lines to shared memory (n = nx + ny + nz doubles); with EX = false also the fast
+// arithmetic's tables: mid-points, 1 / spacing and 1 / half double-spacing (3 n more doubles,
+// computed from the global copy, so no barrier is needed between the two)
+template <bool EX>
 __device__ __forceinline__ void load_grid(const Grid &Gg, double *sh, Grid &G)
 {
     const int n = Gg.nx + Gg.ny + Gg.nz;
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        sh[i] = i < Gg.nx ? Gg.gx[i] : i < Gg.nx + Gg.ny ? Gg.gy[i - Gg.nx] : Gg.gz[i - Gg.nx - Gg.ny];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int q = i < Gg.nx ? 0 : i < Gg.nx + Gg.ny ? 1 : 2;
+        const int j = i - (q == 0 ? 0 : q == 1 ? Gg.nx : Gg.nx + Gg.ny);
+        const int na = q == 0 ? Gg.nx : q == 1 ? Gg.ny : Gg.nz;
+        const double *g = q == 0 ? Gg.gx : q == 1 ? Gg.gy : Gg.gz;
+        sh[i] = g[j];
+        if (!EX) {
+            sh[n + i] = j + 1 < na ? (g[j] + g[j + 1]) / 2.0 : 0.0;
+            sh[2 * n + i] = j + 1 < na ? 1.0 / (g[j + 1] - g[j]) : 0.0;
+            sh[3 * n + i] = j + 2 < na ? 1.0 / ((g[j + 2] - g[j]) / 2.0) : 0.0;
+        }
+    }
     __syncthreads();
     G = Gg;
     G.gx = sh; G.gy = sh + Gg.nx; G.gz = sh + Gg.nx + Gg.ny;
+    if (!EX) {
+        const int off[3] = {0, Gg.nx, Gg.nx + Gg.ny};
+        for (int q = 0; q < 3; q++) {
+            G.gm[q] = sh + n + off[q];
+            G.rl[q] = sh + 2 * n + off[q];
+            G.rm[q] = sh + 3 * n + off[q];
+        }
+    }
 }
 
 // second invariant (mark3mg.c:73-74 computes it as pow(., 0.5)): the correctly rounded square
@@ -527,6 +659,7 @@ __device__ __forceinline__ double inv2(const double *e)
 // movemark: rheology update + RK4 (mark3mg.c:49-310)
 // ------------------------------------------------------------------------------------
 // one marker of movemark (mark3mg.c:49-310)
+template <bool EX>
 __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, const NodeF &F, const Phys &P, double timestep)
 {
     int t = M.t[i];
@@ -538,8 +671,8 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
     double v1[3], e[7], s[6], dis;
     int wn[3];
     VStencil S0;
-    vxyz(G, F, fx, fy, fz, v1, wn, &S0);
-    eps_from(G, F, fx, fy, fz, wn, S0, e, s, &dis);
+    vxyz<EX>(G, F, fx, fy, fz, v1, wn, &S0);
+    eps_from<EX>(G, F, fx, fy, fz, wn, S0, e, s, &dis);
     const double eii = inv2(e), sii = inv2(s);
     const double mpb = e[6] * 1e-5;
     float mk = M.k[i], mv = M.v[i], me = M.e[i], mft = M.ft[i], mw = M.w[i];
@@ -547,7 +680,9 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
     if (t < 50 && mtk > 0) {
         double rii = 1.0;
         if (mv > 0 && fx > G.gx[3] && fx < G.gx[G.nx - 4] && fy > G.gy[3] && fy < G.gy[G.ny - 4] && fz > G.gz[3] && fz < G.gz[G.nz - 4])
-            rii *= pow(0.5 * sii / eii / mv, 0.87);
+            // the power law of the stress ratio; the fast arithmetic takes it as exp(0.87 log r)
+            // (relative difference ~1e-15, far below the FP32 viscosity it feeds)
+            rii *= EX ? pow(0.5 * sii / eii / mv, 0.87) : exp(0.87 * log(0.5 * sii / eii / mv));
         const double mnu = visc(P, mtk, mpb, t, eii, rii, me, mft);
         if (mnu < 0) { atomicOr(P.err, ERR_GRAIN); return; }
         mv = (float)mnu;
@@ -559,10 +694,10 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
     if (P.markmod == 1) { v[0] = v1[0]; v[1] = v1[1]; v[2] = v1[2]; }
     else {
         double v2[3], v3[3], v4[3];
-        vxyz(G, F, fx + v1[0] * timestep / 2.0, fy + v1[1] * timestep / 2.0, fz + v1[2] * timestep / 2.0, v2, wn);
-        vxyz(G, F, fx + v2[0] * timestep / 2.0, fy + v2[1] * timestep / 2.0, fz + v2[2] * timestep / 2.0, v3, wn);
-        vxyz(G, F, fx + v3[0] * timestep, fy + v3[1] * timestep, fz + v3[2] * timestep, v4, wn);
-        for (int k = 0; k < 3; k++) v[k] = (v1[k] + 2.0 * v2[k] + 2.0 * v3[k] + v4[k]) / 6.0;
+        vxyz<EX>(G, F, fx + v1[0] * timestep / 2.0, fy + v1[1] * timestep / 2.0, fz + v1[2] * timestep / 2.0, v2, wn);
+        vxyz<EX>(G, F, fx + v2[0] * timestep / 2.0, fy + v2[1] * timestep / 2.0, fz + v2[2] * timestep / 2.0, v3, wn);
+        vxyz<EX>(G, F, fx + v3[0] * timestep, fy + v3[1] * timestep, fz + v3[2] * timestep, v4, wn);
+        for (int k = 0; k < 3; k++) v[k] = quot<EX>(v1[k] + 2.0 * v2[k] + 2.0 * v3[k] + v4[k], 6.0, 1.0 / 6.0);
     }
     if (P.outgrid == 2) {
         if (fx < 0 || (double)fx > G.xsize) v[1] = v[2] = 0;
@@ -590,14 +725,14 @@ __device__ __forceinline__ void move_one(const Marks &M, long i, const Grid &G, 
 // Persistent grid-stride launch (a few CTAs per SM): the grid lines are staged in shared memory
 // once per CTA instead of once per 256 markers.  Markers are in (tile, cell) order from the last
 // sort, so a warp's interpolation corners hit the same L1 lines.
-template <int MINB>
+template <bool EX, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_move(Marks M, long n, Grid Gg, NodeF F, Phys P, double timestep)
 {
     extern __shared__ double shg[];
     Grid G;
-    load_grid(Gg, shg, G);
+    load_grid<EX>(Gg, shg, G);
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        move_one(M, i, G, F, P, timestep);
+        move_one<EX>(M, i, G, F, P, timestep);
 }
 
 // ------------------------------------------------------------------------------------
@@ -628,7 +763,7 @@ __global__ void k_tile_key(Marks M, long n, Grid Gg, TileGeo T, int *key, int *c
 {
     extern __shared__ double shg[];
     Grid G;
-    load_grid(Gg, shg, G);
+    load_grid<true>(Gg, shg, G);
     for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         const long i = base + threadIdx.x;
         int kk = T.ntiles * CPT;
@@ -780,17 +915,18 @@ __device__ __forceinline__ void phase_density(const Phys &P, int mm2, double mtk
 constexpr int kR2nWarps = 16;
 constexpr int kStage = 15;   // ddx0 ddx1 ddy0 ddy1 ddz0 ddz1 vnu mro mcp*mro mkt mht mbb mtk mrr wxx
 
+template <bool EX>
 __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int *coff, Grid Gg, NodeF F, Phys P,
                                                               TileGeo T, double timestep, double *stage)
 {
     extern __shared__ double sm[];
     double *sacc = sm;                                   // [NACC][NBOX]
     double *stg = sm + NACC * NBOX;                      // [kR2nWarps][32][kStage]
-    double *shg = stg + kR2nWarps * 32 * kStage;         // grid lines
-    int *scode = (int *)(shg + Gg.nx + Gg.ny + Gg.nz);   // [kR2nWarps][32] per-marker corner masks
+    int *scode = (int *)(stg + kR2nWarps * 32 * kStage);   // [kR2nWarps][32] per-marker corner masks
+    double *shg = (double *)(scode + kR2nWarps * 32);      // grid lines (and the fast tables)
     for (int q = threadIdx.x; q < NACC * NBOX; q += blockDim.x) sacc[q] = 0;
     Grid G;
-    load_grid(Gg, shg, G);   // contains __syncthreads
+    load_grid<EX>(Gg, shg, G);   // contains __syncthreads
     const int tile = blockIdx.x;
     const int ty = tile % T.nty, rest = tile / T.nty, tx = rest % T.ntx, tz = rest / T.ntx;
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
@@ -825,7 +961,7 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
                     if (ok && P.densimod >= 2) { atomicOr(P.err, ERR_DENSI); ok = false; }
                     if (ok) {
                         int wn[3];
-                        const double mpb = pr_at(G, F.pr, F.NY, F.NXY, fx, fy, fz, wn) * 1e-5;
+                        const double mpb = pr_at<EX>(G, F.pr, F.NY, F.NXY, fx, fy, fz, wn) * 1e-5;
                         const double mtk = M.k[i];
                         double mnu = M.v[i];
                         if (mnu <= 0 || timestep <= 0) {
@@ -850,14 +986,26 @@ __global__ void __launch_bounds__(32 * kR2nWarps) k_r2n_cells(Marks M, const int
                             if (fy > P.vdeep && mnu > P.nudeep) mnu = P.nudeep;
                             if (fy < 5e+4 && fx > G.xsize - 1e+4 && fz > 1.5e+5 && fz < 8.7e+5 && mnu > 1e+19) mnu = 1e+19;
                             const int m10 = wn[0], m20 = wn[1], m30 = wn[2];
-                            const double dx = G.gx[m10 + 1] - G.gx[m10], dy = G.gy[m20 + 1] - G.gy[m20], dz = G.gz[m30 + 1] - G.gz[m30];
                             double *st = my + lane * kStage;
-                            st[0] = 1.0 - fabs((G.gx[m10] - fx) / dx);
-                            st[1] = 1.0 - fabs((G.gx[m10 + 1] - fx) / dx);
-                            st[2] = 1.0 - fabs((G.gy[m20] - fy) / dy);
-                            st[3] = 1.0 - fabs((G.gy[m20 + 1] - fy) / dy);
-                            st[4] = 1.0 - fabs((G.gz[m30] - fz) / dz);
-                            st[5] = 1.0 - fabs((G.gz[m30 + 1] - fz) / dz);
+                            if (EX) {
+                                const double dx = G.gx[m10 + 1] - G.gx[m10], dy = G.gy[m20 + 1] - G.gy[m20], dz = G.gz[m30 + 1] - G.gz[m30];
+                                st[0] = 1.0 - fabs((G.gx[m10] - fx) / dx);
+                                st[1] = 1.0 - fabs((G.gx[m10 + 1] - fx) / dx);
+                                st[2] = 1.0 - fabs((G.gy[m20] - fy) / dy);
+                                st[3] = 1.0 - fabs((G.gy[m20 + 1] - fy) / dy);
+                                st[4] = 1.0 - fabs((G.gz[m30] - fz) / dz);
+                                st[5] = 1.0 - fabs((G.gz[m30 + 1] - fz) / dz);
+                            } else {
+                                // the marker lies inside its cell: 1 - |g_i - x| / d is the
+                                // distance to the other node over d (exact zeros on nodes)
+                                const double rx = G.rl[0][m10], ry = G.rl[1][m20], rz = G.rl[2][m30];
+                                st[0] = (G.gx[m10 + 1] - fx) * rx;
+                                st[1] = (fx - G.gx[m10]) * rx;
+                                st[2] = (G.gy[m20 + 1] - fy) * ry;
+                                st[3] = (fy - G.gy[m20]) * ry;
+                                st[4] = (G.gz[m30 + 1] - fz) * rz;
+                                st[5] = (fz - G.gz[m30]) * rz;
+                            }
                             st[6] = vm == 0 ? mnu : vm == 1 ? log(mnu) : 1.0 / mnu;
                             st[7] = mro;
                             st[8] = mcp * mro;
@@ -949,18 +1097,30 @@ __device__ __forceinline__ void box_range(int v, int TT, int nt, int &t0, int &t
 struct TkF { const float *tk0, *tk1, *tk, *tk2, *kt, *ro, *cp; long NY, NXY; };
 
 // tkcalc1 (mark3mg.c:2844-2910): cell, spacings, 8 weights and the 4 interpolated T arrays
+// wi[0..7] corner weights; wi[8..10] the cell's spacings (EX) or their reciprocals (fast)
+template <bool EX>
 __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, double y, double z, double *e, int *wn,
                                       long *nodes, double *wi)
 {
     const int m10 = wn[0] = locate(G.gx, G.nx, x, G.ux), m20 = wn[1] = locate(G.gy, G.ny, y, G.uy), m30 = wn[2] = locate(G.gz, G.nz, z, G.uz);
-    const double dx = wi[8] = G.gx[m10 + 1] - G.gx[m10];
-    const double dy = wi[9] = G.gy[m20 + 1] - G.gy[m20];
-    const double dz = wi[10] = G.gz[m30 + 1] - G.gz[m30];
     e[0] = e[1] = e[2] = e[3] = 0;
-    // per-axis weights 1 - |g - x| / d of the two cell nodes (one division each)
-    const double wz[2] = {1.0 - fabs((G.gz[m30] - z) / dz), 1.0 - fabs((G.gz[m30 + 1] - z) / dz)};
-    const double wx[2] = {1.0 - fabs((G.gx[m10] - x) / dx), 1.0 - fabs((G.gx[m10 + 1] - x) / dx)};
-    const double wy[2] = {1.0 - fabs((G.gy[m20] - y) / dy), 1.0 - fabs((G.gy[m20 + 1] - y) / dy)};
+    // per-axis weights 1 - |g - x| / d of the two cell nodes (one division each, or one product
+    // with the reciprocal spacing)
+    double wz[2], wx[2], wy[2];
+    if (EX) {
+        const double dx = wi[8] = G.gx[m10 + 1] - G.gx[m10];
+        const double dy = wi[9] = G.gy[m20 + 1] - G.gy[m20];
+        const double dz = wi[10] = G.gz[m30 + 1] - G.gz[m30];
+        wz[0] = 1.0 - fabs((G.gz[m30] - z) / dz); wz[1] = 1.0 - fabs((G.gz[m30 + 1] - z) / dz);
+        wx[0] = 1.0 - fabs((G.gx[m10] - x) / dx); wx[1] = 1.0 - fabs((G.gx[m10 + 1] - x) / dx);
+        wy[0] = 1.0 - fabs((G.gy[m20] - y) / dy); wy[1] = 1.0 - fabs((G.gy[m20 + 1] - y) / dy);
+    } else {
+        // markers inside their cell: distance to the other node over the spacing
+        const double rx = wi[8] = G.rl[0][m10], ry = wi[9] = G.rl[1][m20], rz = wi[10] = G.rl[2][m30];
+        wz[0] = (G.gz[m30 + 1] - z) * rz; wz[1] = (z - G.gz[m30]) * rz;
+        wx[0] = (G.gx[m10 + 1] - x) * rx; wx[1] = (x - G.gx[m10]) * rx;
+        wy[0] = (G.gy[m20 + 1] - y) * ry; wy[1] = (y - G.gy[m20]) * ry;
+    }
     int q = 0;
 #pragma unroll
     for (int k3 = 0; k3 < 2; k3++) {
@@ -983,7 +1143,7 @@ __device__ __forceinline__ void tk_at(const Grid &G, const TkF &T, double x, dou
 // change; stage 2 sums them per node (lane = 2 * node + quantity) without atomics.
 constexpr int kHmStage = 9;   // wi[0..7], dtk1
 
-template <int MINB>
+template <bool EX, int MINB>
 __global__ void __launch_bounds__(32 * kR2nWarps, MINB) k_heat_mark_cells(Marks M, const int *coff, Grid Gg, TkF T, TileGeo TG,
                                                                     double timestep, double heatdif, double zdeep,
                                                                     double tdeep, double *stage)
@@ -994,7 +1154,7 @@ __global__ void __launch_bounds__(32 * kR2nWarps, MINB) k_heat_mark_cells(Marks 
     double *shg = stg + kR2nWarps * 32 * kHmStage;
     for (int q = threadIdx.x; q < 2 * NBOX; q += blockDim.x) sm[q] = 0;
     Grid G;
-    load_grid(Gg, shg, G);
+    load_grid<EX>(Gg, shg, G);
     const int tile = blockIdx.x;
     const int ty = tile % TG.nty, rest = tile / TG.nty, tx = rest % TG.ntx, tz = rest / TG.ntx;
     const int cx0 = tx * TX, cy0 = ty * TY, cz0 = tz * TZ;
@@ -1019,7 +1179,7 @@ __global__ void __launch_bounds__(32 * kR2nWarps, MINB) k_heat_mark_cells(Marks 
                     double e[4], wi[11];
                     int wn[3];
                     long nodes[8];
-                    tk_at(G, T, fx, fy, fz, e, wn, nodes, wi);
+                    tk_at<EX>(G, T, fx, fy, fz, e, wn, nodes, wi);
                     float mk = M.k[i];
                     if (mk <= 0) {
                         mk = (float)e[3];
@@ -1036,7 +1196,9 @@ __global__ void __launch_bounds__(32 * kR2nWarps, MINB) k_heat_mark_cells(Marks 
                             (mk + e[2] - e[3]) > mtk)
                             mk = (float)(mtk - e[2] + e[3]);
                         const double dtk = e[3] - (double)mk;
-                        double dtk1 = -heatdif * mkt / rocp * 2.0 * (1.0 / wi[8] / wi[8] + 1.0 / wi[9] / wi[9] + 1.0 / wi[10] / wi[10]) * timestep;
+                        const double sum_h2 = EX ? 1.0 / wi[8] / wi[8] + 1.0 / wi[9] / wi[9] + 1.0 / wi[10] / wi[10]
+                                                 : wi[8] * wi[8] + wi[9] * wi[9] + wi[10] * wi[10];
+                        double dtk1 = -heatdif * mkt / rocp * 2.0 * sum_h2 * timestep;
                         if (dtk1 < -150.0) dtk1 = -150.0;
                         dtk1 = dtk * (1.0 - exp(dtk1));
                         mk = __fadd_rn(mk, (float)dtk1);
@@ -1094,17 +1256,18 @@ __global__ void k_heat_mark_gather(const double *stage, TileGeo TG, int nx, int 
 }
 
 // antidiffusion: marker T -= interpolated mean node change (heat3mg.c:722-779)
+template <bool EX>
 __global__ void k_heat_mark_anti(Marks M, const int *off, int ntiles, Grid Gg, TkF T, const double *acc, long N)
 {
     extern __shared__ double shg[];
     Grid G;
-    load_grid(Gg, shg, G);
+    load_grid<EX>(Gg, shg, G);
     const long n = off[ntiles];
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         double e[4], wi[11];
         int wn[3];
         long nodes[8];
-        tk_at(G, T, M.x[i], M.y[i], M.z[i], e, wn, nodes, wi);
+        tk_at<EX>(G, T, M.x[i], M.y[i], M.z[i], e, wn, nodes, wi);
         double iv = 0;
         for (int q = 0; q < 8; q++) iv -= acc[N + nodes[q]] * wi[q];
         M.k[i] = __fadd_rn(M.k[i], (float)iv);
@@ -1341,29 +1504,74 @@ static Phys phys_of(i3g_ctx *c)
     return P;
 }
 
-static size_t grid_smem(i3g_ctx *c) { return sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
+// grid lines plus the fast arithmetic's three tables per axis (load_grid)
+static size_t grid_smem(i3g_ctx *c) { return 4 * sizeof(double) * (c->m.xnumx + c->m.ynumy + c->m.znumz); }
+
+// the marker kernels' arithmetic: the reference's operation order (marker_exact) or the fast one
+static bool mexact(i3g_ctx *c) { return c->p.marker_exact != 0; }
+
+template <bool EX>
+static void launch_move_t(i3g_ctx *c, unsigned grid, const Marks &M, long n, const Grid &G, const NodeF &F, const Phys &P,
+                          double dt)
+{
+    switch (ms(c)->move_minb) {
+    case 3: LAUNCH((k_move<EX, 3>), grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    case 4: LAUNCH((k_move<EX, 4>), grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    default: LAUNCH((k_move<EX, 2>), grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
+    }
+}
 
 static void launch_move(i3g_ctx *c, unsigned grid, const Marks &M, long n, const Grid &G, const NodeF &F, const Phys &P,
                         double dt)
 {
-    switch (ms(c)->move_minb) {
-    case 3: LAUNCH(k_move<3>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
-    case 4: LAUNCH(k_move<4>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
-    default: LAUNCH(k_move<2>, grid, 256, grid_smem(c), M, n, G, F, P, dt); break;
-    }
+    if (mexact(c)) launch_move_t<true>(c, grid, M, n, G, F, P, dt);
+    else launch_move_t<false>(c, grid, M, n, G, F, P, dt);
 }
 
+// resident k_move CTAs per SM (the same for both arithmetic variants: both are capped at the
+// same register count by __launch_bounds__)
 static int move_occupancy(i3g_ctx *c, int *per_sm)
 {
     switch (ms(c)->move_minb) {
-    case 3: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<3>, 256, grid_smem(c))); break;
-    case 4: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<4>, 256, grid_smem(c))); break;
-    default: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<2>, 256, grid_smem(c))); break;
+    case 3: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<false, 3>, 256, grid_smem(c))); break;
+    case 4: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<false, 4>, 256, grid_smem(c))); break;
+    default: I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_move<false, 2>, 256, grid_smem(c))); break;
     }
     return 0;
 }
+
+static void launch_r2n(i3g_ctx *c, const Marks &M, const int *coff, const TileGeo &T, double timestep, double *stage);
+static void launch_heat_mark(i3g_ctx *c, const Marks &M, const int *coff, const TkF &TK, const TileGeo &T, double timestep,
+                             double *stage);
 static size_t r2n_smem(i3g_ctx *c) { return sizeof(double) * (NACC * NBOX + kR2nWarps * 32 * kStage) + grid_smem(c) + sizeof(int) * kR2nWarps * 32; }
 static size_t heat_mark_smem(i3g_ctx *c) { return sizeof(double) * (2 * NBOX + kR2nWarps * 32 * kHmStage) + grid_smem(c); }
+
+static void launch_r2n(i3g_ctx *c, const Marks &M, const int *coff, const TileGeo &T, double timestep, double *stage)
+{
+    if (mexact(c))
+        LAUNCH(k_r2n_cells<true>, ms(c)->ntiles, 32 * kR2nWarps, r2n_smem(c), M, coff, grid_of(c), nodes_of(c), phys_of(c), T,
+               timestep, stage);
+    else
+        LAUNCH(k_r2n_cells<false>, ms(c)->ntiles, 32 * kR2nWarps, r2n_smem(c), M, coff, grid_of(c), nodes_of(c), phys_of(c), T,
+               timestep, stage);
+}
+
+static void launch_heat_mark(i3g_ctx *c, const Marks &M, const int *coff, const TkF &TK, const TileGeo &T, double timestep,
+                             double *stage)
+{
+    MarkerState *S = ms(c);
+    const int nt = S->ntiles;
+    const size_t sm = heat_mark_smem(c);
+    const Grid G = grid_of(c);
+    const double hd = c->p.heatdif, zd = c->p.zdeep, td = c->p.tdeep;
+    if (mexact(c)) {
+        if (S->heat_minb == 2) LAUNCH((k_heat_mark_cells<true, 2>), nt, 32 * kR2nWarps, sm, M, coff, G, TK, T, timestep, hd, zd, td, stage);
+        else LAUNCH((k_heat_mark_cells<true, 1>), nt, 32 * kR2nWarps, sm, M, coff, G, TK, T, timestep, hd, zd, td, stage);
+    } else {
+        if (S->heat_minb == 2) LAUNCH((k_heat_mark_cells<false, 2>), nt, 32 * kR2nWarps, sm, M, coff, G, TK, T, timestep, hd, zd, td, stage);
+        else LAUNCH((k_heat_mark_cells<false, 1>), nt, 32 * kR2nWarps, sm, M, coff, G, TK, T, timestep, hd, zd, td, stage);
+    }
+}
 
 int markers_alloc(i3g_ctx *c)
 {
@@ -1429,12 +1637,20 @@ int markers_alloc(i3g_ctx *c)
         S->move_blocks = (unsigned)std::max(1, sms * std::max(per_sm, 1));
         int a = 0, b = 0;
         I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tile_key, 256, grid_smem(c)));
-        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_heat_mark_anti, 256, grid_smem(c)));
+        I3G_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_heat_mark_anti<false>, 256, grid_smem(c)));
         S->key_blocks = (unsigned)std::max(1, sms * std::max(std::min(a, b), 1));
     }
-    I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
-    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
-    I3G_CUDA(cudaFuncSetAttribute(k_heat_mark_cells<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_r2n_cells<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r2n_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute((k_heat_mark_cells<true, 1>), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute((k_heat_mark_cells<true, 2>), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute((k_heat_mark_cells<false, 1>), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute((k_heat_mark_cells<false, 2>), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heat_mark_smem(c)));
+    for (auto f : {k_move<true, 2>, k_move<true, 3>, k_move<true, 4>, k_move<false, 2>, k_move<false, 3>, k_move<false, 4>})
+        I3G_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem(c)));
+    for (auto f : {k_heat_mark_anti<true>, k_heat_mark_anti<false>})
+        I3G_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem(c)));
+    I3G_CUDA(cudaFuncSetAttribute(k_tile_key, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grid_smem(c)));
     I3G_CUDA(cudaStreamSynchronize(c->st));
     // upload the host markers
     return markers_upload(c, &c->m);
@@ -1601,8 +1817,7 @@ int markers_to_nodes(i3g_ctx *c, double timestep)
     if (rc) return rc;
     TileGeo T{S->ntx, S->nty, S->ntz, S->ntiles};
     if (S->n)
-        LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff, grid_of(c),
-               nodes_of(c), phys_of(c), T, timestep, S->stage);
+        launch_r2n(c, S->a, (const int *)S->coff, T, timestep, S->stage);
     else
         I3G_CUDA(cudaMemsetAsync(S->stage, 0, sizeof(double) * (size_t)S->ntiles * NACC * NBOX, c->st));
     NodeOut O{c->lev[0].nu, c->nxx, c->nxy, c->nxz, c->nyz, c->ro, c->cp, c->kt, c->ht, c->et, c->tk, c->rr, S->tk1};
@@ -1633,15 +1848,16 @@ int markers_heat_update(i3g_ctx *c, double timestep, const float *tk0, const flo
     }
     TkF T{tk0, tk1, c->tk, tk2, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
     TileGeo TG{S->ntx, S->nty, S->ntz, S->ntiles};
-    if (S->heat_minb == 2) LAUNCH(k_heat_mark_cells<2>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
-           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
-        else LAUNCH(k_heat_mark_cells<1>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
-           T, TG, timestep, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
+    launch_heat_mark(c, S->a, (const int *)S->coff, T, TG, timestep, S->stage);
     if (c->p.heatdif != 0) {
         LAUNCH(k_heat_mark_gather, nb(N), 256, 0, (const double *)S->stage, TG, (int)c->m.xnumx, (int)c->m.ynumy,
                (int)c->m.znumz, S->acc, N);
-        LAUNCH(k_heat_mark_anti, std::min(nb(S->n), S->key_blocks), 256, grid_smem(c), S->a, (const int *)S->off,
-               S->ntiles, grid_of(c), T, (const double *)S->acc, N);
+        if (mexact(c))
+            LAUNCH(k_heat_mark_anti<true>, std::min(nb(S->n), S->key_blocks), 256, grid_smem(c), S->a, (const int *)S->off,
+                   S->ntiles, grid_of(c), T, (const double *)S->acc, N);
+        else
+            LAUNCH(k_heat_mark_anti<false>, std::min(nb(S->n), S->key_blocks), 256, grid_smem(c), S->a, (const int *)S->off,
+                   S->ntiles, grid_of(c), T, (const double *)S->acc, N);
     }
     I3G_CUDA(cudaGetLastError());
     return 0;
@@ -1661,13 +1877,9 @@ int markers_time_kernel(i3g_ctx *c, int kind, int reps, double *ms_out, double *
     TkF TK{c->tk, c->tk, c->tk, c->tk, c->kt, c->ro, c->cp, (long)c->m.ynumy, (long)(c->m.xnumx * c->m.ynumy)};
     auto launch = [&]() -> int {
         if (kind == 4)
-            LAUNCH(k_r2n_cells, S->ntiles, 32 * kR2nWarps, r2n_smem(c), S->a, (const int *)S->coff,
-                   grid_of(c), nodes_of(c), phys_of(c), T, 1.0, S->stage);
+            launch_r2n(c, S->a, (const int *)S->coff, T, 1.0, S->stage);
         else if (kind == 9)
-            if (S->heat_minb == 2) LAUNCH(k_heat_mark_cells<2>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
-                   TK, T, 1e10, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
-        else LAUNCH(k_heat_mark_cells<1>, S->ntiles, 32 * kR2nWarps, heat_mark_smem(c), S->a, (const int *)S->coff, grid_of(c),
-                   TK, T, 1e10, c->p.heatdif, c->p.zdeep, c->p.tdeep, S->stage);
+            launch_heat_mark(c, S->a, (const int *)S->coff, TK, T, 1e10, S->stage);
         else
             launch_move(c, std::min(nb(n), S->move_blocks), S->a, n, grid_of(c), nodes_of(c), phys_of(c), 0.0);
         return 0;

@@ -110,6 +110,12 @@ typedef struct i3g_params {
                                          * the FP32 V-cycle on the scaled correction system; precision 0:
                                          * the FP64 V-cycle); 0: one V-cycle per iteration, the
                                          * reference's iteration (with FP64 defect correction for 1) */
+    int32_t marker_exact;               /* marker kernels (movemark, ronurecalc, marker temperatures):
+                                         * 1: the reference's operation order (divisions, separate
+                                         * multiply and add), marker positions bit-identical to the
+                                         * reference's; 0: reciprocal spacings and fused multiply-adds,
+                                         * interpolated values within ~1e-16 relative of those, FP32
+                                         * positions equal except within ~1e-13 m of a rounding boundary */
 } i3g_params;
 
 /* ---- per output file row (load3mg.c:25-58, applied at i3mg.c:64-77) ---------------- */
