@@ -268,8 +268,9 @@ def main():
     ap.add_argument("--workload", default="incl129", choices=tuple(WORKLOADS))
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--sweeps", default=None, help="relaxation sweeps per level, 'down,../up,..'")
-    ap.add_argument("--warm", type=int, default=2, choices=(1, 2),
-                    help="mixed precision: 1 previous step's solution, 2 linear extrapolation from the last two")
+    ap.add_argument("--warm", type=int, default=3, choices=(1, 2, 3),
+                    help="mixed precision: 1 previous step's solution, 2 linear extrapolation from the last two, "
+                         "3 quadratic extrapolation from the last three")
     ap.add_argument("--krylov", type=int, default=8,
                     help="mixed precision: FGMRES restart length around the FP32 V-cycle (0: plain defect correction)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -331,8 +332,8 @@ def main():
         logs.append(runtime.time_step(ctx, mode, f, args.warmup + i, nc))
         st = ctx.stats()
         cycles.append(st["stokes_cycles"])
-        logs[-1].update({k: st[k] for k in ("stokes_cycles", "stokes_rel", "ms_stokes", "ms_heat", "ms_move", "ms_r2n",
-                                            "heat_cycles")})
+        logs[-1].update({k: st[k] for k in ("stokes_cycles", "stokes_rel", "stokes_rel0", "stokes_start", "ms_stokes",
+                                            "ms_heat", "ms_move", "ms_r2n", "heat_cycles")})
     ms = ctx.timer_stop()
     barrier()
     clk = clocks.stop()
@@ -430,7 +431,8 @@ def main():
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
                    "stokes_maxcyc": args.maxcyc, "allow_noconv": bool(nc)},
         "timestep_s": float(np.median([lg["timestep"] for lg in logs])),
-        "stokes_cycles": cycles[args.warmup:], "stokes_rel": [lg["stokes_rel"] for lg in logs], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in
+        "stokes_cycles": cycles[args.warmup:], "stokes_rel": [lg["stokes_rel"] for lg in logs],
+        "stokes_rel0": [lg["stokes_rel0"] for lg in logs], "stokes_start": [lg["stokes_start"] for lg in logs], "phases_ms": {k: float(np.mean([lg[k] for lg in logs])) for k in
                                                            ("ms_stokes", "ms_heat", "ms_move", "ms_r2n")},
         "gpu_launches": int(launches),
         "fp64_multigrid": fp64_mg,

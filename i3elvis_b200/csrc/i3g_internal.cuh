@@ -186,10 +186,11 @@ struct i3g_ctx {
     int coop_blocks = 0;                        // its grid: every CTA resident at once (0: no cooperative launch)
     unsigned *dbar = nullptr;                   // its grid barrier: arrival count, generation
     int *dbar_err = nullptr;                    // set when a grid barrier wait timed out
-    double *hist[2][4] = {};                    // last two converged level-0 solutions (warm_start 2)
+    double *hist[3][4] = {};                    // last three converged level-0 solutions, newest last
+                                                // (warm_start 2 and 3)
     int hist_check = 0;                         // an upload is being compared with the last solution
     int *dflag = nullptr, *hflag = nullptr;     // its result: device flag and pinned host mirror
-    double hist_dt[2] = {0, 0};                 // time steps taken after them
+    double hist_dt[3] = {0, 0, 0};              // time steps taken after them
     int nhist = 0;
     // staged start for the next Stokes solve (i3g_unet_predict); kept only when its relative
     // residual is below the default start's

@@ -1520,7 +1520,7 @@ void stokes_free(i3g_ctx *c)
     c->dbar_err = nullptr;
     stokes_graph_free(c);
     kry_free(c);
-    for (int h = 0; h < 2; h++)
+    for (int h = 0; h < 3; h++)
         for (int v = 0; v < 4; v++) { cudaFree(c->hist[h][v]); c->hist[h][v] = nullptr; }
     for (int l = 0; l < c->nlev; l++) {
         Level &L = c->lev[l];
@@ -1983,7 +1983,7 @@ __global__ void k_same_solution(View<double> L, long pin, double pinit, const do
 int stokes_upload_check(i3g_ctx *c)
 {
     c->hist_check = 0;
-    if (c->nhist == 0 || !c->hist[1][0]) { c->nhist = 0; return 0; }
+    if (c->nhist == 0 || !c->hist[2][0]) { c->nhist = 0; return 0; }
     if (!c->dflag) {
         I3G_CUDA(cudaMalloc((void **)&c->dflag, sizeof(int)));
         I3G_CUDA(cudaMallocHost((void **)&c->hflag, sizeof(int)));
@@ -1992,7 +1992,7 @@ int stokes_upload_check(i3g_ctx *c)
     const long pin = ((long)c->m.pzinit * L0.nx + c->m.pxinit) * L0.ny + c->m.pyinit;
     I3G_CUDA(cudaMemsetAsync(c->dflag, 0, sizeof(int), c->st));
     k_same_solution<<<std::min<long>(nblk(L0.n), 4L * 148), 256, 0, c->st>>>(
-        view<double>(L0, L0.d), pin, c->m.pinit, c->hist[1][0], c->hist[1][1], c->hist[1][2], c->hist[1][3], c->pr,
+        view<double>(L0, L0.d), pin, c->m.pinit, c->hist[2][0], c->hist[2][1], c->hist[2][2], c->hist[2][3], c->pr,
         c->vx, c->vy, c->vz, c->dflag);
     c->launches++;
     I3G_CUDA(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -2231,43 +2231,65 @@ __global__ void k_kr_store(long N, double *z, const float *e0, const float *e1, 
     z[t] = sp * (double)e0[t]; z[N + t] = sv * (double)e1[t]; z[2 * N + t] = sv * (double)e2[t]; z[3 * N + t] = sv * (double)e3[t];
 }
 
-// w = -D w  (the residual kernels leave -A z in w)
-__global__ void k_kr_negscale(long N, double *w, const double *d)
+// One classical Gram-Schmidt pass over the 4N-vector w and the basis v_0..v_{NV-1}, per element
+//   MODE 0: x = w;
+//   MODE 1: x = -d w with the stopping test's row weight of the element's component (pressure
+//           rows d[1], velocity rows d[0]), stored back into w (the residual -A z becomes D A z);
+//   MODE 2: x = w - sum_i h_i v_i, stored back into w (the first projection removed);
+// and the block partial sums of x . v_i (i < NV) and x . x (slot NV).  A grid of a few CTAs per
+// SM with two elements in flight per thread keeps HBM busy; the basis is read once per pass.
+constexpr int kKrBlocks = 4 * 148;
+template <int NV, int MODE>
+__global__ void __launch_bounds__(256) k_kr_proj(double *__restrict__ w, const double *__restrict__ V, long N, long n4,
+                                                 const double *__restrict__ h, const double *__restrict__ d,
+                                                 double *__restrict__ part)
 {
     pdl_enter();
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N) return;
-    const double dv = d[0], dp = d[1];
-    w[t] *= -dp; w[N + t] *= -dv; w[2 * N + t] *= -dv; w[3 * N + t] *= -dv;
-}
-
-// partial sums of w . v_i (i < nv) and, in slot nv, w . w
-__global__ void __launch_bounds__(256) k_kr_dots(const double *w, const double *V, int nv, long n4, double *part)
-{
-    pdl_enter();
-    __shared__ double sh[kKryNq][8];
-    double q[kKryNq], qq = 0;
+    __shared__ double sh[NV + 1][8];
+    double q[NV + 1];
 #pragma unroll
-    for (int i = 0; i < kKryNq; i++) q[i] = 0;
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += (long)gridDim.x * blockDim.x) {
-        const double x = w[t];
+    for (int i = 0; i <= NV; i++) q[i] = 0;
+    double hh[NV > 0 ? NV : 1];
 #pragma unroll
-        for (int i = 0; i < kKryNq - 1; i++)
-            if (i < nv) q[i] += x * V[i * n4 + t];
-        qq += x * x;
+    for (int i = 0; i < NV; i++) hh[i] = MODE == 2 ? h[i] : 0.0;
+    const double dp = MODE == 1 ? -d[1] : 0.0, dv = MODE == 1 ? -d[0] : 0.0;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x; t0 < n4; t0 += 2 * stride) {
+        double x[2], v[2][NV > 0 ? NV : 1];
+        bool in[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const long t = t0 + u * stride;
+            in[u] = t < n4;
+            x[u] = in[u] ? w[t] : 0.0;
+#pragma unroll
+            for (int i = 0; i < NV; i++) v[u][i] = in[u] ? __ldg(V + i * n4 + t) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const long t = t0 + u * stride;
+            double y = x[u];
+            if (MODE == 1) y *= t < N ? dp : dv;
+            if (MODE == 2)
+#pragma unroll
+                for (int i = 0; i < NV; i++) y -= hh[i] * v[u][i];
+            if (MODE != 0 && in[u]) w[t] = y;
+#pragma unroll
+            for (int i = 0; i < NV; i++) q[i] += y * v[u][i];
+            q[NV] += y * y;
+        }
     }
     const int wi = threadIdx.x >> 5, ln = threadIdx.x & 31;
 #pragma unroll
-    for (int i = 0; i < kKryNq; i++) {
-        if (i > nv) break;
-        const double v = warp_sum(i == nv ? qq : q[i]);
-        if (ln == 0) sh[i][wi] = v;
+    for (int i = 0; i <= NV; i++) {
+        const double r = warp_sum(q[i]);
+        if (ln == 0) sh[i][wi] = r;
     }
     __syncthreads();
-    if ((int)threadIdx.x <= nv) {
-        double v = 0;
-        for (int a = 0; a < 8; a++) v += sh[threadIdx.x][a];
-        part[(long)blockIdx.x * kKryNq + threadIdx.x] = v;
+    if ((int)threadIdx.x <= NV) {
+        double r = 0;
+        for (int a = 0; a < 8; a++) r += sh[threadIdx.x][a];
+        part[(long)blockIdx.x * kKryNq + threadIdx.x] = r;
     }
 }
 
@@ -2282,16 +2304,6 @@ __global__ void k_kr_dot_final(const double *part, int nblk, int nq, double *out
     if (ln == 0) out[qi] = v;
 }
 
-// w -= sum_i h_i v_i
-__global__ void k_kr_axpy(double *w, const double *V, int nv, long n4, const double *h)
-{
-    pdl_enter();
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n4) return;
-    double x = w[t];
-    for (int i = 0; i < nv; i++) x -= h[i] * V[i * n4 + t];
-    w[t] = x;
-}
 
 // v = (w - sum_i h_i v_i) / |.|, the squared norm taken as w.w - sum_i h_i^2 (hw[nv] = w.w from
 // the projection pass; v_0..v_{nv-1} are orthonormal)
@@ -2341,6 +2353,16 @@ __global__ void k_extrapolate(long n, double *u, const double *a, const double *
     u[t] = a[t] + r * (a[t] - b[t]);
 }
 
+// u = wa a + wb b + wc c: the next solution predicted from the last three
+__global__ void k_extrapolate3(long n, double *u, const double *a, const double *b, const double *cc, double wa, double wb,
+                               double wc)
+{
+    pdl_enter();
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    u[t] = wa * a[t] + wb * b[t] + wc * cc[t];
+}
+
 // Row-weighted dots of a staged start's residual change dr = r0 - r (r0: the default start's
 // residual, r = L.r: the staged start's) over the rows of the stopping test: out[0] += <r0, dr>,
 // out[1] += <dr, dr>, weight wm on non-boundary velocity rows and wc on pressure rows.
@@ -2372,6 +2394,30 @@ __global__ void __launch_bounds__(256) k_guess_dots(View<double> L, const double
     }
 }
 
+// k_kr_proj<nv, mode> for a run-time basis size nv <= kKryMax
+template <int MODE>
+static void kr_proj_launch(i3g_ctx *c, int nv, double *w, const double *V, long N, long n4, const double *h, const double *d,
+                           double *part)
+{
+    switch (nv) {
+#define KR_CASE(k) case k: LAUNCH((k_kr_proj<k, MODE>), kKrBlocks, 256, w, V, N, n4, h, d, part); break;
+    KR_CASE(0) KR_CASE(1) KR_CASE(2) KR_CASE(3) KR_CASE(4) KR_CASE(5) KR_CASE(6) KR_CASE(7) KR_CASE(8)
+    KR_CASE(9) KR_CASE(10) KR_CASE(11) KR_CASE(12) KR_CASE(13) KR_CASE(14) KR_CASE(15) KR_CASE(16)
+#undef KR_CASE
+    default: break;
+    }
+}
+
+static int kr_proj(i3g_ctx *c, int nv, int mode, double *w, long N, long n4, const double *h, const double *d, double *part)
+{
+    if (nv < 0 || nv > kKryMax) return set_error(c, I3G_E_ARG, "Krylov basis of %d vectors above %d", nv, kKryMax);
+    const double *V = kry(c)->V;
+    if (mode == 0) kr_proj_launch<0>(c, nv, w, V, N, n4, h, d, part);
+    else if (mode == 1) kr_proj_launch<1>(c, nv, w, V, N, n4, h, d, part);
+    else kr_proj_launch<2>(c, nv, w, V, N, n4, h, d, part);
+    return 0;
+}
+
 static int kry_alloc(i3g_ctx *c, int m)
 {
     KrylovState *K = kry(c);
@@ -2386,7 +2432,7 @@ static int kry_alloc(i3g_ctx *c, int m)
     ALLOC(K->Z, double, m * n4);
     ALLOC(K->W, double, n4);
     ALLOC(K->F0, double, n4);
-    ALLOC(K->part, double, (long)c->red_blocks * kKryNq);
+    ALLOC(K->part, double, (long)kKrBlocks * kKryNq);
     ALLOC(K->hdev, double, 3 * kKryNq + 2);
     if (c->p.precision == 0) ALLOC(K->save, double, 2 * n4);
     I3G_CUDA(cudaMallocHost((void **)&K->hhost, (3 * kKryNq + 2) * sizeof(double)));
@@ -2477,15 +2523,14 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
                             (const int *)B.ocomp, (const double *)B.ok);
         }
     }
-    LAUNCH(k_kr_negscale, nblk(N), 256, N, K->W, d);
-    // classical Gram-Schmidt, twice; the second projection's pass also yields w.w, from which the
-    // last kernel forms the norm while it subtracts the projection and normalises
+    // classical Gram-Schmidt, twice: the first pass also applies the row weights (w = D A z), the
+    // second subtracts the first projection while it forms the second one and w.w, from which the
+    // last kernel takes the norm while it subtracts the second projection and normalises
     double *h1 = K->hdev, *h2 = K->hdev + kKryNq;
-    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
-    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h1);
-    LAUNCH(k_kr_axpy, nblk(n4), 256, K->W, (const double *)K->V, j + 1, n4, (const double *)h1);
-    LAUNCH(k_kr_dots, nb, 256, (const double *)K->W, (const double *)K->V, j + 1, n4, K->part);
-    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, nb, j + 2, h2);
+    if (int rc = kr_proj(c, j + 1, 1, K->W, N, n4, nullptr, d, K->part)) return rc;
+    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, kKrBlocks, j + 2, h1);
+    if (int rc = kr_proj(c, j + 1, 2, K->W, N, n4, h1, d, K->part)) return rc;
+    LAUNCH(k_kr_dot_final, 1, 32 * (j + 2), (const double *)K->part, kKrBlocks, j + 2, h2);
     LAUNCH(k_kr_axpy_normalize, nblk(n4), 256, K->V + (long)(j + 1) * n4, (const double *)K->W, (const double *)K->V,
            j + 1, n4, (const double *)h2);
     I3G_CUDA(cudaMemcpyAsync(K->hhost, K->hdev, 2 * kKryNq * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -2538,8 +2583,8 @@ static int kry_cycle(i3g_ctx *c, int multinum, double rtol, int maxsteps, int *s
     LAUNCH(k_kr_from_r, nblk(N), 256, N, (const double *)L0.d.r[0], (const double *)L0.d.r[1],
            (const double *)L0.d.r[2], (const double *)L0.d.r[3], K->V, d);
     double *nrm = K->hdev + 2 * kKryNq;
-    LAUNCH(k_kr_dots, c->red_blocks, 256, (const double *)K->V, (const double *)K->V, 0, n4, K->part);
-    LAUNCH(k_kr_dot_final, 1, 32, (const double *)K->part, c->red_blocks, 1, nrm);
+    if (int rc = kr_proj(c, 0, 0, K->V, N, n4, nullptr, d, K->part)) return rc;
+    LAUNCH(k_kr_dot_final, 1, 32, (const double *)K->part, kKrBlocks, 1, nrm);
     I3G_CUDA(cudaMemcpyAsync(K->hhost + 2 * kKryNq, nrm, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     LAUNCH(k_kr_normalize, nblk(n4), 256, n4, (const double *)K->V, K->V, (const double *)nrm);
     I3G_CUDA(cudaStreamSynchronize(c->st));
@@ -2609,13 +2654,25 @@ int stokes_solve(i3g_ctx *c, double *timestep)
         c->hist_check = 0;
     }
     c->st_.stokes_start = 0;
-    if (c->p.warm_start == 2 && c->nhist == 2 && c->hist_dt[0] > 0) {
+    if (c->p.warm_start == 3 && c->nhist == 3 && c->hist_dt[0] > 0 && c->hist_dt[1] > 0) {
+        c->st_.stokes_start = 3;
+        // quadratic (Lagrange) extrapolation in time from the last three converged solutions at
+        // t0 < t1 < t2 to t3 = t2 + dt, with h1 = t1 - t0, h2 = t2 - t1, h3 = dt (the step taken
+        // after the newest solution); equal steps give 3 x2 - 3 x1 + x0
+        const double h1 = c->hist_dt[0], h2 = c->hist_dt[1], h3 = c->hist_dt[2];
+        const double w0 = h3 * (h2 + h3) / (h1 * (h1 + h2));
+        const double w1 = -h3 * (h1 + h2 + h3) / (h1 * h2);
+        const double w2 = (h1 + h2 + h3) * (h2 + h3) / ((h1 + h2) * h2);
+        for (int v = 0; v < 4; v++)
+            LAUNCH(k_extrapolate3, nblk(L0.n), 256, L0.n, L0.d.u[v], (const double *)c->hist[2][v],
+                   (const double *)c->hist[1][v], (const double *)c->hist[0][v], w2, w1, w0);
+    } else if (c->p.warm_start >= 2 && c->nhist >= 2 && c->hist_dt[1] > 0) {
         c->st_.stokes_start = 1;
         // linear extrapolation in time from the last two converged solutions
-        const double r = c->hist_dt[1] / c->hist_dt[0];
+        const double r = c->hist_dt[2] / c->hist_dt[1];
         for (int v = 0; v < 4; v++)
-            LAUNCH(k_extrapolate, nblk(L0.n), 256, L0.n, L0.d.u[v], (const double *)c->hist[1][v],
-                   (const double *)c->hist[0][v], r);
+            LAUNCH(k_extrapolate, nblk(L0.n), 256, L0.n, L0.d.u[v], (const double *)c->hist[2][v],
+                   (const double *)c->hist[1][v], r);
     }
     // boundary rows of the initial guess consistent with their partners
     for (int v = 0; v < 4; v++) bc_apply<double>(c, 0, v, true);
@@ -2737,20 +2794,26 @@ int stokes_solve(i3g_ctx *c, double *timestep)
     c->st_.stokes_rel = std::max(mom, cont);
     c->st_.stokes_mom_rel = mom;
     c->st_.stokes_cont_rel = cont;
-    if (c->p.warm_start == 2 && conv) {
-        if (!c->hist[0][0])
-            for (int h = 0; h < 2; h++)
-                for (int v = 0; v < 4; v++) ALLOC(c->hist[h][v], double, L0.n);
+    const bool keep = c->p.warm_start >= 2 && conv;
+    if (keep) {
+        // the oldest slot takes the new solution, which becomes the newest (slot 2)
+        const int nh = c->p.warm_start == 3 ? 3 : 2;
+        for (int h = 3 - nh; h < 3; h++)
+            for (int v = 0; v < 4; v++)
+                if (!c->hist[h][v]) ALLOC(c->hist[h][v], double, L0.n);
         for (int v = 0; v < 4; v++) {
-            std::swap(c->hist[0][v], c->hist[1][v]);
-            I3G_CUDA(cudaMemcpyAsync(c->hist[1][v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
+            double *old = c->hist[3 - nh][v];
+            for (int h = 3 - nh; h < 2; h++) c->hist[h][v] = c->hist[h + 1][v];
+            c->hist[2][v] = old;
+            I3G_CUDA(cudaMemcpyAsync(c->hist[2][v], L0.d.u[v], L0.n * 8, cudaMemcpyDeviceToDevice, c->st));
         }
     }
     if ((rc = finish_solve(c, timestep))) return rc;
-    if (c->p.warm_start == 2 && conv) {
+    if (keep) {
         c->hist_dt[0] = c->hist_dt[1];
-        c->hist_dt[1] = *timestep;
-        c->nhist = std::min(c->nhist + 1, 2);
+        c->hist_dt[1] = c->hist_dt[2];
+        c->hist_dt[2] = *timestep;
+        c->nhist = std::min(c->nhist + 1, c->p.warm_start == 3 ? 3 : 2);
     }
     I3G_CUDA(cudaEventRecord(e1, c->st));
     I3G_CUDA(cudaEventSynchronize(e1));

@@ -104,7 +104,9 @@ typedef struct i3g_params {
                                          * 2: linear extrapolation in time from the last two converged
                                          * solutions (falls back to 1 until two exist; an upload of nodal
                                          * fields whose v, P differ from the last solution as downloaded
-                                         * resets it, an upload of exactly that state keeps it) */
+                                         * resets it, an upload of exactly that state keeps it);
+                                         * 3: quadratic extrapolation from the last three (linear while
+                                         * only two exist), same reset rule */
     int32_t krylov;                     /* > 0: restarted FGMRES(krylov) (<= 16) on the FP64 residual,
                                          * preconditioned by one V-cycle of this precision (precision 1:
                                          * the FP32 V-cycle on the scaled correction system; precision 0:
@@ -141,7 +143,8 @@ typedef struct i3g_stats {
     int32_t stokes_start;               /* start of the last i3g_stokes: 0 the nodal v, P
                                            (uploaded or the last solution), 1 extrapolated
                                            from the last two solutions (warm_start 2), 2 the
-                                           staged guess (i3g_unet_predict)                */
+                                           staged guess (i3g_unet_predict), 3 extrapolated
+                                           from the last three (warm_start 3)              */
 } i3g_stats;
 
 typedef struct i3g_ctx i3g_ctx;

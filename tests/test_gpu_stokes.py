@@ -137,26 +137,32 @@ def test_solve_matches_reference(name, precision, krylov):
     assert 0 < dt < 1e30
 
 
-def test_extrapolated_warm_start_reaches_same_solution():
-    """warm_start 2 (linear extrapolation from the last two solutions) changes only the start of
-    the iteration: after three time steps the state equals the one of warm_start 1 to the
-    solver tolerance, with no more V-cycles."""
+@pytest.mark.parametrize("warm", [2, 3])
+def test_extrapolated_warm_start_reaches_same_solution(warm):
+    """warm_start 2 and 3 (linear / quadratic extrapolation from the last two / three solutions)
+    change only the start of the iteration: after four time steps the state equals the one of
+    warm_start 1 to the solver tolerance, with no more V-cycles, and the start kinds follow the
+    history (previous solution, then linear, then quadratic)."""
     from i3elvis_b200 import runtime
-    sols, cyc = [], []
-    for warm in (1, 2):
+    sols, cyc, starts = [], [], []
+    for w in (1, warm):
         p, mode, fx = golden("sphere17")
-        par = abi.make_params(mode, stokes_rtol=1e-10, stokes_maxcyc=3000, precision=1, krylov=8, warm_start=warm)
+        par = abi.make_params(mode, stokes_rtol=1e-10, stokes_maxcyc=3000, precision=1, krylov=8, warm_start=w)
         g = lib.Context(abi.ModelBuffers(p), par, abi.make_file_params(mode.files[0]))
         f = mode.files[0]
-        c = []
-        for n0 in range(3):
+        c, st = [], []
+        for n0 in range(4):
             runtime.time_step(g, mode, f, n0)
             c.append(g.stats()["stokes_cycles"])
+            st.append(g.stats()["stokes_start"])
         n0 = cases.level_sizes(p, mode.multinum)[0]
         sols.append(g.get(abi.A_SOL, 0, 4 * n0))
         cyc.append(c)
+        starts.append(st)
         g.close()
     a, b = sols[0].reshape(-1, 4), sols[1].reshape(-1, 4)
     for k in (1, 2, 3):
         assert np.linalg.norm(a[:, k] - b[:, k]) <= 1e-6 * np.linalg.norm(a[:, k]), (k, cyc)
-    assert cyc[1][2] <= cyc[0][2] + 2, cyc
+    assert cyc[1][3] <= cyc[0][3] + 2, cyc
+    assert starts[0] == [0, 0, 0, 0], starts
+    assert starts[1] == ([0, 0, 1, 1] if warm == 2 else [0, 0, 1, 3]), starts
