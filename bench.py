@@ -59,8 +59,10 @@ def default_sweeps(mn):
 # Sweeps of the FP32 V-cycle when it preconditions FGMRES: the Krylov iteration removes the slow
 # components, so a lighter cycle (a quarter of the reference's sweeps) reaches the tolerance sooner
 # in time (incl129, previous-step start: 24 V-cycles in 82 ms against 14 in 104 ms with the full
-# sweeps; with the extrapolated start FGMRES(8), (12) and (16) all take 15-17 V-cycles, 51-54 ms).
-MIXED_SWEEPS = {4: "2,4,4,8/2,4,4,8,16", 3: "2,4,4/2,4,4,8", 2: "2,4/2,4,8"}
+# sweeps).  On the coarsest level 4 sweeps do as well as 16 (incl129 with the quadratic start:
+# 13-14 V-cycles either way, Stokes 36.0 -> 30.8 ms per step); one level-0 sweep per leg, or fewer
+# on levels 1-3, costs more V-cycles than it saves.
+MIXED_SWEEPS = {4: "2,4,4,8/2,4,4,8,4", 3: "2,4,4/2,4,4,4", 2: "2,4/2,4,4"}
 
 
 def build_case(name, seed_offset=0, sweeps=None):

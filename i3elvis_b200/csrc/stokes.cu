@@ -12,6 +12,7 @@
 // rows, residuals and relaxation updates agree bit for bit with the CPU oracle.  The FP32
 // path (mixed precision) uses the same stencil code on viscosity and geometry scaled to O(1).
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 #include <utility>
@@ -493,24 +494,41 @@ struct BcDev4 {
     BcDev b[4];
 };
 
+// one component's row of residual_at
+template <typename T, int V>
+__device__ __forceinline__ void residual_row(const View<T> &L, long n)
+{
+    int i, j, k;
+    node_ijk(L, n, i, j, k);
+    if (!row_exists(V, i, j, k, L.nx, L.ny, L.nz) || (L.bc[n] & (1 << V))) return;
+    if (V == 0) { T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); L.r0[n] = s; }
+    if (V == 1) { T s = L.f1[n]; xrow<T, true>(L, i, j, k, n, s); L.r1[n] = s; }
+    if (V == 2) { T s = L.f2[n]; yrow<T, true>(L, i, j, k, n, s); L.r2[n] = s; }
+    if (V == 3) { T s = L.f3[n]; zrow<T, true>(L, i, j, k, n, s); L.r3[n] = s; }
+}
+
+// Residual of all rows, one component per blockIdx.y (a thread computes one row, so four times
+// as many threads as nodes keep enough loads in flight); blocks from rowblocks on take the
+// boundary rows of that component (they write only boundary nodes, which the row threads skip,
+// and read no residual).  Each row uses the same per-row function as residual_at: bit-identical.
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_residual_bc(View<T> L, BcDev4 B, unsigned rowblocks)
+__global__ void __launch_bounds__(256) k_residual_bc(View<T> L, BcDev4 B, unsigned rowblocks)
 {
     pdl_enter();
+    const int v = blockIdx.y;
     if (blockIdx.x >= rowblocks) {
-        int t = (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
-        for (int v = 0; v < 4; v++) {
-            if (t < B.b[v].n) {
-                bc_residual_at<T>(L, v, t, B.b[v].node, B.b[v].onode, B.b[v].ocomp, B.b[v].ok);
-                return;
-            }
-            t -= B.b[v].n;
-        }
+        const int t = (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
+        if (t < B.b[v].n) bc_residual_at<T>(L, v, t, B.b[v].node, B.b[v].onode, B.b[v].ocomp, B.b[v].ok);
         return;
     }
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.nxy * L.nz) return;
-    residual_at<T>(L, n);
+    switch (v) {
+    case 0: residual_row<T, 0>(L, n); break;
+    case 1: residual_row<T, 1>(L, n); break;
+    case 2: residual_row<T, 2>(L, n); break;
+    default: residual_row<T, 3>(L, n); break;
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -578,6 +596,57 @@ __global__ void __launch_bounds__(256) k_restrict(View<T> F, View<T> Cc, TrView 
     restrict_at<T, V>(F, Cc, tx, ty, tz, n);
 }
 
+// FP32 restriction with four lanes per coarse row (the FP32 V-cycle's restriction): lane q of a
+// group sums the fine contributors of the z-entries gptr[k] + q, + q + 4, ..., the group's partial
+// sums and weights are added by two shuffles, and the pressure rows' 1 / nd_coarse is applied once
+// to the sum instead of to every term.  A coarse row gathers up to 4 x 4 x 4 contributors, so one
+// thread per row is a long chain of dependent loads; four shorten it and fill small levels.  The
+// FP32 sums come out in a different order than the FP64 restriction's (which follows the
+// reference's scatter order bit for bit); the FP32 V-cycle is a preconditioner only.
+template <int V>
+__device__ __forceinline__ void restrict_split_at(const View<float> &F, const View<float> &Cc, const TrView &tx,
+                                                  const TrView &ty, const TrView &tz, long n, int q, bool live)
+{
+    int i = 0, j = 0, k = 0;
+    float sum = 0.f, ws = 0.f;
+    bool row = false;
+    const float *fr = V == 0 ? F.r0 : V == 1 ? F.r1 : V == 2 ? F.r2 : F.r3;
+    if (live) {
+        node_ijk(Cc, n, i, j, k);
+        row = row_exists(V, i, j, k, Cc.nx, Cc.ny, Cc.nz) && !(Cc.bc[n] & (1 << V));
+        if (row) {
+            for (int ez = tz.gptr[k] + q; ez < tz.gptr[k + 1]; ez += 4) {
+                const int fk = tz.gf[ez];
+                const float wz = (float)tz.gw[ez];
+                for (int ex = tx.gptr[i]; ex < tx.gptr[i + 1]; ex++) {
+                    const int fi = tx.gf[ex];
+                    const float wx = (float)tx.gw[ex];
+                    for (int ey = ty.gptr[j]; ey < ty.gptr[j + 1]; ey++) {
+                        const int fj = ty.gf[ey];
+                        if (!row_exists(V, fi, fj, fk, F.nx, F.ny, F.nz)) continue;
+                        const long m = (long)fk * F.nxy + (long)fi * F.ny + fj;
+                        if (F.bc[m] & (1 << V)) continue;
+                        const float swt = wx * (float)ty.gw[ey] * wz;
+                        sum += (V == 0 ? fr[m] * F.nd[m] : fr[m]) * swt;
+                        ws += swt;
+                    }
+                }
+            }
+        }
+    }
+    sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+    ws += __shfl_xor_sync(0xffffffffu, ws, 1);
+    sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+    ws += __shfl_xor_sync(0xffffffffu, ws, 2);
+    if (!live || q != 0) return;
+    float *cu = V == 0 ? Cc.u0 : V == 1 ? Cc.u1 : V == 2 ? Cc.u2 : Cc.u3;
+    float *cf_ = V == 0 ? Cc.f0 : V == 1 ? Cc.f1 : V == 2 ? Cc.f2 : Cc.f3;
+    cu[n] = 0.f;
+    if (!row) { cf_[n] = 0.f; return; }
+    if (V == 0) sum /= Cc.nd[n];
+    cf_[n] = ws != 0.f ? sum / ws : sum;
+}
+
 // vpprolong (move3mg.c:2748-3063): fine += sum_8 coarse * weight * koef
 template <typename T, int V>
 __device__ __forceinline__ void prolong_at(const View<T> &F, const View<T> &Cc, const TrView &tx, const TrView &ty,
@@ -630,6 +699,22 @@ __global__ void __launch_bounds__(256) k_restrict4(View<T> F, View<T> Cc, Tr4 R)
     case 1: restrict_at<T, 1>(F, Cc, R.t[1][0], R.t[1][1], R.t[1][2], n); break;
     case 2: restrict_at<T, 2>(F, Cc, R.t[2][0], R.t[2][1], R.t[2][2], n); break;
     default: restrict_at<T, 3>(F, Cc, R.t[3][0], R.t[3][1], R.t[3][2], n); break;
+    }
+}
+
+// four components (blockIdx.y), four lanes per coarse row
+__global__ void __launch_bounds__(256) k_restrict4_f32(View<float> F, View<float> Cc, Tr4 R)
+{
+    pdl_enter();
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long n = t >> 2;
+    const int q = (int)(t & 3);
+    const bool live = n < Cc.nxy * Cc.nz;
+    switch (blockIdx.y) {
+    case 0: restrict_split_at<0>(F, Cc, R.t[0][0], R.t[0][1], R.t[0][2], n, q, live); break;
+    case 1: restrict_split_at<1>(F, Cc, R.t[1][0], R.t[1][1], R.t[1][2], n, q, live); break;
+    case 2: restrict_split_at<2>(F, Cc, R.t[2][0], R.t[2][1], R.t[2][2], n, q, live); break;
+    default: restrict_split_at<3>(F, Cc, R.t[3][0], R.t[3][1], R.t[3][2], n, q, live); break;
     }
 }
 
@@ -1632,9 +1717,9 @@ static void residual_t(i3g_ctx *c, int l)
     if (c->fuse) {
         BcDev4 B;
         long nb = 0;
-        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L.bcl[v]); nb += L.bcl[v].n; }
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L.bcl[v]); nb = std::max(nb, (long)L.bcl[v].n); }
         const unsigned rows = nblk(L.n);
-        LAUNCH(k_residual_bc<T>, rows + nblk(nb), 256, V, B, rows);
+        LAUNCH(k_residual_bc<T>, dim3(rows + nblk(nb), 4), 256, V, B, rows);
         return;
     }
     LAUNCH(k_residual<T>, nblk(L.n), 256, V);
@@ -1697,7 +1782,10 @@ static void restrict_t(i3g_ctx *c, int l)
         Tr4 R;
         for (int v = 0; v < 4; v++)
             for (int ax = 0; ax < 3; ax++) R.t[v][ax] = trview(F.tr[ax][kStag[v][ax]]);
-        LAUNCH(k_restrict4<T>, dim3(nblk(Cc.n), 4), 256, VF, VC, R);
+        if constexpr (std::is_same<T, float>::value)
+            LAUNCH(k_restrict4_f32, dim3(nblk(4 * Cc.n), 4), 256, VF, VC, R);
+        else
+            LAUNCH(k_restrict4<T>, dim3(nblk(Cc.n), 4), 256, VF, VC, R);
         return;
     }
 #define RST(V_) LAUNCH((k_restrict<T, V_>), nblk(Cc.n), 256, VF, VC, trview(F.tr[0][kStag[V_][0]]), \
@@ -2513,8 +2601,8 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
     if (c->fuse) {
         BcDev4 B;
         long nb = 0;
-        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L0.bcl[v]); nb += L0.bcl[v].n; }
-        LAUNCH(k_residual_bc<double>, nblk(N) + nblk(nb), 256, Vz, B, nblk(N));
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L0.bcl[v]); nb = std::max(nb, (long)L0.bcl[v].n); }
+        LAUNCH(k_residual_bc<double>, dim3(nblk(N) + nblk(nb), 4), 256, Vz, B, nblk(N));
     } else {
         LAUNCH(k_residual<double>, nblk(N), 256, Vz);
         for (int v = 0; v < 4; v++) {
