@@ -379,6 +379,225 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a)
 }
 
 // ---------------------------------------------------------------------------------------
+// brick-staged tcgen05 convolution (CIN, COUT in {16, 32}: the layers of levels 0 and 1)
+// ---------------------------------------------------------------------------------------
+// k_conv_tc fetches every tap's 128-row operand from L2 (27 shifted copies of the input per
+// output tile) and waits on each fetch.  Here a persistent CTA keeps all 27 taps' weights in
+// shared memory and walks over output tiles of 2 x 8 x 8 nodes (z, x, y): it loads the tile's
+// input brick with its one-node halo (4 x 10 x 10 rows) once, then for every tap gathers the
+// shifted 128-row operand from the brick into one of two aligned operand buffers (the canonical
+// no-swizzle K-major layout) while the tensor core runs the previous tap's MMA.  One thread
+// issues the MMAs (M = 128, N = COUT, K = 16) into the CTA's TMEM accumulator; tcgen05.commit
+// arrives on the operand buffer's mbarrier, which the gather of the tap after next waits for.
+// The epilogue is k_conv_tc's (bias, skip add, ReLU or the backward ReLU mask, BF16 or FP32
+// stores of the interior rows).
+constexpr int kBz = 2, kBx = 8, kBy = 8;                    // output tile (z, x, y): 128 rows
+constexpr int kHz = kBz + 2, kHx = kBx + 2, kHy = kBy + 2;   // input brick with halo
+constexpr int kBrickRows = kHz * kHx * kHy;
+constexpr int kTapsPerStage = 3;                            // the three dy taps of one (dz, dx)
+
+template <int CIN, int COUT>
+struct BrickShape {
+    static constexpr int CH = CIN / 8;                         // 16-byte channel chunks per row
+    static constexpr int ABYTES = kTileM * CIN * 2;            // one tap's A operand
+    static constexpr int TAPB = COUT * CIN * 2;                // one tap's B operand
+    static constexpr int WBYTES = 27 * TAPB;
+    static constexpr int BRICK = kBrickRows * CIN * 2;
+    static constexpr int NST = CIN == 16 ? 3 : 2;              // stages (of three tap operands) in flight
+    // brick rows hold their 16-byte chunks XOR-swizzled: chunk j of row r sits in slot
+    // j ^ ((r >> SWS) & (CH - 1)), so that the eight consecutive rows a quarter-warp gathers fall
+    // in distinct banks (rows 4 apart (CIN 16) or 2 apart (CIN 32) would otherwise collide)
+    static constexpr int SWS = CIN == 16 ? 2 : 1;
+    static __device__ __forceinline__ int slot(int r, int j) { return r * CH + (j ^ ((r >> SWS) & (CH - 1))); }
+    static constexpr int STB = kTapsPerStage * ABYTES;
+    static constexpr int SMEM = 1024 + NST * STB + WBYTES + BRICK;
+    static constexpr uint32_t NCOL = COUT < 32 ? 32 : COUT;
+    static constexpr uint32_t IDESC = ConvShape<CIN, COUT>::IDESC;
+    static_assert((CIN == 16 || CIN == 32) && (COUT == 16 || COUT == 32), "brick kernel channel counts");
+    static_assert(TAPB % 512 == 0 && ABYTES % 1024 == 0, "operand alignment");
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_conv_brick(ConvArgs a, int ntx, int nty, int ntiles)
+{
+    using S = BrickShape<CIN, COUT>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar[S::NST];
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // operand buffers and weights at 1024-byte boundaries (tensor-core operand alignment)
+    const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
+    const uint32_t sA0 = sbase, sW = sbase + S::NST * S::STB, sBrick = sW + S::WBYTES;
+    uint8_t *const gbase = smem + (sbase - smem_u32(smem));
+    const uint8_t *const brick = gbase + S::NST * S::STB + S::WBYTES;
+    uint8_t *const abuf = gbase;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(S::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S::NST; s++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // all taps' weights, once per CTA: tap t, output channel n, chunk j at t*TAPB + j*(COUT*16) + n*16
+    for (int q = tid; q < 27 * COUT * S::CH; q += 128) {
+        const int t = q / (COUT * S::CH), rem = q - t * (COUT * S::CH);
+        const int n = rem / S::CH, j = rem - n * S::CH;
+        cp_async16(sW + (uint32_t)(t * S::TAPB + j * (COUT * 16) + n * 16), a.w + ((long)t * COUT + n) * CIN + j * 8, 16);
+    }
+    const long XY = (long)a.d.X * a.d.Y;
+    // input brick of a tile: padded rows (z0-1 .. z0+2, x0-1 .. x0+8, y0-1 .. y0+8), zero outside
+    auto tile_origin = [&](int tile, int &z0, int &x0, int &y0) {
+        const int ty = tile % nty, r2 = tile / nty, tx = r2 % ntx, tz = r2 / ntx;
+        z0 = 1 + kBz * tz; x0 = 1 + kBx * tx; y0 = 1 + kBy * ty;
+    };
+    auto load_brick = [&](int tile) {
+        int z0, x0, y0;
+        tile_origin(tile, z0, x0, y0);
+        for (int q = tid; q < kBrickRows * S::CH; q += 128) {
+            const int br = q / S::CH, j = q - br * S::CH;
+            const int bz = br / (kHx * kHy), bxy = br - bz * (kHx * kHy), bx = bxy / kHy, by = bxy - bx * kHy;
+            const int zz = z0 - 1 + bz, xx = x0 - 1 + bx, yy = y0 - 1 + by;
+            const bool ok = zz < a.d.Z && xx < a.d.X && yy < a.d.Y;
+            const long src = ok ? (long)zz * XY + (long)xx * a.d.Y + yy : 0;
+            cp_async16(sBrick + (uint32_t)(S::slot(br, j) * 16), a.in + src * CIN + j * 8, ok ? 16 : 0);
+        }
+    };
+    if ((int)blockIdx.x < ntiles) load_brick(blockIdx.x);
+    cp_async_commit();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    long g = 0;             // stages issued by this CTA so far (buffer g % NST, its commit number g / NST)
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        int z0, x0, y0;
+        tile_origin(tile, z0, x0, y0);
+        cp_async_wait<0>();   // this tile's brick (and, the first time, the weights)
+        __syncthreads();
+        // output row r = tid: tile-local (tz, tx, ty) = (r >> 6, (r >> 3) & 7, r & 7)
+        const int oz = tid >> 6, ox = (tid >> 3) & 7, oy = tid & 7;
+        // stage st = (dz, dx) gathers and multiplies the three taps dy = 0, 1, 2
+        for (int st = 0; st < 9; st++, g++) {
+            const int b = (int)(g % S::NST);
+            int fail = 0;
+            // the buffer was last read by the MMAs of stage g - NST
+            if (g >= S::NST && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)((g / S::NST - 1) & 1))) fail = 1;
+            const int dz = st / 3, dx = st % 3;
+            const int br0 = ((oz + dz) * kHx + (ox + dx)) * kHy + oy;
+            uint8_t *dst = abuf + b * S::STB + tid * 16;
+            if (!fail) {
+#pragma unroll
+                for (int dy = 0; dy < kTapsPerStage; dy++)
+#pragma unroll
+                    for (int j = 0; j < S::CH; j++)
+                        *reinterpret_cast<uint4 *>(dst + dy * S::ABYTES + j * (kTileM * 16)) =
+                            *reinterpret_cast<const uint4 *>(brick + S::slot(br0 + dy, j) * 16);
+            }
+            fence_proxy_async();   // the gathered operands to the tensor core's (async) proxy
+            if (__syncthreads_or(fail)) { failed = true; break; }
+            if (tid == 0) {
+                tc_fence_after();
+#pragma unroll
+                for (int dy = 0; dy < kTapsPerStage; dy++) {
+                    const int tap = st * 3 + dy;   // = dz * 9 + dx * 3 + dy
+                    const uint32_t sA = sA0 + (uint32_t)(b * S::STB + dy * S::ABYTES), sB = sW + (uint32_t)(tap * S::TAPB);
+#pragma unroll
+                    for (int k = 0; k < CIN / 16; k++) {
+                        const uint64_t da = smem_desc(sA + (uint32_t)(2 * k * kTileM * 16), kTileM * 16, 128);
+                        const uint64_t db = smem_desc(sB + (uint32_t)(2 * k * COUT * 16), COUT * 16, 128);
+                        tc_mma(tmem, da, db, S::IDESC, (tap > 0 || k > 0) ? 1u : 0u);
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&mbar[b]))
+                             : "memory");
+            }
+        }
+        if (failed) break;
+        // every gather of this tile is done: the next tile's brick loads while the epilogue runs
+        if (tile + (int)gridDim.x < ntiles) load_brick(tile + gridDim.x);
+        cp_async_commit();
+        // the last commit arrives once every MMA of this tile completed
+        const long gl = g - 1;
+        int fail = 0;
+        if (!mbar_wait(smem_u32(&mbar[gl % S::NST]), (uint32_t)((gl / S::NST) & 1))) fail = 1;
+        if (__syncthreads_or(fail)) { failed = true; break; }
+        tc_fence_after();
+        const int zz = z0 + oz, xx = x0 + ox, yy = y0 + oy;
+        const bool valid = zz <= a.d.nz && xx <= a.d.nx && yy <= a.d.ny;
+        const long p = (long)zz * XY + (long)xx * a.d.Y + yy;
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            float v[16];
+            tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);   // whole warp
+            if (!valid) continue;
+            if (a.bias) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) v[q] += a.bias[c0 + q];
+            }
+            if (a.add) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float f[8];
+                    unpack8(*reinterpret_cast<const uint4 *>(a.add + p * COUT + c0 + 8 * h), f);
+#pragma unroll
+                    for (int q = 0; q < 8; q++) v[8 * h + q] += f[q];
+                }
+            }
+            if (a.relu) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) v[q] = fmaxf(v[q], 0.0f);
+            }
+            if (a.mask) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float f[8];
+                    unpack8(*reinterpret_cast<const uint4 *>(a.mask + p * COUT + c0 + 8 * h), f);
+#pragma unroll
+                    for (int q = 0; q < 8; q++) v[8 * h + q] = f[q] > 0.0f ? v[8 * h + q] : 0.0f;
+                }
+            }
+            if (a.out) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float f[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) f[q] = v[8 * h + q];
+                    *reinterpret_cast<uint4 *>(a.out + p * COUT + c0 + 8 * h) = pack8(f);
+                }
+            }
+            if (a.out32) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4)
+                    *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0 + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+            }
+        }
+        // TMEM reads done before the next tile's first MMA overwrites the accumulator; brick and
+        // operand buffers free for the next tile
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (failed) {
+        // No more epilogues.  MMAs committed before the timeout may still write TMEM and read the
+        // operand buffers: one more bounded wait on the last commit before the columns are released.
+        if (tid == 0) {
+            atomicExch(a.err, 1);
+            if (g > 0) mbar_wait(smem_u32(&mbar[(g - 1) % S::NST]), (uint32_t)(((g - 1) / S::NST) & 1));
+        }
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::NCOL) : "memory");
+}
+
+// ---------------------------------------------------------------------------------------
 // weight and bias gradients (FP32, CUDA cores)
 // dW[tap][co][ci] += sum_rows G[row][co] * X[row + off_tap][ci];  db[co] += sum_rows G[row][co]
 // ---------------------------------------------------------------------------------------
@@ -748,8 +967,46 @@ cudaError_t launch_conv_t(const ConvArgs &a, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// persistent grid of the brick kernel: every resident CTA on every SM, at most one per tile
+template <int CIN, int COUT>
+cudaError_t launch_brick_t(const ConvArgs &a, cudaStream_t st)
+{
+    using S = BrickShape<CIN, COUT>;
+    static int per_sm = 0, sms = 0;
+    if (!per_sm) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv_brick<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+        if (e != cudaSuccess) return e;
+        // the whole unified L1 as shared memory, so that several CTAs fit on an SM
+        e = cudaFuncSetAttribute(k_conv_brick<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        // resident CTAs per SM from the shared-memory footprint (each CTA also holds NCOL <= 32 of
+        // the 512 TMEM columns and 128 threads of at most 64 registers, neither of which binds)
+        int smem_sm = 0;
+        if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+        per_sm = std::max(1, std::min(8, smem_sm / (S::SMEM + 1024 + 64)));
+    }
+    const int ntx = (a.d.nx + kBx - 1) / kBx, nty = (a.d.ny + kBy - 1) / kBy, ntz = (a.d.nz + kBz - 1) / kBz;
+    const int ntiles = ntx * nty * ntz;
+    const int grid = std::min(ntiles, sms * per_sm);
+    if (grid < 1) return cudaSuccess;
+    k_conv_brick<CIN, COUT><<<grid, 128, S::SMEM, st>>>(a, ntx, nty, ntiles);
+    return cudaGetLastError();
+}
+
+// The brick kernel takes the layers with 16 or 32 channels in and out (the fine levels, most of
+// the network's time); k_conv_tc the wider ones.  I3G_CONV_BRICK=0 sends every layer to k_conv_tc.
 cudaError_t launch_conv(int cin, int cout, const ConvArgs &a, cudaStream_t st)
 {
+    static const bool brick = !getenv("I3G_CONV_BRICK") || atoi(getenv("I3G_CONV_BRICK")) != 0;
+    if (brick) {
+#define I3G_BRICK_CASE(I, O) \
+        if (cin == I && cout == O) return launch_brick_t<I, O>(a, st);
+        I3G_BRICK_CASE(16, 16) I3G_BRICK_CASE(16, 32) I3G_BRICK_CASE(32, 16) I3G_BRICK_CASE(32, 32)
+#undef I3G_BRICK_CASE
+    }
 #define I3G_CONV_CASE(I, O) \
     if (cin == I && cout == O) return launch_conv_t<I, O>(a, st);
     I3G_CONV_CASE(16, 16) I3G_CONV_CASE(16, 32) I3G_CONV_CASE(32, 16) I3G_CONV_CASE(32, 32) I3G_CONV_CASE(32, 64)
