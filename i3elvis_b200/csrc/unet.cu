@@ -598,6 +598,180 @@ __global__ void __launch_bounds__(128) k_conv_brick(ConvArgs a, int ntx, int nty
 }
 
 // ---------------------------------------------------------------------------------------
+// weight gradients on tcgen05 (CIN, COUT in {16, 32})
+// ---------------------------------------------------------------------------------------
+// dW[tap][co][ci] = sum over rows of X[row + off_tap][ci] * G[row][co]: per tap a GEMM whose K
+// dimension is the grid's rows.  A persistent CTA walks over the same 2 x 8 x 8 output tiles as
+// k_conv_brick: it loads the tile's input brick and the tile's 128 rows of G, gathers the shifted
+// tap operands from the brick into chunk planes ([channel chunk][row][16 B], as the forward
+// gather does), and multiplies them with the tensor core in MN-major form: M = the 128 rows
+// (tap, ci) of a group of 128 / CIN taps, N = COUT, K = 16 rows per MMA, eight MMAs per tile and
+// group.  Every group accumulates in its own TMEM columns over all the CTA's tiles; at the end
+// each CTA adds its sums to dW (FP32 atomics, one per weight per CTA).
+template <int CIN, int COUT>
+struct WgradShape {
+    static constexpr int CH = CIN / 8, CHO = COUT / 8;
+    static constexpr int TPG = kTileM / CIN;                        // taps per group: M = 128
+    static constexpr int NG = (27 + TPG - 1) / TPG;                 // groups
+    static constexpr int ABYTES = kTileM * CIN * 2;                 // one tap's operand (chunk planes)
+    static constexpr int GRPB = TPG * ABYTES;                       // one group's operands = 32 KB
+    static constexpr int GBYTES = kTileM * COUT * 2;                // the tile's rows of G
+    static constexpr int BRICK = kBrickRows * CIN * 2;
+    static constexpr int SMEM = 1024 + 2 * GRPB + GBYTES + BRICK;
+    static constexpr uint32_t NCOLS = NG * COUT;                    // accumulator columns in use
+    static constexpr uint32_t NCOL = NCOLS <= 32 ? 32 : NCOLS <= 64 ? 64 : NCOLS <= 128 ? 128 : 256;
+    // kind::f16, D FP32, A and B BF16, both MN-major (bits 15, 16), N = COUT, M = 128
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                      ((uint32_t)(COUT >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+    static constexpr int SWS = CIN == 16 ? 2 : 1;
+    static __device__ __forceinline__ int slot(int r, int j) { return r * CH + (j ^ ((r >> SWS) & (CH - 1))); }
+    static_assert((CIN == 16 || CIN == 32) && (COUT == 16 || COUT == 32), "tcgen05 weight-gradient channel counts");
+    static_assert(GRPB % 1024 == 0 && GBYTES % 1024 == 0, "operand alignment");
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *X, const bf16 *G, float *part, Dims d, int ntx, int nty,
+                                                  int ntiles, int *err)
+{
+    using S = WgradShape<CIN, COUT>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
+    const uint32_t sG = sbase + 2 * S::GRPB, sBrick = sG + S::GBYTES;
+    uint8_t *const gbase = smem + (sbase - smem_u32(smem));
+    const uint8_t *const brick = gbase + 2 * S::GRPB + S::GBYTES;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(S::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < 2; s++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long XY = (long)d.X * d.Y;
+    const int oz = tid >> 6, ox = (tid >> 3) & 7, oy = tid & 7;   // this thread's row of the tile
+    long g = 0;               // groups issued (buffer g & 1, its commit number g >> 1)
+    bool failed = false, first = true;
+    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        const int ty = tile % nty, r2 = tile / nty, tx = r2 % ntx, tz = r2 / ntx;
+        const int z0 = 1 + kBz * tz, x0 = 1 + kBx * tx, y0 = 1 + kBy * ty;
+        // the previous tile's MMAs read G and the group buffers: all of them done before the loads
+        int fail0 = 0;
+        if (g > 0 && !mbar_wait(smem_u32(&mbar[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail0 = 1;
+        if (__syncthreads_or(fail0)) { failed = true; break; }
+        for (int q = tid; q < kBrickRows * S::CH; q += 128) {
+            const int br = q / S::CH, j = q - br * S::CH;
+            const int bz = br / (kHx * kHy), bxy = br - bz * (kHx * kHy), bx = bxy / kHy, by = bxy - bx * kHy;
+            const int zz = z0 - 1 + bz, xx = x0 - 1 + bx, yy = y0 - 1 + by;
+            const bool ok = zz < d.Z && xx < d.X && yy < d.Y;
+            const long src = ok ? (long)zz * XY + (long)xx * d.Y + yy : 0;
+            cp_async16(sBrick + (uint32_t)(S::slot(br, j) * 16), X + src * CIN + j * 8, ok ? 16 : 0);
+        }
+        {
+            // G rows of the tile (zero outside the interior: rows beyond the array are not loaded)
+            const int zz = z0 + oz, xx = x0 + ox, yy = y0 + oy;
+            const bool ok = zz <= d.nz && xx <= d.nx && yy <= d.ny;
+            const long p = ok ? (long)zz * XY + (long)xx * d.Y + yy : 0;
+#pragma unroll
+            for (int j = 0; j < S::CHO; j++) cp_async16(sG + (uint32_t)(j * (kTileM * 16) + tid * 16), G + p * COUT + j * 8, ok ? 16 : 0);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int gi = 0; gi < S::NG; gi++, g++) {
+            const int b = (int)(g & 1);
+            int fail = 0;
+            if (g >= 2 && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)(((g - 2) >> 1) & 1))) fail = 1;
+            if (!fail) {
+                uint8_t *dst = gbase + b * S::GRPB + tid * 16;
+#pragma unroll
+                for (int tl = 0; tl < S::TPG; tl++) {
+                    const int tap = gi * S::TPG + tl;
+                    if (tap < 27) {
+                        const int dz = tap / 9, dx = (tap / 3) % 3, dy = tap % 3;
+                        const int br = ((oz + dz) * kHx + (ox + dx)) * kHy + (oy + dy);
+#pragma unroll
+                        for (int j = 0; j < S::CH; j++)
+                            *reinterpret_cast<uint4 *>(dst + tl * S::ABYTES + j * (kTileM * 16)) =
+                                *reinterpret_cast<const uint4 *>(brick + S::slot(br, j) * 16);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < S::CH; j++)
+                            *reinterpret_cast<uint4 *>(dst + tl * S::ABYTES + j * (kTileM * 16)) = make_uint4(0, 0, 0, 0);
+                    }
+                }
+            }
+            fence_proxy_async();
+            if (__syncthreads_or(fail)) { failed = true; break; }
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t sA = sbase + (uint32_t)(b * S::GRPB);
+                // MN-major, no swizzle: the leading byte offset is the stride between core matrices
+                // along K (8-row groups, 128 B apart), the stride byte offset the one along M or N
+                // (channel chunks, 2048 B apart)
+#pragma unroll
+                for (int kk = 0; kk < kTileM / 16; kk++) {
+                    const uint64_t da = smem_desc(sA + (uint32_t)(kk * 256), 128, kTileM * 16);
+                    const uint64_t db = smem_desc(sG + (uint32_t)(kk * 256), 128, kTileM * 16);
+                    tc_mma(tmem + (uint32_t)(gi * COUT), da, db, S::IDESC, (first && kk == 0) ? 0u : 1u);
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&mbar[b]))
+                             : "memory");
+            }
+        }
+        first = false;
+    }
+    int fail = 0;
+    if (g > 0 && !mbar_wait(smem_u32(&mbar[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+    failed = __syncthreads_or(fail || failed) != 0;
+    if (failed) {
+        if (tid == 0) atomicExch(err, 1);
+    } else if (g > 0) {
+        // this CTA's sums to its slot of the partial buffer (k_wgrad_reduce adds the slots):
+        // TMEM lane m = (tap within the group, ci); column gi * COUT + co
+        float *dW = part + (long)blockIdx.x * 27 * COUT * CIN;
+        tc_fence_after();
+        const int m = warp * 32 + lane, tl = m / CIN, ci = m % CIN;
+#pragma unroll
+        for (int gi = 0; gi < S::NG; gi++) {
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float v[16];
+                tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(gi * COUT + c0), v);   // whole warp
+                const int tap = gi * S::TPG + tl;
+                if (tap < 27) {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) dW[((long)tap * COUT + c0 + q) * CIN + ci] = v[q];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::NCOL) : "memory");
+}
+
+// dW[i] += sum over the CTAs' partial sums part[c][i]
+__global__ void k_wgrad_reduce(const float *part, int nparts, int n, float *dW)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.0f;
+    for (int c = 0; c < nparts; c++) s += part[(long)c * n + i];
+    dW[i] += s;
+}
+
+// ---------------------------------------------------------------------------------------
 // weight and bias gradients (FP32, CUDA cores)
 // dW[tap][co][ci] += sum_rows G[row][co] * X[row + off_tap][ci];  db[co] += sum_rows G[row][co]
 // ---------------------------------------------------------------------------------------
@@ -1032,14 +1206,59 @@ void launch_wgrad_t(const bf16 *X, const bf16 *G, float *dW, float *db, const Di
     k_bgrad<COUT><<<(unsigned)bb, 256, 0, st>>>(G, db, d.np);
 }
 
-void launch_wgrad(int cin, int cout, const bf16 *X, const bf16 *G, float *dW, float *db, const Dims &d, const Offs &o,
-                  cudaStream_t st)
+// resident k_wgrad_tc CTAs per SM: the shared-memory footprint decides (at most 2, so that the
+// TMEM columns of one SM's CTAs stay within 512)
+constexpr int kWgradPerSm = 2;
+
+template <int CIN, int COUT>
+cudaError_t launch_wgrad_tc_t(const bf16 *X, const bf16 *G, float *dW, float *db, const Dims &d, float *part, int slots,
+                              int *err, cudaStream_t st)
 {
+    using S = WgradShape<CIN, COUT>;
+    static int per_sm = 0, sms = 0;
+    if (!per_sm) {
+        cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
+            return e;
+        int dev = 0, smem_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+        per_sm = std::max(1, std::min(kWgradPerSm, smem_sm / (S::SMEM + 1024 + 64)));
+    }
+    const int ntx = (d.nx + kBx - 1) / kBx, nty = (d.ny + kBy - 1) / kBy, ntz = (d.nz + kBz - 1) / kBz;
+    const int ntiles = ntx * nty * ntz;
+    const int grid = std::min(std::min(ntiles, sms * per_sm), slots);
+    if (grid >= 1) {
+        k_wgrad_tc<CIN, COUT><<<grid, 128, S::SMEM, st>>>(X, G, part, d, ntx, nty, ntiles, err);
+        const int n = 27 * COUT * CIN;
+        k_wgrad_reduce<<<(n + 255) / 256, 256, 0, st>>>(part, grid, n, dW);
+    }
+    const long bb = (d.np + 255) / 256 < 1184 ? (d.np + 255) / 256 : 1184;
+    k_bgrad<COUT><<<(unsigned)bb, 256, 0, st>>>(G, db, d.np);
+    return cudaGetLastError();
+}
+
+// Weight and bias gradients of one layer.  The 16/32-channel layers (levels 0 and 1) run on the
+// tensor cores (k_wgrad_tc, partial sums per CTA in part[slots][27 * 32 * 32]); the wider ones, or
+// all with I3G_WGRAD_TC=0, on the CUDA cores (k_wgrad).
+cudaError_t launch_wgrad(int cin, int cout, const bf16 *X, const bf16 *G, float *dW, float *db, const Dims &d, const Offs &o,
+                         float *part, int slots, int *err, cudaStream_t st)
+{
+    static const bool tc = !getenv("I3G_WGRAD_TC") || atoi(getenv("I3G_WGRAD_TC")) != 0;
+    if (tc) {
+#define I3G_WT_CASE(I, O) \
+        if (cin == I && cout == O) return launch_wgrad_tc_t<I, O>(X, G, dW, db, d, part, slots, err, st);
+        I3G_WT_CASE(16, 16) I3G_WT_CASE(16, 32) I3G_WT_CASE(32, 16) I3G_WT_CASE(32, 32)
+#undef I3G_WT_CASE
+    }
 #define I3G_WG_CASE(I, O) \
-    if (cin == I && cout == O) { launch_wgrad_t<I, O>(X, G, dW, db, d, o, st); return; }
+    if (cin == I && cout == O) { launch_wgrad_t<I, O>(X, G, dW, db, d, o, st); return cudaGetLastError(); }
     I3G_WG_CASE(16, 16) I3G_WG_CASE(16, 32) I3G_WG_CASE(32, 32) I3G_WG_CASE(32, 64) I3G_WG_CASE(64, 64)
     I3G_WG_CASE(64, 128) I3G_WG_CASE(128, 128) I3G_WG_CASE(128, 64) I3G_WG_CASE(64, 32) I3G_WG_CASE(32, 16)
 #undef I3G_WG_CASE
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace unet
@@ -1063,6 +1282,8 @@ struct i3g_unet {
     double *pr_prev = nullptr;                  // start pressure of the last captured input
     double *dsum = nullptr;                     // device reductions
     int *derr = nullptr;
+    float *wpart = nullptr;                     // per-CTA weight-gradient sums of k_wgrad_tc
+    int wpart_slots = 0;
     Scales sc = {21.0f, 0.5f, 3300.0f, 0.01f, 1e-10f, 1e6f};
     int adam_t = 0;
 };
@@ -1136,8 +1357,8 @@ int backward(i3g_unet *u)
         const LayerDef &ld = kL[l];
         const int in = ld.in, out = ld.out;
         const Dims &d = u->L[kT[out].lev];
-        launch_wgrad(kT[in].ch, kT[out].ch, u->act[in], u->grd[out], u->grad + u->woff[l], u->grad + u->boff[l], d,
-                     u->off[kT[out].lev], u->st);
+        UCHK(launch_wgrad(kT[in].ch, kT[out].ch, u->act[in], u->grd[out], u->grad + u->woff[l], u->grad + u->boff[l], d,
+                          u->off[kT[out].lev], u->wpart, u->wpart_slots, u->derr, u->st));
         if (l == 0) break;
         ConvArgs a = conv_args(u, kT[out].lev);
         a.in = u->grd[out];
@@ -1273,6 +1494,12 @@ int i3g_unet_create(int nx, int ny, int nz, int capacity, uint64_t seed, i3g_une
     UALLOC(u->pr_prev, double, n0);
     UALLOC(u->dsum, double, 4);
     UALLOC(u->derr, int, 1);
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, u->dev) != cudaSuccess || sms < 1) sms = 148;
+        u->wpart_slots = sms * kWgradPerSm;
+        UALLOC(u->wpart, float, (long)u->wpart_slots * 27 * 32 * 32);
+    }
 #undef UALLOC
     // He initialisation (normal, std sqrt(2 / fan_in)); the output layer starts 100x smaller so
     // that an untrained network leaves the default start almost unchanged
@@ -1322,6 +1549,7 @@ void i3g_unet_destroy(i3g_unet *u)
     cudaFree(u->pr_prev);
     cudaFree(u->dsum);
     cudaFree(u->derr);
+    cudaFree(u->wpart);
     if (u->st) cudaStreamDestroy(u->st);
     delete u;
 }
@@ -1529,6 +1757,63 @@ int i3g_unet_predict(i3g_unet *u, i3g_ctx *c)
 // Single convolution through the tensor-core kernel on host data (BF16 bit patterns):
 // in [np][cin], w [27][cout][cin], bias [cout] or null, add [np][cout] or null; out [np][cout]
 // FP32 (rows outside the interior are left at zero).  Padded grid of nz+2 x nx+2 x ny+2 rows.
+// Weight and bias gradients of one convolution layer on host data (BF16 bit patterns): x the
+// layer's input [np][cin], g the gradient of its output [np][cout] (zero on the halo rows); dw
+// [27][cout][cin] and db [cout] FP32, overwritten.  Padded grid of nz+2 x nx+2 x ny+2 rows.
+int i3g_unet_wgrad_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *x, const uint16_t *g, float *dw,
+                        float *db)
+{
+    if (!x || !g || !dw || !db || nx < 1 || ny < 1 || nz < 1) return set_global_error(I3G_E_ARG, "wgrad: bad argument");
+    const Dims d = make_dims(nz, nx, ny);
+    Offs o;
+    tap_offsets(d, o.off);
+    bf16 *dx = nullptr, *dg = nullptr;
+    float *ddw = nullptr, *ddb = nullptr, *part = nullptr;
+    int *derr = nullptr;
+    cudaStream_t st = nullptr;
+    auto done = [&](int r) {
+        if (st) cudaStreamSynchronize(st);
+        cudaFree(dx);
+        cudaFree(dg);
+        cudaFree(ddw);
+        cudaFree(ddb);
+        cudaFree(part);
+        cudaFree(derr);
+        if (st) cudaStreamDestroy(st);
+        return r;
+    };
+#define CCHK(call)                                          \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return done(fail_cuda(e_, #call)); \
+    } while (0)
+    int dev = 0, sms = 0;
+    CCHK(cudaGetDevice(&dev));
+    CCHK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int slots = std::max(1, sms) * kWgradPerSm;
+    const long nw = 27L * cin * cout;
+    CCHK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CCHK(cudaMalloc((void **)&dx, d.np * cin * 2));
+    CCHK(cudaMalloc((void **)&dg, d.np * cout * 2));
+    CCHK(cudaMalloc((void **)&ddw, nw * 4));
+    CCHK(cudaMalloc((void **)&ddb, cout * 4));
+    CCHK(cudaMalloc((void **)&part, (long)slots * 27 * 32 * 32 * 4));
+    CCHK(cudaMalloc((void **)&derr, 4));
+    CCHK(cudaMemsetAsync(derr, 0, 4, st));
+    CCHK(cudaMemsetAsync(ddw, 0, nw * 4, st));
+    CCHK(cudaMemsetAsync(ddb, 0, cout * 4, st));
+    CCHK(cudaMemcpyAsync(dx, x, d.np * cin * 2, cudaMemcpyHostToDevice, st));
+    CCHK(cudaMemcpyAsync(dg, g, d.np * cout * 2, cudaMemcpyHostToDevice, st));
+    CCHK(launch_wgrad(cin, cout, dx, dg, ddw, ddb, d, o, part, slots, derr, st));
+    CCHK(cudaMemcpyAsync(dw, ddw, nw * 4, cudaMemcpyDeviceToHost, st));
+    CCHK(cudaMemcpyAsync(db, ddb, cout * 4, cudaMemcpyDeviceToHost, st));
+    int h = 0;
+    CCHK(cudaMemcpyAsync(&h, derr, 4, cudaMemcpyDeviceToHost, st));
+    CCHK(cudaStreamSynchronize(st));
+#undef CCHK
+    return done(h ? set_global_error(I3G_E_CUDA, "wgrad: tensor-core stage wait timed out") : 0);
+}
+
 int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *in, const uint16_t *w,
                        const float *bias, const uint16_t *add, int relu, float *out)
 {

@@ -47,6 +47,7 @@ def _bind():
     L.i3g_unet_time_conv.argtypes = [P, C.c_int, C.c_int, dp, dp]
     u16 = C.POINTER(C.c_uint16)
     L.i3g_unet_conv_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, u16, u16, fp, u16, C.c_int, fp]
+    L.i3g_unet_wgrad_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, u16, u16, fp, fp]
     L.i3g_stokes_guess_info.argtypes = [P, ip, dp, dp, dp]
     _bound = True
     return L
@@ -79,6 +80,22 @@ def conv_host(cin, cout, dims, x_bits, w_bits, bias=None, add_bits=None, relu=Fa
                                 None if ad is None else ad.ctypes.data_as(u16), int(relu),
                                 out.ctypes.data_as(C.POINTER(C.c_float))))
     return out
+
+
+def wgrad_host(cin, cout, dims, x_bits, g_bits):
+    """Weight and bias gradients of one layer (``i3g_unet_wgrad_host``): BF16 bit patterns of the
+    input [rows][cin] and of the output gradient [rows][cout] over the padded grid of
+    ``dims = (nz, nx, ny)``; returns dW [27][cout][cin] and db [cout] (FP32)."""
+    L = _bind()
+    nz, nx, ny = dims
+    u16 = C.POINTER(C.c_uint16)
+    x = np.ascontiguousarray(x_bits, np.uint16)
+    g = np.ascontiguousarray(g_bits, np.uint16)
+    dw = np.zeros((27, cout, cin), np.float32)
+    db = np.zeros(cout, np.float32)
+    _check(L.i3g_unet_wgrad_host(cin, cout, nx, ny, nz, x.ctypes.data_as(u16), g.ctypes.data_as(u16),
+                                 dw.ctypes.data_as(C.POINTER(C.c_float)), db.ctypes.data_as(C.POINTER(C.c_float))))
+    return dw, db
 
 
 def guess_info(ctx: lib.Context):

@@ -340,6 +340,13 @@ int i3g_unet_time_conv(i3g_unet *u, int layer, int reps, double *ms, double *byt
  * [rows][cout], interior rows only.  cin, cout in {16, 32, 64, 128} as the network pairs them. */
 int i3g_unet_conv_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *in, const uint16_t *w,
                        const float *bias, const uint16_t *add, int relu, float *out);
+/* Weight and bias gradients of one convolution layer on host BF16 bit patterns over the same
+ * padded grid: x [rows][cin] the layer's input, g [rows][cout] the gradient of its output (zero
+ * on halo rows); dw [27][cout][cin] = sum_rows g[row][co] x[row + tap offset][ci] and db [cout]
+ * in FP32 (tcgen05 for cin, cout in {16, 32}, CUDA cores otherwise).  No reference counterpart
+ * (the reference has no network); used by the tests. */
+int i3g_unet_wgrad_host(int cin, int cout, int nx, int ny, int nz, const uint16_t *x, const uint16_t *g, float *dw,
+                        float *db);
 /* Last i3g_stokes: used = -1 no staged start, 0 rejected, 1 used; relative residuals of the
  * staged start (after scaling its correction by alpha) and of the default start; alpha is the
  * factor a >= 0 minimising the row-weighted residual of default + a (staged - default). */
