@@ -494,41 +494,28 @@ struct BcDev4 {
     BcDev b[4];
 };
 
-// one component's row of residual_at
-template <typename T, int V>
-__device__ __forceinline__ void residual_row(const View<T> &L, long n)
-{
-    int i, j, k;
-    node_ijk(L, n, i, j, k);
-    if (!row_exists(V, i, j, k, L.nx, L.ny, L.nz) || (L.bc[n] & (1 << V))) return;
-    if (V == 0) { T s = L.f0[n]; crow<T, true>(L, i, j, k, n, s); L.r0[n] = s; }
-    if (V == 1) { T s = L.f1[n]; xrow<T, true>(L, i, j, k, n, s); L.r1[n] = s; }
-    if (V == 2) { T s = L.f2[n]; yrow<T, true>(L, i, j, k, n, s); L.r2[n] = s; }
-    if (V == 3) { T s = L.f3[n]; zrow<T, true>(L, i, j, k, n, s); L.r3[n] = s; }
-}
-
-// Residual of all rows, one component per blockIdx.y (a thread computes one row, so four times
-// as many threads as nodes keep enough loads in flight); blocks from rowblocks on take the
-// boundary rows of that component (they write only boundary nodes, which the row threads skip,
-// and read no residual).  Each row uses the same per-row function as residual_at: bit-identical.
+// Residual of all rows; blocks from rowblocks on take the boundary rows of the four components
+// (they write only boundary nodes, which the row threads skip, and read no residual).  One thread
+// computes the four rows of a node, which share most of their loads (one thread per row and
+// component took 25 % longer with a cold L2).
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual_bc(View<T> L, BcDev4 B, unsigned rowblocks)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_residual_bc(View<T> L, BcDev4 B, unsigned rowblocks)
 {
     pdl_enter();
-    const int v = blockIdx.y;
     if (blockIdx.x >= rowblocks) {
-        const int t = (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
-        if (t < B.b[v].n) bc_residual_at<T>(L, v, t, B.b[v].node, B.b[v].onode, B.b[v].ocomp, B.b[v].ok);
+        int t = (int)(blockIdx.x - rowblocks) * (int)blockDim.x + (int)threadIdx.x;
+        for (int v = 0; v < 4; v++) {
+            if (t < B.b[v].n) {
+                bc_residual_at<T>(L, v, t, B.b[v].node, B.b[v].onode, B.b[v].ocomp, B.b[v].ok);
+                return;
+            }
+            t -= B.b[v].n;
+        }
         return;
     }
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= L.nxy * L.nz) return;
-    switch (v) {
-    case 0: residual_row<T, 0>(L, n); break;
-    case 1: residual_row<T, 1>(L, n); break;
-    case 2: residual_row<T, 2>(L, n); break;
-    default: residual_row<T, 3>(L, n); break;
-    }
+    residual_at<T>(L, n);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1717,9 +1704,9 @@ static void residual_t(i3g_ctx *c, int l)
     if (c->fuse) {
         BcDev4 B;
         long nb = 0;
-        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L.bcl[v]); nb = std::max(nb, (long)L.bcl[v].n); }
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L.bcl[v]); nb += L.bcl[v].n; }
         const unsigned rows = nblk(L.n);
-        LAUNCH(k_residual_bc<T>, dim3(rows + nblk(nb), 4), 256, V, B, rows);
+        LAUNCH(k_residual_bc<T>, rows + nblk(nb), 256, V, B, rows);
         return;
     }
     LAUNCH(k_residual<T>, nblk(L.n), 256, V);
@@ -2601,8 +2588,8 @@ static int kry_enqueue_step(i3g_ctx *c, int j, int multinum)
     if (c->fuse) {
         BcDev4 B;
         long nb = 0;
-        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L0.bcl[v]); nb = std::max(nb, (long)L0.bcl[v].n); }
-        LAUNCH(k_residual_bc<double>, dim3(nblk(N) + nblk(nb), 4), 256, Vz, B, nblk(N));
+        for (int v = 0; v < 4; v++) { B.b[v] = bcdev(L0.bcl[v]); nb += L0.bcl[v].n; }
+        LAUNCH(k_residual_bc<double>, nblk(N) + nblk(nb), 256, Vz, B, nblk(N));
     } else {
         LAUNCH(k_residual<double>, nblk(N), 256, Vz);
         for (int v = 0; v < 4; v++) {

@@ -3,7 +3,7 @@
  *
  * Run in a directory holding file.t3c, mode.t3c and the input .prn, like the reference:
  *
- *     i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-files N]
+ *     i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-warm W] [-exact] [-files N]
  *     i3g -roundtrip in.prn out.prn      (read and rewrite a .prn; no GPU used)
  *     i3g -dump-mode mode.t3c            (print the parsed parameters; no GPU used)
  *
@@ -12,7 +12,8 @@
  * parameter row (i3mg.c:64-77) and cyc0max time steps of
  *     Stokes (vpiterate) -> heat (titerate) -> markers (movemark) -> nodes (ronurecalc)
  * (i3mg.c:80-147), then saver and file.t3c.  Solver controls that the reference does not
- * have (relative stopping tolerances, precision) come from the command line.
+ * have (relative stopping tolerances, precision, FGMRES, the extrapolated Stokes start -warm 2|3,
+ * the marker kernels in the reference's operation order -exact) come from the command line.
  *
  * Saving overlaps the computation: the model images live in page-locked memory, each output
  * file's state is downloaded into a staging image, and a writer thread writes the .prn file and
@@ -111,7 +112,7 @@ static int roundtrip(const char *in, const char *out)
 int main(int argc, char **argv)
 {
     double rtol = 1e-8, heat_rtol = 1e-10;
-    int maxcyc = 2000, precision = 0, max_files = -1, krylov = 0;
+    int maxcyc = 2000, precision = 0, max_files = -1, krylov = 0, warm = 1, exact = 0;
     for (int a = 1; a < argc; a++) {
         if (!strcmp(argv[a], "-roundtrip") && a + 2 < argc) return roundtrip(argv[a + 1], argv[a + 2]);
         else if (!strcmp(argv[a], "-dump-mode") && a + 1 < argc) return dump_mode(argv[a + 1]);
@@ -120,9 +121,11 @@ int main(int argc, char **argv)
         else if (!strcmp(argv[a], "-maxcyc") && a + 1 < argc) maxcyc = atoi(argv[++a]);
         else if (!strcmp(argv[a], "-mixed")) precision = 1;
         else if (!strcmp(argv[a], "-krylov") && a + 1 < argc) krylov = atoi(argv[++a]);
+        else if (!strcmp(argv[a], "-warm") && a + 1 < argc) warm = atoi(argv[++a]);
+        else if (!strcmp(argv[a], "-exact")) exact = 1;
         else if (!strcmp(argv[a], "-files") && a + 1 < argc) max_files = atoi(argv[++a]);
         else {
-            fprintf(stderr, "usage: i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-files N]\n"
+            fprintf(stderr, "usage: i3g [-rtol R] [-heat-rtol R] [-maxcyc N] [-mixed] [-krylov M] [-warm W] [-exact] [-files N]\n"
                             "       i3g -roundtrip in.prn out.prn\n");
             return 2;
         }
@@ -150,8 +153,9 @@ int main(int argc, char **argv)
     md.p.heat_rtol = heat_rtol;
     md.p.heat_maxcyc = maxcyc;
     md.p.precision = precision;
-    md.p.warm_start = 1;
+    md.p.warm_start = warm;
     md.p.krylov = krylov;
+    md.p.marker_exact = exact;
     i3g_ctx *c = NULL;
     if (check(i3g_create(&p.m, &md.p, &c), NULL, "i3g_create")) return 1;
     int rc = 0;
