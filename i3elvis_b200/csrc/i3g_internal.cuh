@@ -186,6 +186,9 @@ struct i3g_ctx {
     int coop_blocks = 0;                        // its grid: every CTA resident at once (0: no cooperative launch)
     unsigned *dbar = nullptr;                   // its grid barrier: arrival count, generation
     int *dbar_err = nullptr;                    // set when a grid barrier wait timed out
+    // FP32 smoother's pressure scale: the face rows' harmonic-mean viscosity where it exceeds the
+    // cell viscosity by more than this factor (k_nd_schur; 0: the cell viscosity everywhere)
+    int nd_schur = 10;
     double *hist[3][4] = {};                    // last three converged level-0 solutions, newest last
                                                 // (warm_start 2 and 3)
     int hist_check = 0;                         // an upload is being compared with the last solution

@@ -1076,6 +1076,75 @@ __global__ void k_eta_f32(long n, const double *ec, const double *exy, const dou
     fnd[t] = (float)((double)nd[t] * inv_ref);
 }
 
+// Pressure-update scale of the FP32 preconditioner's smoother.  The reference scales a cell's
+// pressure correction by the cell's own viscosity (nd = etac, p -= r nd p0koef).  The diagonal of
+// the pressure Schur complement B diag(A)^-1 B^T is the sum over the cell's six faces of
+// (1/h)^2 / diag(face velocity row), so its inverse scales with the harmonic mean of the face rows'
+// viscosities: a weak cell enclosed by stiff material (a weak layer's cell inside a 1e24
+// lithosphere) needs corrections set by its stiff neighbours, and the cell viscosity makes them
+// 1e5 times too small (its divergence stalls; the subduction model's continuity residual stopped
+// at 1e-3).  In regions of smooth viscosity the two scales agree.
+//
+// weighted mean of a velocity row's six stencil viscosities: the row's diagonal over the one it has
+// with unit viscosity (xrow, yrow, zrow coefficients)
+__device__ double vrow_eta(const View<double> &L, int V, int i, int j, int k, long n)
+{
+    const long NY = L.ny, NXY = L.nxy;
+    double w[6], e[6];
+    if (V == 1) {
+        const double XK = 2.0 * L.isx[i], YK = L.icy[j + 1], ZK = L.icz[k + 1];
+        w[0] = XK * L.icx[i]; w[1] = XK * L.icx[i + 1]; w[2] = YK * L.isy[j]; w[3] = YK * L.isy[j + 1];
+        w[4] = ZK * L.isz[k]; w[5] = ZK * L.isz[k + 1];
+        e[0] = L.etac[n + NXY + 1]; e[1] = L.etac[n + NXY + NY + 1]; e[2] = L.etaxy[n]; e[3] = L.etaxy[n + 1];
+        e[4] = L.etaxz[n]; e[5] = L.etaxz[n + NXY];
+    } else if (V == 2) {
+        const double XK = L.icx[i + 1], YK = 2.0 * L.isy[j], ZK = L.icz[k + 1];
+        w[0] = YK * L.icy[j]; w[1] = YK * L.icy[j + 1]; w[2] = XK * L.isx[i]; w[3] = XK * L.isx[i + 1];
+        w[4] = ZK * L.isz[k]; w[5] = ZK * L.isz[k + 1];
+        e[0] = L.etac[n + NY + NXY]; e[1] = L.etac[n + NY + 1 + NXY]; e[2] = L.etaxy[n]; e[3] = L.etaxy[n + NY];
+        e[4] = L.etayz[n]; e[5] = L.etayz[n + NXY];
+    } else {
+        const double XK = L.icx[i + 1], YK = L.icy[j + 1], ZK = 2.0 * L.isz[k];
+        w[0] = ZK * L.icz[k]; w[1] = ZK * L.icz[k + 1]; w[2] = XK * L.isx[i]; w[3] = XK * L.isx[i + 1];
+        w[4] = YK * L.isy[j]; w[5] = YK * L.isy[j + 1];
+        e[0] = L.etac[n + NY + 1]; e[1] = L.etac[n + NY + 1 + NXY]; e[2] = L.etaxz[n]; e[3] = L.etaxz[n + NY];
+        e[4] = L.etayz[n]; e[5] = L.etayz[n + 1];
+    }
+    double sw = 0, se = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++) { sw += w[q]; se += w[q] * e[q]; }
+    return sw > 0 ? se / sw : 0.0;
+}
+
+// fnd[cell] = the harmonic mean over the cell's interior face rows of vrow_eta where it exceeds the
+// cell viscosity by more than the factor ratio, scaled like the FP32 copy; the cell viscosity
+// otherwise.  Only a weak cell (nearly) enclosed by stiff material reaches a large ratio; on the
+// boundary of a weak inclusion the weak faces keep the harmonic mean within a few times the cell
+// viscosity, and changing the scale there costs the inclusion models a V-cycle per step.
+__global__ void k_nd_schur(View<double> L, float *fnd, double inv_ref, double ratio)
+{
+    pdl_enter();
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L.nxy * L.nz) return;
+    int i, j, k;
+    node_ijk(L, n, i, j, k);
+    if (!row_exists(0, i, j, k, L.nx, L.ny, L.nz)) return;
+    const long v0 = n - L.nxy - L.ny - 1;
+    const int fi[6] = {i - 1, i, i - 1, i - 1, i - 1, i - 1}, fj[6] = {j - 1, j - 1, j - 1, j, j - 1, j - 1},
+              fk[6] = {k - 1, k - 1, k - 1, k - 1, k - 1, k}, fv[6] = {1, 1, 2, 2, 3, 3};
+    const long fm[6] = {v0, v0 + L.ny, v0, v0 + 1, v0, v0 + L.nxy};
+    double inv = 0;
+    int cnt = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        if (!row_exists(fv[q], fi[q], fj[q], fk[q], L.nx, L.ny, L.nz) || (L.bc[fm[q]] & (1 << fv[q]))) continue;
+        const double e = vrow_eta(L, fv[q], fi[q], fj[q], fk[q], fm[q]);
+        if (e > 0) { inv += 1.0 / e; cnt++; }
+    }
+    const double h = cnt ? (double)cnt / inv : 0.0;
+    if (h > ratio * L.etac[n]) fnd[n] = (float)(h * inv_ref);
+}
+
 // level-0 right-hand side (move3mg.c:751, 942, 1140) and boundary constants
 __global__ void k_rhs0(View<double> L, const float *ro, double gx, double gy, double gz)
 {
@@ -1490,6 +1559,7 @@ int stokes_alloc(i3g_ctx *c)
     // I3G_FUSE: 0 one launch per boundary pass, residual part and transfer component; 1 boundary
     // rows in-kernel on levels >= 1 (default); 3 on level 0 too
     if (const char *e = getenv("I3G_FUSE")) c->fuse = atoi(e);
+    if (const char *e = getenv("I3G_ND_SCHUR")) c->nd_schur = std::max(0, atoi(e));
     if (c->tail_cluster > 8) {
         I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         I3G_CUDA(cudaFuncSetAttribute(k_vcycle_cluster<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1653,6 +1723,8 @@ int stokes_setup(i3g_ctx *c)
         LAUNCH(k_eta, nblk(L.n), 256, a);
         LAUNCH(k_eta_f32, nblk(L.n), 256, L.n, L.d.etac, L.d.etaxy, L.d.etaxz, L.d.etayz, (const float *)a.nd,
                L.s.etac, L.s.etaxy, L.s.etaxz, L.s.etayz, L.s.nd, 1.0 / c->eta_ref);
+        if (c->nd_schur > 0)
+            LAUNCH(k_nd_schur, nblk(L.n), 256, view<double>(L, L.d), L.s.nd, 1.0 / c->eta_ref, (double)c->nd_schur);
         for (int v = 0; v < 4; v++) {
             I3G_CUDA(cudaMemsetAsync(L.d.u[v], 0, L.n * 8, c->st));
             I3G_CUDA(cudaMemsetAsync(L.d.f[v], 0, L.n * 8, c->st));

@@ -166,3 +166,37 @@ def test_extrapolated_warm_start_reaches_same_solution(warm):
     assert cyc[1][3] <= cyc[0][3] + 2, cyc
     assert starts[0] == [0, 0, 0, 0], starts
     assert starts[1] == ([0, 0, 1, 1] if warm == 2 else [0, 0, 1, 3]), starts
+
+
+def test_weak_layer_cells_converge_with_face_pressure_scale(monkeypatch):
+    """Visco-plastic subduction model at 65 x 33 x 65 (weak layer of 1e19 Pa s inside a 1e24
+    lithosphere): the FP32 preconditioner with the face rows' pressure scale for enclosed weak
+    cells reaches relative residual 1e-8; with the cell viscosity as the scale (the reference's
+    nd) the continuity residual of those cells stalls."""
+    from i3elvis_b200 import config, model, runtime
+    from i3elvis_b200.prn import YEAR
+    prn, _ = model.subduction(nx=65, ny=33, nz=65, mnum=2, multinum=3, seed=11)
+    dx = 1000e3 / 64
+    mode = config.Mode(infile="in0.prn", multinum=3, multicyc=1, multinnn=((2, 4, 4, 0), (2, 4, 4, 4)),
+                       p0koef=0.71, p1koef=1.0, v0koef=0.7, v1koef=0.7, nubeg=1e18, nuend=1e24,
+                       files=[config.OutFile("out1.prn", maxxystep=0.5 * dx, maxtmstep_yr=1e9, nubeg=1e18,
+                                             nuend=1e24, p0koef=0.71, p1koef=1.0, p0koef2=0.71, p1koef2=0.0,
+                                             multinum=3, multinum2=3)])
+    res = {}
+    for scale in ("10", "0"):
+        monkeypatch.setenv("I3G_ND_SCHUR", scale)
+        par = abi.make_params(mode, stokes_rtol=1e-8, stokes_maxcyc=200, precision=1, krylov=8, warm_start=1)
+        g = lib.Context(abi.ModelBuffers(prn), par, abi.make_file_params(mode.files[0]))
+        runtime.prepare(g)
+        try:
+            g.stokes(0, 1e9 * YEAR)
+            ok = True
+        except lib.I3gError as e:
+            assert abi.E_CODES.get(e.code) == "NOCONV", e
+            ok = False
+        res[scale] = (ok, g.stats())
+        g.close()
+    ok, st = res["10"]
+    assert ok and st["stokes_rel"] <= 1e-8 and st["stokes_cycles"] < 200, st
+    ok0, st0 = res["0"]
+    assert not ok0 and st0["stokes_cont_rel"] > 1e-5, st0
