@@ -1127,15 +1127,48 @@ void tap_offsets(const Dims &d, int *off)
                 off[(dz + 1) * 9 + (dx + 1) * 3 + (dy + 1)] = dz * d.X * d.Y + dx * d.Y + dy;
 }
 
+// Per-device launch set-up of a persistent tensor-core kernel: its shared-memory attributes (set
+// once per device: a function attribute belongs to the device it was set on) and its grid, every
+// resident CTA on every SM from the shared-memory footprint (each CTA holds at most 256 of the
+// 512 TMEM columns and 128 threads of fewer than 96 registers, which bind less)
+struct LaunchSetup { int sms = 0, per_sm = 0; };
+constexpr int kMaxDev = 64;
+
+template <typename K>
+cudaError_t persistent_setup(K kernel, int smem, int max_per_sm, LaunchSetup (&cache)[kMaxDev], LaunchSetup &out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    LaunchSetup &c = cache[dev];
+    if (!c.per_sm) {
+        if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+        // the whole unified L1 as shared memory, so that several CTAs fit on an SM
+        if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess) return e;
+        int sms = 0, smem_sm = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+        c.sms = sms;
+        c.per_sm = std::max(1, std::min(max_per_sm, smem_sm / (smem + 1024 + 64)));
+    }
+    out = c;
+    return cudaSuccess;
+}
+
 template <int CIN, int COUT>
 cudaError_t launch_conv_t(const ConvArgs &a, cudaStream_t st)
 {
     using S = ConvShape<CIN, COUT>;
-    static bool attr = false;
-    if (!attr) {
+    static bool attr[kMaxDev] = {};
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return e0;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
         cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
         if (e != cudaSuccess) return e;
-        attr = true;
+        attr[dev] = true;
     }
     k_conv_tc<CIN, COUT><<<nblk(a.d.np, kTileM), 128, S::SMEM, st>>>(a);
     return cudaGetLastError();
@@ -1146,22 +1179,10 @@ template <int CIN, int COUT>
 cudaError_t launch_brick_t(const ConvArgs &a, cudaStream_t st)
 {
     using S = BrickShape<CIN, COUT>;
-    static int per_sm = 0, sms = 0;
-    if (!per_sm) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv_brick<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
-        if (e != cudaSuccess) return e;
-        // the whole unified L1 as shared memory, so that several CTAs fit on an SM
-        e = cudaFuncSetAttribute(k_conv_brick<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return e;
-        int dev = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-        // resident CTAs per SM from the shared-memory footprint (each CTA also holds NCOL <= 32 of
-        // the 512 TMEM columns and 128 threads of at most 64 registers, neither of which binds)
-        int smem_sm = 0;
-        if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
-        per_sm = std::max(1, std::min(8, smem_sm / (S::SMEM + 1024 + 64)));
-    }
+    static LaunchSetup cache[kMaxDev];
+    LaunchSetup ls;
+    if (cudaError_t e = persistent_setup(k_conv_brick<CIN, COUT>, S::SMEM, 8, cache, ls)) return e;
+    const int sms = ls.sms, per_sm = ls.per_sm;
     const int ntx = (a.d.nx + kBx - 1) / kBx, nty = (a.d.ny + kBy - 1) / kBy, ntz = (a.d.nz + kBz - 1) / kBz;
     const int ntiles = ntx * nty * ntz;
     const int grid = std::min(ntiles, sms * per_sm);
@@ -1215,18 +1236,10 @@ cudaError_t launch_wgrad_tc_t(const bf16 *X, const bf16 *G, float *dW, float *db
                               int *err, cudaStream_t st)
 {
     using S = WgradShape<CIN, COUT>;
-    static int per_sm = 0, sms = 0;
-    if (!per_sm) {
-        cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
-        if (e != cudaSuccess) return e;
-        if ((e = cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
-            return e;
-        int dev = 0, smem_sm = 0;
-        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
-        per_sm = std::max(1, std::min(kWgradPerSm, smem_sm / (S::SMEM + 1024 + 64)));
-    }
+    static LaunchSetup cache[kMaxDev];
+    LaunchSetup ls;
+    if (cudaError_t e = persistent_setup(k_wgrad_tc<CIN, COUT>, S::SMEM, kWgradPerSm, cache, ls)) return e;
+    const int sms = ls.sms, per_sm = ls.per_sm;
     const int ntx = (d.nx + kBx - 1) / kBx, nty = (d.ny + kBy - 1) / kBy, ntz = (d.nz + kBz - 1) / kBz;
     const int ntiles = ntx * nty * ntz;
     const int grid = std::min(std::min(ntiles, sms * per_sm), slots);
