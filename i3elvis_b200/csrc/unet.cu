@@ -385,12 +385,15 @@ __global__ void __launch_bounds__(128) k_conv_tc(ConvArgs a)
 // output tile) and waits on each fetch.  Here a persistent CTA keeps all 27 taps' weights in
 // shared memory and walks over output tiles of 2 x 8 x 8 nodes (z, x, y): it loads the tile's
 // input brick with its one-node halo (4 x 10 x 10 rows) once, then for every tap gathers the
-// shifted 128-row operand from the brick into one of two aligned operand buffers (the canonical
-// no-swizzle K-major layout) while the tensor core runs the previous tap's MMA.  One thread
-// issues the MMAs (M = 128, N = COUT, K = 16) into the CTA's TMEM accumulator; tcgen05.commit
-// arrives on the operand buffer's mbarrier, which the gather of the tap after next waits for.
-// The epilogue is k_conv_tc's (bias, skip add, ReLU or the backward ReLU mask, BF16 or FP32
-// stores of the interior rows).
+// shifted 128-row operands of three taps at a time from the brick into one of NST aligned
+// operand stages (the canonical no-swizzle K-major layout).  The work is split by warp: four
+// producer warps gather the stages and arrive on the stage's "full" mbarrier (no CTA-wide barrier
+// per stage); a fifth warp, one thread, waits for "full", issues the MMAs (M = 128, N = COUT,
+// K = 16) into the CTA's TMEM accumulator and commits to the stage's "empty" mbarrier, which the
+// producers wait for before they reuse the stage, and after a tile's last stage to "accf".  The
+// producers load the next tile's brick and then run the epilogue of the tile (k_conv_tc's: bias,
+// skip add, ReLU or the backward ReLU mask, BF16 or FP32 stores of the interior rows) once
+// "accf" says its MMAs completed.
 constexpr int kBz = 2, kBx = 8, kBy = 8;                    // output tile (z, x, y): 128 rows
 constexpr int kHz = kBz + 2, kHx = kBx + 2, kHy = kBy + 2;   // input brick with halo
 constexpr int kBrickRows = kHz * kHx * kHy;
@@ -417,47 +420,46 @@ struct BrickShape {
     static_assert(TAPB % 512 == 0 && ABYTES % 1024 == 0, "operand alignment");
 };
 
+// producer warps of the brick kernels (warps 0-3) and the MMA warp (warp 4)
+constexpr int kProducers = 128, kBrickThreads = kProducers + 32;
+
+// OR of a flag over the producer warps; named barrier 1, so the MMA warp does not take part
+__device__ __forceinline__ bool producers_or(bool v)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r)
+                 : "r"((uint32_t)v), "n"(kProducers)
+                 : "memory");
+    return r != 0;
+}
+
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) k_conv_brick(ConvArgs a, int ntx, int nty, int ntiles)
+__global__ void __launch_bounds__(kBrickThreads) k_conv_brick(ConvArgs a, int ntx, int nty, int ntiles)
 {
     using S = BrickShape<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar[S::NST];
+    __shared__ __align__(8) uint64_t full[S::NST], empty[S::NST], accf;
     __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5;
-    // operand buffers and weights at 1024-byte boundaries (tensor-core operand alignment)
+    // operand stages and weights at 1024-byte boundaries (tensor-core operand alignment)
     const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
     const uint32_t sA0 = sbase, sW = sbase + S::NST * S::STB, sBrick = sW + S::WBYTES;
     uint8_t *const gbase = smem + (sbase - smem_u32(smem));
     const uint8_t *const brick = gbase + S::NST * S::STB + S::WBYTES;
     uint8_t *const abuf = gbase;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(S::NCOL)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (tid == 0) {
-        for (int s = 0; s < S::NST; s++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    // all taps' weights, once per CTA: tap t, output channel n, chunk j at t*TAPB + j*(COUT*16) + n*16
-    for (int q = tid; q < 27 * COUT * S::CH; q += 128) {
-        const int t = q / (COUT * S::CH), rem = q - t * (COUT * S::CH);
-        const int n = rem / S::CH, j = rem - n * S::CH;
-        cp_async16(sW + (uint32_t)(t * S::TAPB + j * (COUT * 16) + n * 16), a.w + ((long)t * COUT + n) * CIN + j * 8, 16);
-    }
     const long XY = (long)a.d.X * a.d.Y;
-    // input brick of a tile: padded rows (z0-1 .. z0+2, x0-1 .. x0+8, y0-1 .. y0+8), zero outside
     auto tile_origin = [&](int tile, int &z0, int &x0, int &y0) {
         const int ty = tile % nty, r2 = tile / nty, tx = r2 % ntx, tz = r2 / ntx;
         z0 = 1 + kBz * tz; x0 = 1 + kBx * tx; y0 = 1 + kBy * ty;
     };
+    // input brick of a tile, loaded by the producers: padded rows (z0-1 .. z0+2, x0-1 .. x0+8,
+    // y0-1 .. y0+8), zero outside the array
     auto load_brick = [&](int tile) {
         int z0, x0, y0;
         tile_origin(tile, z0, x0, y0);
-        for (int q = tid; q < kBrickRows * S::CH; q += 128) {
+        for (int q = tid; q < kBrickRows * S::CH; q += kProducers) {
             const int br = q / S::CH, j = q - br * S::CH;
             const int bz = br / (kHx * kHy), bxy = br - bz * (kHx * kHy), bx = bxy / kHy, by = bxy - bx * kHy;
             const int zz = z0 - 1 + bz, xx = x0 - 1 + bx, yy = y0 - 1 + by;
@@ -466,134 +468,167 @@ __global__ void __launch_bounds__(128) k_conv_brick(ConvArgs a, int ntx, int nty
             cp_async16(sBrick + (uint32_t)(S::slot(br, j) * 16), a.in + src * CIN + j * 8, ok ? 16 : 0);
         }
     };
-    if ((int)blockIdx.x < ntiles) load_brick(blockIdx.x);
-    cp_async_commit();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(S::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S::NST; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(kProducers) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])) : "memory");
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (tid < kProducers) {
+        // all taps' weights, once per CTA: tap t, output channel n, chunk j at t*TAPB + j*(COUT*16) + n*16
+        for (int q = tid; q < 27 * COUT * S::CH; q += kProducers) {
+            const int t = q / (COUT * S::CH), rem = q - t * (COUT * S::CH);
+            const int n = rem / S::CH, j = rem - n * S::CH;
+            cp_async16(sW + (uint32_t)(t * S::TAPB + j * (COUT * 16) + n * 16), a.w + ((long)t * COUT + n) * CIN + j * 8, 16);
+        }
+        if ((int)blockIdx.x < ntiles) load_brick(blockIdx.x);
+        cp_async_commit();
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    long g = 0;             // stages issued by this CTA so far (buffer g % NST, its commit number g / NST)
-    bool failed = false;
-    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        int z0, x0, y0;
-        tile_origin(tile, z0, x0, y0);
-        cp_async_wait<0>();   // this tile's brick (and, the first time, the weights)
-        __syncthreads();
-        // output row r = tid: tile-local (tz, tx, ty) = (r >> 6, (r >> 3) & 7, r & 7)
-        const int oz = tid >> 6, ox = (tid >> 3) & 7, oy = tid & 7;
-        // stage st = (dz, dx) gathers and multiplies the three taps dy = 0, 1, 2
-        for (int st = 0; st < 9; st++, g++) {
-            const int b = (int)(g % S::NST);
-            int fail = 0;
-            // the buffer was last read by the MMAs of stage g - NST
-            if (g >= S::NST && !mbar_wait(smem_u32(&mbar[b]), (uint32_t)((g / S::NST - 1) & 1))) fail = 1;
-            const int dz = st / 3, dx = st % 3;
-            const int br0 = ((oz + dz) * kHx + (ox + dx)) * kHy + oy;
-            uint8_t *dst = abuf + b * S::STB + tid * 16;
-            if (!fail) {
+    volatile int *abort_flag = &s_abort;
+    long issued = 0;   // MMA thread: stages committed
+    if (warp == kProducers / 32) {
+        // ---- MMA issuer: one thread ----
+        if ((tid & 31) == 0) {
+            long g = 0;
+            bool mfail = false;
+            for (int tile = blockIdx.x; tile < ntiles && !mfail; tile += gridDim.x) {
+                for (int st = 0; st < 9; st++, g++) {
+                    const int b = (int)(g % S::NST);
+                    if (!mbar_wait(smem_u32(&full[b]), (uint32_t)((g / S::NST) & 1))) { mfail = true; break; }
+                    tc_fence_after();
 #pragma unroll
-                for (int dy = 0; dy < kTapsPerStage; dy++)
+                    for (int dy = 0; dy < kTapsPerStage; dy++) {
+                        const int tap = st * 3 + dy;
+                        const uint32_t sA = sA0 + (uint32_t)(b * S::STB + dy * S::ABYTES), sB = sW + (uint32_t)(tap * S::TAPB);
 #pragma unroll
-                    for (int j = 0; j < S::CH; j++)
-                        *reinterpret_cast<uint4 *>(dst + dy * S::ABYTES + j * (kTileM * 16)) =
-                            *reinterpret_cast<const uint4 *>(brick + S::slot(br0 + dy, j) * 16);
-            }
-            fence_proxy_async();   // the gathered operands to the tensor core's (async) proxy
-            if (__syncthreads_or(fail)) { failed = true; break; }
-            if (tid == 0) {
-                tc_fence_after();
-#pragma unroll
-                for (int dy = 0; dy < kTapsPerStage; dy++) {
-                    const int tap = st * 3 + dy;   // = dz * 9 + dx * 3 + dy
-                    const uint32_t sA = sA0 + (uint32_t)(b * S::STB + dy * S::ABYTES), sB = sW + (uint32_t)(tap * S::TAPB);
-#pragma unroll
-                    for (int k = 0; k < CIN / 16; k++) {
-                        const uint64_t da = smem_desc(sA + (uint32_t)(2 * k * kTileM * 16), kTileM * 16, 128);
-                        const uint64_t db = smem_desc(sB + (uint32_t)(2 * k * COUT * 16), COUT * 16, 128);
-                        tc_mma(tmem, da, db, S::IDESC, (tap > 0 || k > 0) ? 1u : 0u);
+                        for (int k = 0; k < CIN / 16; k++) {
+                            const uint64_t da = smem_desc(sA + (uint32_t)(2 * k * kTileM * 16), kTileM * 16, 128);
+                            const uint64_t db = smem_desc(sB + (uint32_t)(2 * k * COUT * 16), COUT * 16, 128);
+                            tc_mma(tmem, da, db, S::IDESC, (tap > 0 || k > 0) ? 1u : 0u);
+                        }
                     }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&empty[b]))
+                                 : "memory");
+                    issued = g + 1;
                 }
+                if (mfail) break;
+                // arrives once every MMA of this tile completed
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&mbar[b]))
+                                 smem_u32(&accf))
                              : "memory");
             }
+            // MMAs still in flight read the stages and write TMEM: wait for the last commit
+            if (issued > 0) {
+                const long gl = issued - 1;
+                if (!mbar_wait(smem_u32(&empty[gl % S::NST]), (uint32_t)((gl / S::NST) & 1))) mfail = true;
+            }
+            if (mfail) *abort_flag = 1;
         }
-        if (failed) break;
-        // every gather of this tile is done: the next tile's brick loads while the epilogue runs
-        if (tile + (int)gridDim.x < ntiles) load_brick(tile + gridDim.x);
-        cp_async_commit();
-        // the last commit arrives once every MMA of this tile completed
-        const long gl = g - 1;
-        int fail = 0;
-        if (!mbar_wait(smem_u32(&mbar[gl % S::NST]), (uint32_t)((gl / S::NST) & 1))) fail = 1;
-        if (__syncthreads_or(fail)) { failed = true; break; }
-        tc_fence_after();
-        const int zz = z0 + oz, xx = x0 + ox, yy = y0 + oy;
-        const bool valid = zz <= a.d.nz && xx <= a.d.nx && yy <= a.d.ny;
-        const long p = (long)zz * XY + (long)xx * a.d.Y + yy;
+    } else {
+        // ---- producers (warps 0-3): gathers, next brick, epilogue ----
+        // A failed (timed-out) wait only sets this thread's flag: every producer still arrives on
+        // every stage and reaches every producer barrier, and all stop together where the flags
+        // are combined (an unbounded named barrier must never miss a participant).
+        const int oz = tid >> 6, ox = (tid >> 3) & 7, oy = tid & 7;   // output row r = tid of the tile
+        long g = 0;
+        int q = 0;
+        bool fail = false;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, q++) {
+            int z0, x0, y0;
+            tile_origin(tile, z0, x0, y0);
+            cp_async_wait<0>();                  // this thread's part of the brick (and weights)
+            if (producers_or(fail)) { fail = true; break; }   // and everyone's part
+            for (int st = 0; st < 9; st++, g++) {
+                const int b = (int)(g % S::NST);
+                // the stage's buffer was last read by the MMAs of stage g - NST
+                if (!fail && g >= S::NST && !mbar_wait(smem_u32(&empty[b]), (uint32_t)((g / S::NST - 1) & 1))) fail = true;
+                if (!fail) {
+                    const int dz = st / 3, dx = st % 3;
+                    const int br0 = ((oz + dz) * kHx + (ox + dx)) * kHy + oy;
+                    uint8_t *dst = abuf + b * S::STB + tid * 16;
 #pragma unroll
-        for (int c0 = 0; c0 < COUT; c0 += 16) {
-            float v[16];
-            tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);   // whole warp
-            if (!valid) continue;
-            if (a.bias) {
+                    for (int dy = 0; dy < kTapsPerStage; dy++)
 #pragma unroll
-                for (int q = 0; q < 16; q++) v[q] += a.bias[c0 + q];
-            }
-            if (a.add) {
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    float f[8];
-                    unpack8(*reinterpret_cast<const uint4 *>(a.add + p * COUT + c0 + 8 * h), f);
-#pragma unroll
-                    for (int q = 0; q < 8; q++) v[8 * h + q] += f[q];
+                        for (int j = 0; j < S::CH; j++)
+                            *reinterpret_cast<uint4 *>(dst + dy * S::ABYTES + j * (kTileM * 16)) =
+                                *reinterpret_cast<const uint4 *>(brick + S::slot(br0 + dy, j) * 16);
                 }
+                fence_proxy_async();   // the gathered operands to the tensor core's (async) proxy
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[b])) : "memory");
             }
-            if (a.relu) {
+            // every producer's gathers of this tile are done: the next tile's brick loads while the
+            // epilogue runs
+            if (producers_or(fail)) { fail = true; break; }
+            if (tile + (int)gridDim.x < ntiles) load_brick(tile + gridDim.x);
+            cp_async_commit();
+            if (!mbar_wait(smem_u32(&accf), (uint32_t)(q & 1))) fail = true;
+            // the TMEM load below is warp-collective: the warp decides together
+            if (__any_sync(0xffffffffu, fail)) { fail = true; continue; }
+            tc_fence_after();
+            const int zz = z0 + oz, xx = x0 + ox, yy = y0 + oy;
+            const bool valid = zz <= a.d.nz && xx <= a.d.nx && yy <= a.d.ny;
+            const long p = (long)zz * XY + (long)xx * a.d.Y + yy;
+            float v[COUT];
 #pragma unroll
-                for (int q = 0; q < 16; q++) v[q] = fmaxf(v[q], 0.0f);
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float t16[16];
+                tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, t16);   // whole warp
+#pragma unroll
+                for (int e = 0; e < 16; e++) v[c0 + e] = t16[e];
             }
-            if (a.mask) {
+            // TMEM read: the next tile's first MMA overwrites the accumulator only after the
+            // gathers that follow, ordered after these reads by this fence and the mbarrier
+            tc_fence_before();
+            if (valid) {
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int c0 = 0; c0 < COUT; c0 += 8) {
                     float f[8];
-                    unpack8(*reinterpret_cast<const uint4 *>(a.mask + p * COUT + c0 + 8 * h), f);
 #pragma unroll
-                    for (int q = 0; q < 8; q++) v[8 * h + q] = f[q] > 0.0f ? v[8 * h + q] : 0.0f;
+                    for (int e = 0; e < 8; e++) f[e] = v[c0 + e] + (a.bias ? a.bias[c0 + e] : 0.0f);
+                    if (a.add) {
+                        float h[8];
+                        unpack8(*reinterpret_cast<const uint4 *>(a.add + p * COUT + c0), h);
+#pragma unroll
+                        for (int e = 0; e < 8; e++) f[e] += h[e];
+                    }
+                    if (a.relu) {
+#pragma unroll
+                        for (int e = 0; e < 8; e++) f[e] = fmaxf(f[e], 0.0f);
+                    }
+                    if (a.mask) {
+                        float h[8];
+                        unpack8(*reinterpret_cast<const uint4 *>(a.mask + p * COUT + c0), h);
+#pragma unroll
+                        for (int e = 0; e < 8; e++) f[e] = h[e] > 0.0f ? f[e] : 0.0f;
+                    }
+                    if (a.out) *reinterpret_cast<uint4 *>(a.out + p * COUT + c0) = pack8(f);
+                    if (a.out32) {
+                        *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0) = make_float4(f[0], f[1], f[2], f[3]);
+                        *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0 + 4) = make_float4(f[4], f[5], f[6], f[7]);
+                    }
                 }
-            }
-            if (a.out) {
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    float f[8];
-#pragma unroll
-                    for (int q = 0; q < 8; q++) f[q] = v[8 * h + q];
-                    *reinterpret_cast<uint4 *>(a.out + p * COUT + c0 + 8 * h) = pack8(f);
-                }
-            }
-            if (a.out32) {
-#pragma unroll
-                for (int q = 0; q < 16; q += 4)
-                    *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0 + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
             }
         }
-        // TMEM reads done before the next tile's first MMA overwrites the accumulator; brick and
-        // operand buffers free for the next tile
-        tc_fence_before();
-        __syncthreads();
+        cp_async_wait<0>();
+        if (fail) *abort_flag = 1;
     }
-    if (failed) {
-        // No more epilogues.  MMAs committed before the timeout may still write TMEM and read the
-        // operand buffers: one more bounded wait on the last commit before the columns are released.
-        if (tid == 0) {
-            atomicExch(a.err, 1);
-            if (g > 0) mbar_wait(smem_u32(&mbar[(g - 1) % S::NST]), (uint32_t)(((g - 1) / S::NST) & 1));
-        }
-        __syncthreads();
-    }
-    cp_async_wait<0>();
-    tc_fence_before();
     __syncthreads();
+    if (tid == 0 && *abort_flag) atomicExch(a.err, 1);
+    tc_fence_after();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::NCOL) : "memory");
 }
 
@@ -1187,7 +1222,7 @@ cudaError_t launch_brick_t(const ConvArgs &a, cudaStream_t st)
     const int ntiles = ntx * nty * ntz;
     const int grid = std::min(ntiles, sms * per_sm);
     if (grid < 1) return cudaSuccess;
-    k_conv_brick<CIN, COUT><<<grid, 128, S::SMEM, st>>>(a, ntx, nty, ntiles);
+    k_conv_brick<CIN, COUT><<<grid, kBrickThreads, S::SMEM, st>>>(a, ntx, nty, ntiles);
     return cudaGetLastError();
 }
 
