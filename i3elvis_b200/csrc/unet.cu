@@ -38,6 +38,7 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include "i3g_internal.cuh"
 
@@ -624,6 +625,239 @@ __global__ void __launch_bounds__(kBrickThreads) k_conv_brick(ConvArgs a, int nt
             }
         }
         cp_async_wait<0>();
+        if (fail) *abort_flag = 1;
+    }
+    __syncthreads();
+    if (tid == 0 && *abort_flag) atomicExch(a.err, 1);
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::NCOL) : "memory");
+}
+
+// ---------------------------------------------------------------------------------------
+// TMA-fed tcgen05 convolution (CIN, COUT in {16, 32})
+// ---------------------------------------------------------------------------------------
+// Output tiles of 1 x 16 x 8 nodes (z, x, y).  For each tile one thread issues TMA loads (a 4-D
+// tensor map (channels, y, x, z) over the padded activation) of the input box z0-1..z0+1,
+// x0-1..x0+16 and the 8 y rows y0-1+dy.., one box per dy in {0, 1, 2}, straight into the operand
+// layout of the tensor core: a node's channels land as one row of CIN * 2 bytes (32 B with the
+// 32-byte swizzle, 64 B with the 64-byte one), [z 3][x 18][y 8][row], so 8 consecutive y rows are
+// one swizzle atom of the K-major layout, consecutive x are 8 rows apart and the operand of tap
+// (dz, dx, dy) is the dy box at (dz * 18 + dx) atoms; K steps of 16 channels advance 32 bytes inside
+// the row.  Every operand start stays on its atom, no copy through registers, and one TMA row per
+// node and box (16-byte rows, one per channel chunk, were half as fast).  Boxes stream through a ring of NB slots with a
+// "full" (TMA bytes) and an "empty" (MMA commit) mbarrier each.  A second thread issues, per box,
+// the 9 x CIN/16 MMAs (M = 128, N = COUT, K = 16) of its taps into one of two TMEM accumulators
+// and commits to the slot's "empty" mbarrier, and after a tile's third box to the accumulator's
+// "full" one; four warps read the accumulator (tcgen05.ld), arrive on its "empty" mbarrier and run
+// k_conv_tc's epilogue.  Loads, MMAs and epilogues of consecutive boxes and tiles overlap.  Every
+// wait is bounded.
+constexpr int kTz = 1, kTx = 16, kTy = 8;                   // output tile: 128 rows
+constexpr int kQz = kTz + 2, kQx = kTx + 2, kQy = kTy;      // one dy box
+constexpr int kBoxRows = kQz * kQx * kQy;                   // 432 nodes
+constexpr int kTmaThreads = 192;                           // warps 0-3 epilogue, 4 loads, 5 MMAs
+
+template <int CIN, int COUT>
+struct TmaShape {
+    static constexpr int CH = CIN / 8;
+    static constexpr int ROWB = CIN * 2;                    // bytes of one node in a box
+    static constexpr int TXB = kBoxRows * ROWB;             // bytes one box's load delivers
+    static constexpr int BOXB = (TXB + 1023) / 1024 * 1024;  // one dy box's slot
+    static constexpr int TAPB = COUT * CIN * 2;
+    static constexpr int WBYTES = 27 * TAPB;
+    // ring of box stages: the most that keeps two CTAs on an SM (228 KiB of shared memory, 1 KiB
+    // reserved per CTA) if that is at least a tile's three boxes, else the most for one CTA
+    static constexpr int NB2 = (233472 / 2 - 2048 - 1024 - WBYTES) / BOXB;
+    static constexpr int NB1 = (232448 - 1024 - WBYTES) / BOXB;
+    static constexpr int NB = NB2 >= 3 ? (NB2 < 8 ? NB2 : 8) : (NB1 < 8 ? NB1 : 8);
+    static constexpr int SMEM = 1024 + NB * BOXB + WBYTES;
+    static constexpr uint32_t NCOL = 2 * COUT < 32 ? 32 : 2 * COUT;
+    static constexpr uint32_t IDESC = ConvShape<CIN, COUT>::IDESC;
+    // layout type of the A descriptor (bits 61-63): 6 = 32-byte swizzle, 4 = 64-byte swizzle
+    static constexpr uint64_t ALAYOUT = (CIN == 16 ? 6ull : 4ull) << 61;
+    static_assert((CIN == 16 || CIN == 32) && (COUT == 16 || COUT == 32), "TMA convolution channel counts");
+    static_assert(BOXB % 1024 == 0, "TMA destinations on their swizzle atoms");
+    static_assert(NB >= 2 && SMEM <= 232448, "shared memory of the box ring");
+};
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                 ::"r"(dst), "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
+                 : "memory");
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kTmaThreads) k_conv_tma(const __grid_constant__ CUtensorMap map, ConvArgs a, int ntx, int nty,
+                                                         int ntiles)
+{
+    using S = TmaShape<CIN, COUT>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bfull[S::NB], bempty[S::NB], afull[2], aempty[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
+    const uint32_t sT = sbase, sW = sbase + S::NB * S::BOXB;
+    const long XY = (long)a.d.X * a.d.Y;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(S::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S::NB; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bfull[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bempty[s])) : "memory");
+        }
+        for (int s = 0; s < 2; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&afull[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&aempty[s])), "r"(kProducers) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    // all taps' weights, once per CTA (B operands: tap t, output channel n, chunk j at
+    // t*TAPB + j*(COUT*16) + n*16)
+    if (tid < kProducers) {
+        for (int q = tid; q < 27 * COUT * S::CH; q += kProducers) {
+            const int t = q / (COUT * S::CH), rem = q - t * (COUT * S::CH);
+            const int n = rem / S::CH, j = rem - n * S::CH;
+            cp_async16(sW + (uint32_t)(t * S::TAPB + j * (COUT * 16) + n * 16), a.w + ((long)t * COUT + n) * CIN + j * 8, 16);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        fence_proxy_async();   // the weights to the tensor core's (async) proxy
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    volatile int *abort_flag = &s_abort;
+    auto origin = [&](int tile, int &z0, int &x0, int &y0) {
+        const int ty = tile % nty, r2 = tile / nty, tx = r2 % ntx, tz = r2 / ntx;
+        z0 = 1 + kTz * tz; x0 = 1 + kTx * tx; y0 = 1 + kTy * ty;
+    };
+    if (warp == 4) {
+        // ---- TMA loads: one thread; box g = 3 * (tile's index in this CTA) + dy in slot g % NB ----
+        if (lane == 0) {
+            long g = 0, last = -1;
+            bool fail = false;
+            for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
+                int z0, x0, y0;
+                origin(tile, z0, x0, y0);
+                for (int dy = 0; dy < 3; dy++, g++) {
+                    const int sl = (int)(g % S::NB);
+                    const long use = g / S::NB;
+                    // the slot was last read by the MMAs of box g - NB
+                    if (use >= 1 && !mbar_wait(smem_u32(&bempty[sl]), (uint32_t)((use - 1) & 1))) { fail = true; break; }
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&bfull[sl])),
+                                 "r"((uint32_t)S::TXB)
+                                 : "memory");
+                    tma_load_4d(sT + (uint32_t)(sl * S::BOXB), &map, 0, y0 - 1 + dy, x0 - 1, z0 - 1, smem_u32(&bfull[sl]));
+                    last = g;
+                }
+            }
+            // loads still in flight write shared memory: their barrier before the CTA may end
+            if (last >= 0 && !mbar_wait(smem_u32(&bfull[last % S::NB]), (uint32_t)((last / S::NB) & 1))) fail = true;
+            if (fail) *abort_flag = 1;
+        }
+    } else if (warp == 5) {
+        // ---- MMA issuer: one thread ----
+        if (lane == 0) {
+            long g = 0, last = -1;
+            int q = 0;
+            bool fail = false;
+            for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x, q++) {
+                const int b = q & 1, u = q >> 1;
+                // the accumulator was last read by the epilogue of tile q - 2
+                if (u >= 1 && !mbar_wait(smem_u32(&aempty[b]), (uint32_t)((u - 1) & 1))) { fail = true; break; }
+                const uint32_t acc = tmem + (uint32_t)(b * COUT);
+                for (int dy = 0; dy < 3; dy++, g++) {
+                    const int sl = (int)(g % S::NB);
+                    if (!mbar_wait(smem_u32(&bfull[sl]), (uint32_t)((g / S::NB) & 1))) { fail = true; break; }
+                    tc_fence_after();
+#pragma unroll
+                    for (int t9 = 0; t9 < 9; t9++) {
+                        const int dz = t9 / 3, dx = t9 % 3, tap = dz * 9 + dx * 3 + dy;
+                        const uint32_t sA = sT + (uint32_t)(sl * S::BOXB + (dz * kQx + dx) * 8 * S::ROWB);
+                        const uint32_t sB = sW + (uint32_t)(tap * S::TAPB);
+#pragma unroll
+                        for (int k = 0; k < CIN / 16; k++) {
+                            const uint64_t da = smem_desc(sA + (uint32_t)(32 * k), 16, 8 * S::ROWB) | S::ALAYOUT;
+                            const uint64_t db = smem_desc(sB + (uint32_t)(2 * k * COUT * 16), COUT * 16, 128);
+                            tc_mma(acc, da, db, S::IDESC, (dy > 0 || t9 > 0 || k > 0) ? 1u : 0u);
+                        }
+                    }
+                    // the slot is free once these MMAs complete
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&bempty[sl]))
+                                 : "memory");
+                    last = g;
+                }
+                if (fail) break;
+                // the accumulator is full once this tile's MMAs complete
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&afull[b]))
+                             : "memory");
+            }
+            // MMAs still in flight read the ring and write TMEM: wait for the last commit
+            if (last >= 0 && !mbar_wait(smem_u32(&bempty[last % S::NB]), (uint32_t)((last / S::NB) & 1))) fail = true;
+            if (fail) *abort_flag = 1;
+        }
+    } else {
+        // ---- epilogue warps 0-3: TMEM lane m = row (tx = m / 8, ty = m % 8) of the tile ----
+        const int m = tid, ox = m >> 3, oy = m & 7;
+        int q = 0;
+        bool fail = false;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, q++) {
+            const int b = q & 1, u = q >> 1;
+            if (!mbar_wait(smem_u32(&afull[b]), (uint32_t)(u & 1))) fail = true;
+            if (__any_sync(0xffffffffu, fail)) { fail = true; break; }   // tcgen05.ld is warp-collective
+            tc_fence_after();
+            float v[COUT];
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float t16[16];
+                tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * COUT + c0), t16);
+#pragma unroll
+                for (int e = 0; e < 16; e++) v[c0 + e] = t16[e];
+            }
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&aempty[b])) : "memory");
+            int z0, x0, y0;
+            origin(tile, z0, x0, y0);
+            const int zz = z0, xx = x0 + ox, yy = y0 + oy;
+            if (zz > a.d.nz || xx > a.d.nx || yy > a.d.ny) continue;
+            const long p = (long)zz * XY + (long)xx * a.d.Y + yy;
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 8) {
+                float f[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) f[e] = v[c0 + e] + (a.bias ? a.bias[c0 + e] : 0.0f);
+                if (a.add) {
+                    float h[8];
+                    unpack8(*reinterpret_cast<const uint4 *>(a.add + p * COUT + c0), h);
+#pragma unroll
+                    for (int e = 0; e < 8; e++) f[e] += h[e];
+                }
+                if (a.relu) {
+#pragma unroll
+                    for (int e = 0; e < 8; e++) f[e] = fmaxf(f[e], 0.0f);
+                }
+                if (a.mask) {
+                    float h[8];
+                    unpack8(*reinterpret_cast<const uint4 *>(a.mask + p * COUT + c0), h);
+#pragma unroll
+                    for (int e = 0; e < 8; e++) f[e] = h[e] > 0.0f ? f[e] : 0.0f;
+                }
+                if (a.out) *reinterpret_cast<uint4 *>(a.out + p * COUT + c0) = pack8(f);
+                if (a.out32) {
+                    *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0) = make_float4(f[0], f[1], f[2], f[3]);
+                    *reinterpret_cast<float4 *>(a.out32 + p * COUT + c0 + 4) = make_float4(f[4], f[5], f[6], f[7]);
+                }
+            }
+        }
         if (fail) *abort_flag = 1;
     }
     __syncthreads();
@@ -1226,11 +1460,66 @@ cudaError_t launch_brick_t(const ConvArgs &a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// The brick kernel takes the layers with 16 or 32 channels in and out (the fine levels, most of
-// the network's time); k_conv_tc the wider ones.  I3G_CONV_BRICK=0 sends every layer to k_conv_tc.
+// cuTensorMapEncodeTiled of the driver, looked up once through the runtime (the library links
+// only the runtime); null when the driver does not offer it
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+// TMA-fed kernel: a 4-D tensor map (channels, y, x, z) over the input with a 32-byte (16 channels)
+// or 64-byte (32 channels) swizzle; rows past the array's ends load as zeros.  Without the driver
+// entry point (or with an input that is not 16-byte aligned) the layer goes to the brick kernel.
+template <int CIN, int COUT>
+cudaError_t launch_tma_t(const ConvArgs &a, cudaStream_t st)
+{
+    using S = TmaShape<CIN, COUT>;
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc || (reinterpret_cast<uintptr_t>(a.in) & 15u)) return launch_brick_t<CIN, COUT>(a, st);
+    static LaunchSetup cache[kMaxDev];
+    LaunchSetup ls;
+    if (cudaError_t e = persistent_setup(k_conv_tma<CIN, COUT>, S::SMEM, 8, cache, ls)) return e;
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    const cuuint64_t dim[4] = {(cuuint64_t)CIN, (cuuint64_t)a.d.Y, (cuuint64_t)a.d.X, (cuuint64_t)a.d.Z};
+    const cuuint64_t stride[3] = {(cuuint64_t)CIN * 2, (cuuint64_t)a.d.Y * CIN * 2, (cuuint64_t)a.d.X * a.d.Y * CIN * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)CIN, (cuuint32_t)kQy, (cuuint32_t)kQx, (cuuint32_t)kQz}, estr[4] = {1, 1, 1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.in, dim, stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CIN == 16 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const int ntx = (a.d.nx + kTx - 1) / kTx, nty = (a.d.ny + kTy - 1) / kTy, ntz = (a.d.nz + kTz - 1) / kTz;
+    const int ntiles = ntx * nty * ntz;
+    const int grid = std::min(ntiles, ls.sms * ls.per_sm);
+    if (grid < 1) return cudaSuccess;
+    k_conv_tma<CIN, COUT><<<grid, kTmaThreads, S::SMEM, st>>>(map, a, ntx, nty, ntiles);
+    return cudaGetLastError();
+}
+
+// Layers with 16 or 32 channels in and out (the fine levels, most of the network's time) go to the
+// TMA-fed kernel (I3G_CONV_TMA=0: the brick kernel; with I3G_CONV_BRICK=0 as well: k_conv_tc); the
+// wider ones to k_conv_tc.
 cudaError_t launch_conv(int cin, int cout, const ConvArgs &a, cudaStream_t st)
 {
     static const bool brick = !getenv("I3G_CONV_BRICK") || atoi(getenv("I3G_CONV_BRICK")) != 0;
+    static const bool tma = !getenv("I3G_CONV_TMA") || atoi(getenv("I3G_CONV_TMA")) != 0;
+    if (tma) {
+#define I3G_TMA_CASE(I, O) \
+        if (cin == I && cout == O) return launch_tma_t<I, O>(a, st);
+        I3G_TMA_CASE(16, 16) I3G_TMA_CASE(16, 32) I3G_TMA_CASE(32, 16) I3G_TMA_CASE(32, 32)
+#undef I3G_TMA_CASE
+    }
     if (brick) {
 #define I3G_BRICK_CASE(I, O) \
         if (cin == I && cout == O) return launch_brick_t<I, O>(a, st);
@@ -1934,8 +2223,11 @@ int i3g_unet_time(i3g_unet *u, int reps, double *ms_train, double *ms_forward)
     cudaEvent_t e0 = ev.a, e1 = ev.b;
     const int slot = 0;
     const long n = u->L[0].n;
-    int rc = 0;
     float ms = 0;
+    // one untimed pass first: the first launch of each kernel loads its module and sets its attributes
+    int rc = load_sample(u, u->ds_in + slot * kInCh * n);
+    if (!rc) rc = forward(u);
+    if (rc) return rc;
     UCHK(cudaEventRecord(e0, u->st));
     for (int r = 0; r < reps && !rc; r++) {
         if ((rc = load_sample(u, u->ds_in + slot * kInCh * n))) break;

@@ -176,9 +176,10 @@ def summarize(rows):
     return out
 
 
-def bench(n: int, reps: int = 10):
-    """Device times of the network on an n^3 grid: forward pass, training step, and every
-    forward convolution with its achieved bandwidth (algorithmic bytes / time)."""
+def bench(n: int, reps: int = 10, layers=None, convs_only: bool = False):
+    """Device times of the network on an n^3 grid: forward pass, training step (unless
+    ``convs_only``), and each forward convolution in ``layers`` (default all) with its achieved
+    bandwidth (algorithmic bytes / time)."""
     net = UNet(n, n, n, capacity=1, seed=1)
     N = n ** 3
     g = np.linspace(0.0, 1.0, n)
@@ -188,9 +189,9 @@ def bench(n: int, reps: int = 10):
     tg4 = np.stack([1e6 * np.sin(2 * xx + yy).ravel()] + [1e-10 * np.cos(k + 3 * yy).ravel() for k in range(3)]).astype(np.float32)
     net.set_scales(21.0, 0.5, 3300.0, 0.02, 1e-10, 1e6)
     net.set_sample(0, in5, tg4)
-    ms_train, ms_fwd = net.time(reps)
+    ms_train, ms_fwd = net.time(reps) if not convs_only else (None, None)
     convs = []
-    for layer in range(15):
+    for layer in (range(15) if layers is None else layers):
         ms, by = net.time_conv(layer, 3 * reps)
         convs.append({"layer": layer, "ms": ms, "bytes": by, "gbs": by / (ms * 1e-3) / 1e9})
     net.close()
@@ -200,6 +201,9 @@ def bench(n: int, reps: int = 10):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--bench", type=int, default=0, help="only time the network on an N^3 grid")
+    ap.add_argument("--layers", default=None, help="with --bench: comma list of the convolutions to time")
+    ap.add_argument("--reps", type=int, default=10, help="with --bench: timed repetitions")
+    ap.add_argument("--convs-only", action="store_true", help="with --bench: skip the forward and training times")
     ap.add_argument("--n", type=int, default=33)
     ap.add_argument("--mnum", type=int, default=2)
     ap.add_argument("--train", type=int, default=48, help="training seeds")
@@ -213,7 +217,8 @@ def main(argv=None):
     import torch
     torch.cuda.set_device(0)
     if a.bench:
-        print(json.dumps(bench(a.bench)))
+        layers = [int(v) for v in a.layers.split(",")] if a.layers else None
+        print(json.dumps(bench(a.bench, a.reps, layers, a.convs_only)))
         return 0
     case = Case(n=a.n, mnum=a.mnum)
     nsamp = a.train * a.steps
