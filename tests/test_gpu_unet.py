@@ -46,6 +46,42 @@ def test_conv_matches_oracle(cin, cout):
     assert not np.any(halo)
 
 
+@pytest.mark.parametrize("cin,cout", [(16, 16), (32, 16), (32, 32)])
+def test_conv_many_tiles_per_cta(cin, cout):
+    """64 x 49 x 33 nodes = 1280 output tiles of 1 x 16 x 8 (4 x 5 x 64, partial in x and y): every
+    persistent CTA of the TMA-fed kernel walks four or more tiles, so its box slots and both TMEM
+    accumulators are reused many times."""
+    from i3elvis_b200 import warmstart as W
+    rng = np.random.default_rng(7 + cin * 100 + cout)
+    dims = (64, 49, 33)
+    x = U.bf16(rng.normal(size=dims + (cin,)))
+    w = U.bf16(rng.normal(0, 1 / np.sqrt(27 * cin), size=(27, cout, cin)))
+    b = rng.normal(0, 0.1, size=cout).astype(np.float32)
+    add = U.bf16(rng.normal(0, 0.5, size=dims + (cout,)))
+    out = W.conv_host(cin, cout, dims, U.bf16_bits(_rows(x)), U.bf16_bits(w), b, U.bf16_bits(_rows(add)), relu=True)
+    ref = np.maximum(U.conv3(x, w, b.astype(np.float64)) + add, 0.0)
+    got = out.reshape(dims[0] + 2, dims[1] + 2, dims[2] + 2, cout)
+    assert np.max(np.abs(got[1:-1, 1:-1, 1:-1] - ref)) <= 2e-5 * np.max(np.abs(ref)) + 1e-6
+    halo = got.copy()
+    halo[1:-1, 1:-1, 1:-1] = 0
+    assert not np.any(halo)
+
+
+def test_conv_brick_fallback_matches_oracle():
+    """The same parity cases on the brick kernel, the path taken when the driver offers no
+    tensor-map encoder (I3G_CONV_TMA=0), in a child process: the switch is read once per process."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, I3G_CONV_TMA="0")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider", os.path.abspath(__file__),
+                        "-k", "test_conv_matches_oracle or test_conv_many_tiles_per_cta"],
+                       cwd=root, env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout and "skipped" not in r.stdout.splitlines()[-1], r.stdout[-500:]
+
+
 @pytest.mark.parametrize("cin,cout", PAIRS)
 def test_wgrad_matches_oracle(cin, cout):
     """Weight and bias gradients of one layer (tcgen05 for 16/32 channels, CUDA cores for the
