@@ -37,6 +37,7 @@
 // All waits on mbarriers are bounded (2 s); a timeout sets an error flag read by the host.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -1402,6 +1403,7 @@ void tap_offsets(const Dims &d, int *off)
 // 512 TMEM columns and 128 threads of fewer than 96 registers, which bind less)
 struct LaunchSetup { int sms = 0, per_sm = 0; };
 constexpr int kMaxDev = 64;
+std::mutex g_setup_mu;   // the per-device set-up caches may be filled from several host threads
 
 template <typename K>
 cudaError_t persistent_setup(K kernel, int smem, int max_per_sm, LaunchSetup (&cache)[kMaxDev], LaunchSetup &out)
@@ -1410,6 +1412,7 @@ cudaError_t persistent_setup(K kernel, int smem, int max_per_sm, LaunchSetup (&c
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_setup_mu);
     LaunchSetup &c = cache[dev];
     if (!c.per_sm) {
         if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
@@ -1434,10 +1437,13 @@ cudaError_t launch_conv_t(const ConvArgs &a, cudaStream_t st)
     cudaError_t e0 = cudaGetDevice(&dev);
     if (e0 != cudaSuccess) return e0;
     if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
-    if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
-        if (e != cudaSuccess) return e;
-        attr[dev] = true;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        if (!attr[dev]) {
+            cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+            if (e != cudaSuccess) return e;
+            attr[dev] = true;
+        }
     }
     k_conv_tc<CIN, COUT><<<nblk(a.d.np, kTileM), 128, S::SMEM, st>>>(a);
     return cudaGetLastError();
