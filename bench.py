@@ -142,46 +142,103 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clock, power and clock-event (throttle) reasons sampled during the timed region: NVML
+    read-only queries every 20 ms from a thread, else nvidia-smi every 200 ms.  Nothing is set."""
+    PERIOD_S = 0.02
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, dev):
-        self.dev = dev
+    def __init__(self, dev, nvml=None):
+        self.dev = dev          # CUDA device index
+        self.nvml = nvml        # an NVML module (pynvml when None)
         self.proc = None
         self.file = None
+        self.thread = None
+        self.rows = []          # (sm MHz, max sm MHz, W, [4 reason flags])
+
+    def _nvml_index(self):
+        """NVML index of the CUDA device (CUDA_VISIBLE_DEVICES may renumber the devices)."""
+        try:
+            import torch
+            return int(torch.cuda._get_nvml_device_index(self.dev))
+        except Exception:
+            return self.dev
+
+    def _start_nvml(self):
+        try:
+            nv = self.nvml
+            if nv is None:
+                import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self._nvml_index())
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = [getattr(nv, "nvmlClocksEventReason" + k, d) for k, d in
+                    (("HwSlowdown", 0x8), ("HwThermalSlowdown", 0x40), ("SwThermalSlowdown", 0x20), ("SwPowerCap", 0x4))]
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def sample():
+                m = int(reasons(h))
+                return (float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), smax, nv.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                        ["Active" if m & b else "Not Active" for b in bits])
+            sample()            # a failing query falls back to nvidia-smi here, not in the thread
+        except Exception:
+            return False
+        self._nv, self._stop = nv, threading.Event()
+
+        def run():
+            while True:
+                try:
+                    self.rows.append(sample())
+                except Exception:
+                    pass
+                if self._stop.wait(self.PERIOD_S):
+                    break
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        return True
 
     def start(self):
-        if not shutil.which("nvidia-smi"):
+        self.rows = []
+        if self._start_nvml() or not shutil.which("nvidia-smi"):
             return
         self.file = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
-        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self._nvml_index()), f"--query-gpu={self.Q}",
                                       "--format=csv,noheader,nounits", "-lms", "200"],
                                      stdout=self.file, stderr=subprocess.DEVNULL)
 
     def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        self.proc.wait()
-        self.file.flush()
-        rows = []
-        with open(self.file.name) as fh:
-            for line in fh:
-                f = [x.strip() for x in line.split(",")]
-                if len(f) >= 7:
-                    try:
-                        rows.append((float(f[0]), float(f[1]), float(f[2]), f[3:7]))
-                    except ValueError:
-                        pass
-        os.unlink(self.file.name)
+        source = None
+        if self.thread:
+            self._stop.set()
+            self.thread.join()
+            try:
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
+            source = "nvml"
+        elif self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.file.flush()
+            with open(self.file.name) as fh:
+                for line in fh:
+                    f = [x.strip() for x in line.split(",")]
+                    if len(f) >= 7:
+                        try:
+                            self.rows.append((float(f[0]), float(f[1]), float(f[2]), f[3:7]))
+                        except ValueError:
+                            pass
+            os.unlink(self.file.name)
+            source = "nvidia-smi"
+        rows = self.rows
         if not rows:
             return None
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        reasons = sorted({self.NAMES[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
         return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
-                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons, "source": source}
 
 
 # titerate (heat3mg.c:463-560) repeats its iteration block until heatsum <= HEATMIN, which its
