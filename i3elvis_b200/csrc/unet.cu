@@ -25,15 +25,19 @@
 // implicit GEMM: D[128 rows][Cout] = sum over 27 taps and Cin of A_tap[128 rows][Cin] *
 // W_tap[Cin][Cout], with A_tap a contiguous block of 128 rows shifted by the tap's offset.
 //
-// Convolution kernel (forward and input gradient): one CTA per 128-row tile, four warps.
-// Operand tiles are staged with cp.async (zero fill outside the array) in a 4-deep ring,
-// 1024-byte aligned, in the canonical no-swizzle K-major layout of the tensor core (8 rows x
-// 16 B core matrices),
-// one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = 128, N = Cout, K = 16)
-// into a TMEM accumulator and tcgen05.commit signals the stage's mbarrier; the epilogue reads
-// TMEM with tcgen05.ld (warp w owns rows 32w..32w+31), adds bias and the skip tensor,
-// applies ReLU or the ReLU mask of the backward pass and stores BF16 (FP32 for tests).
-// Weight gradients are FP32 CUDA-core reductions (27 x Cout x Cin outputs over all rows).
+// Convolution kernels (forward and input gradient; tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in
+// TMEM, M = 128 rows, N = Cout, K = 16; the epilogue reads TMEM with tcgen05.ld, adds bias and
+// the skip tensor, applies ReLU or the ReLU mask of the backward pass and stores BF16, or FP32
+// for tests):
+//   k_conv_tma   16/32 channels in and out (the fine levels, most of the time): persistent CTAs,
+//                TMA boxes of a 4-D tensor map in the swizzled K-major operand layout, a ring of
+//                box stages, one MMA thread, two TMEM accumulators, four epilogue warps;
+//   k_conv_brick the same channel counts when no tensor-map encoder is available: producer warps
+//                gather taps from a cp.async brick into no-swizzle operand stages;
+//   k_conv_tc    wider layers: one CTA per 128-row tile, each tap's shifted block staged with
+//                cp.async (zero fill outside the array) in a 4-deep ring.
+// Weight gradients: k_wgrad_tc on the tensor cores for 16/32 channels (MN-major operands, a
+// partial sum per CTA, k_wgrad_reduce), FP32 CUDA-core reductions (k_wgrad) for the rest.
 // All waits on mbarriers are bounded (2 s); a timeout sets an error flag read by the host.
 #include <cmath>
 #include <cstring>
