@@ -6,13 +6,20 @@
 // The marker -> node pass gives each CTA one tile and each warp one cell: the warp computes
 // its markers' properties, then sums them per node of the cell in registers, and adds the
 // per-cell sums to the tile's FP64 node sums in shared memory in 8 parity classes of cells
-// that share no node -- no atomics inside the tile.  The reference's scatter
-// (mark3mg.c:848-924) adds into shared node arrays from many threads without atomics; here
-// the only atomics are the global ones for nodes on tile faces, once per tile.  An
-// original-index array lets downloads return markers in the reference's order.
+// that share no node -- no atomics inside the tile.  Each tile writes its box of node sums to
+// a staging buffer and k_r2n_gather adds, per node, the boxes of the tiles holding it in a
+// fixed order: no atomics at all, the same sums on every run.  The reference's scatter
+// (mark3mg.c:848-924) adds into shared node arrays from many threads without atomics.  The
+// only atomics of the file are the counters of the (tile, cell) sort.  An original-index
+// array lets downloads return markers in the reference's order.
 //
-// This file is compiled with -fmad=false so that the interpolation arithmetic rounds like
-// the CPU restatement (transcendentals may still differ in the last unit).
+// Two arithmetic variants of the interpolation and rheology (template parameter EX, chosen by
+// i3g_params.marker_exact): the reference's operation order (EX = true), and reciprocal tables,
+// distance-form weights, factorised trilinear sums and explicit fused multiply-adds (EX = false,
+// about twice as fast).  This file is compiled with -fmad=false so that the exact variant
+// rounds like the CPU restatement (transcendentals may still differ in the last unit); the fast
+// variant's fused operations are written out.
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
