@@ -11,6 +11,15 @@
 // FP64 arithmetic uses explicitly rounded operations in the reference's operand order, so
 // rows, residuals and relaxation updates agree bit for bit with the CPU oracle.  The FP32
 // path (mixed precision) uses the same stencil code on viscosity and geometry scaled to O(1).
+//
+// Solve drivers (stokes_solve): the reference's FP64 V-cycle iteration; FP32 V-cycles inside
+// FP64 defect correction; or FGMRES(m) (i3g_params.krylov) with the FP32 V-cycle as the
+// preconditioner and fused Gram-Schmidt kernels (k_kr_proj).  The FP32 smoother's pressure
+// update of weak cells enclosed by stiff material is scaled by their faces' viscosity
+// (k_nd_schur).  The start is the previous solution, its linear or quadratic extrapolation
+// (k_extrapolate3), or a staged learned correction, whichever has the smaller residual.  An
+// iteration (and each FGMRES step index) is captured as a CUDA graph and replayed, captured
+// again only when the level count, the precision or the relaxation factors change.
 #include <algorithm>
 #include <type_traits>
 #include <cmath>
