@@ -450,8 +450,9 @@ def main():
         log(f"plain FP64 multigrid: {s64:.1f} ms Stokes+heat per step, this run {s32:.1f} ms")
 
     # rooflines of the step's main kernels, each timed live with an empty L2 before every launch
-    # (library's cold-cache timer) against the algorithmic bytes of SURVEY section 8(d); the
-    # dominant kernel is the one with the most device time per step
+    # (library's cold-cache timer) against each kernel's algorithmic bytes per unit (marker,
+    # node) times the units of one launch; the dominant kernel is the one with the most device
+    # time per step
     peak, peak_src = peaks()
     traffic_tab = {}
     tf = os.path.join(ROOT, "profiles", "traffic.json")
