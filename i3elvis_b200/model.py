@@ -310,6 +310,59 @@ def make_prn(spec: ModelSpec, rocks: dict, types: np.ndarray, marks_xyz, seed: i
     return Prn(head, rtab, nodes, gx, gy, gz, bond, marks)
 
 
+def write_init_t3c(path, spec: ModelSpec, rocks: dict, background: int, bodies, boxes, out_name="init0.prn") -> None:
+    """Write the model as the reference's ``init.t3c`` (read by ``in3mg.c:64-956``), so that the
+    reference's own initial-condition program builds the same first ``.prn`` as ``make_prn``:
+
+    * grid parameters and marker jitter (``in3mg.c:69-91``; ``spec.nonstab`` = 0 places the
+      markers on the regular sub-grid, the reference's jitter draws ``rand()``),
+    * no data file to reload, the output file ``out_name`` (binary),
+    * the rock table, one row of the 24 columns of ``ROCK_FIELDS`` per type (``in3mg.c:201-236``),
+    * the boundary-condition boxes ``boxes`` (``BcBox``; ``in3mg.c:242-300``) with absolute node
+      indices,
+    * the rock bodies: first a box of rock ``background`` around the whole model (a marker in no
+      body keeps type 0 in the reference), then ``bodies`` in order (``abi.Body`` records as
+      ``i3g_init_markers`` takes them: shape 0 box ``n``, 1 ellipsoid ``sn``, 2 cylinder ``cn``;
+      ``in3mg.c:548-797``),
+    * one temperature box of type 0 over the model, ``spec.t_top`` at y = 0 and
+      ``spec.t_bottom`` at y = ysize (``in3mg.c:801-955``).
+    """
+    nx, ny, nz = spec.shape
+    f = repr
+    L = ["/grid_PARAMETERS_DESCRIPTIONS"]
+    L += [str(nx), str(ny), str(nz)] + [str(m) for m in spec.mnum]
+    L += [f(float(v)) for v in spec.size] + [str(v) for v in spec.pinit_cell]
+    L += [f(float(spec.pinit))] + [f(float(g)) for g in spec.gravity] + ["0.0"]
+    L += [f"{int(spec.nonstab)} {f(float(spec.jitter))} {f(float(spec.jitter))} {f(float(spec.jitter))}", ""]
+    L += ["/MARKERS_TYPES_FILE_NAME_Y(Name)_N(0)", "0", "/DATA_OUTPUT_FILE_NAME____TYPE", f"{out_name} b", ""]
+    L += ["/ROCKS_DESCRIPTIONS"]
+    for t in sorted(rocks):
+        L.append(f"{t} " + " ".join(f(float(getattr(rocks[t], c))) for c in ROCK_FIELDS))
+    L += ["~", "/BONDARY_CONDITIONS_DESCRIPTIONS"]
+    for b in boxes:
+        row = f"{b.var} {b.x0} {b.x1} {b.y0} {b.y1} {b.z0} {b.z1} {f(float(b.c))} {f(float(b.k))}"
+        if b.k:
+            row += " {} {} {}".format(*b.shift)
+        L.append(row + " 0 0")
+    L += ["~", "/ROCKS_BOXES_DESCRIPTION"]
+
+    def body_row(tok, ex, e, xs, ys, zs):
+        pts = " ".join(f"{f(float(xs[n]))} {f(float(ys[n]))} {f(float(zs[n]))}" for n in range(8))
+        return f"{tok} {f(float(ex))} {f(float(e))} {pts}"
+    lo, hi = -0.1, 1.1
+    L.append(body_row(str(background), 0.0, 0.0, [hi if n & 2 else lo for n in range(8)],
+                      [hi if n & 1 else lo for n in range(8)], [hi if n & 4 else lo for n in range(8)]))
+    for b in bodies:
+        tok = {0: "", 1: "s", 2: "c"}[b.shape] + str(b.rock)
+        L.append(body_row(tok, b.ex, b.e, list(b.x), list(b.y), list(b.z)))
+    L += ["~", "/TEMPERATURE_BOXES_TYPE_x0_x2_y0_y1_y2_y3_z0_x5_x7_y4_y5_y6_y7_z7_T0..T7"]
+    tt, tb = f(float(spec.t_top)), f(float(spec.t_bottom))
+    L.append("0 0 1 0 1 0 1 0 0 1 0 1 0 1 1 " + " ".join([tt, tb] * 4))
+    L += ["~", ""]
+    with open(path, "w") as fh:
+        fh.write("\n".join(L))
+
+
 # ---------------------------------------------------------------------------------------
 # Named workloads
 # ---------------------------------------------------------------------------------------
@@ -318,15 +371,17 @@ INCLUSION_TYPES = (3, 4, 5, 6, 9, 10, 11, 12, 13, 14, 15, 19)
 
 
 def sinking_sphere(n=33, size_km=100.0, mnum=3, multinum=2, seed=1, radius_km=20.0, stretch=0.0,
-                   sphere_rho=3400.0, centre_frac=(0.5, 0.5, 0.5), plastic=None):
+                   sphere_rho=3400.0, centre_frac=(0.5, 0.5, 0.5), plastic=None, nonstab=100):
     """Plain sinking sphere: eta 1e23 / rho 3400 sphere in eta 1e21 / rho 3300 matrix,
     g = 10 along the vertical, free slip, linear T 273 -> 1573 K, k = 3, cp = 1000.
 
     ``stretch`` makes the grid lines non-uniform (see ``_grid``); ``plastic = (a, b)`` gives the
     matrix Drucker-Prager yielding sigma_y = a + b P (rock columns a0 = a1 = a, b0 = b1 = b,
-    viscalc's brittle branch, mark3mg.c:1148-1198)."""
+    viscalc's brittle branch, mark3mg.c:1148-1198); ``nonstab = 0`` leaves the markers on the
+    regular sub-grid."""
     L = size_km * 1e3
-    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum, stretch=stretch)
+    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum, stretch=stretch,
+                     nonstab=nonstab)
     xyz = build_markers(spec, seed)
     x, y, z = (a.astype(np.float64) for a in xyz)
     c = [f * L for f in centre_frac]
