@@ -213,6 +213,7 @@ class ModelSpec:
     t_bottom: float = 1573.0
     multinum: int = 2
     stretch: float = 0.0     # 0: uniform grid lines; a in (0, 1): spacing (1 - a cos(2 pi s)) * size/(n-1)
+    spheres: tuple = ()      # (rock, (x, y, z) centre in metres, radius in metres) of the bodies, in order
 
 
 def _grid(n, size, stretch=0.0):
@@ -397,14 +398,15 @@ def sinking_sphere(n=33, size_km=100.0, mnum=3, multinum=2, seed=1, radius_km=20
 
 def random_inclusions(n=129, size_km=200.0, mnum=3, multinum=4, seed=7, count=100,
                       r_km=(2.0, 8.0), rho=(3250.0, 3450.0), contrast=None,
-                      arrhenius=True, activation=5e5, eta_ref=1e21, t_ref=923.0):
+                      arrhenius=True, activation=5e5, eta_ref=1e21, t_ref=923.0, nonstab=100):
     """Random spherical inclusions in an Arrhenius matrix.
 
     Inclusion centres, radii and densities are seeded; densities (and, when ``contrast``
     is given, log-uniform viscosity contrasts up to ``contrast``) are binned into at most
-    12 rock types because the reference keeps rock properties per type."""
+    12 rock types because the reference keeps rock properties per type.  ``nonstab = 0`` leaves
+    the markers on the regular sub-grid."""
     L = size_km * 1e3
-    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum)
+    spec = ModelSpec(shape=(n, n, n), size=(L, L, L), mnum=(mnum,) * 3, multinum=multinum, nonstab=nonstab)
     rng = np.random.default_rng(seed)
     cen = rng.uniform(0.1 * L, 0.9 * L, size=(count, 3))
     rad = rng.uniform(r_km[0] * 1e3, r_km[1] * 1e3, size=count)
@@ -436,6 +438,8 @@ def random_inclusions(n=129, size_km=200.0, mnum=3, multinum=4, seed=7, count=10
         idx = markers_in_box(spec, cen[i] - r, cen[i] + r)
         d2 = ((x[idx] - cen[i, 0]) ** 2 + (y[idx] - cen[i, 1]) ** 2 + (z[idx] - cen[i, 2]) ** 2)
         types[idx[d2 <= r * r]] = INCLUSION_TYPES[tbin[i]]
+    spec = dataclasses.replace(spec, spheres=tuple((INCLUSION_TYPES[tbin[i]], tuple(float(v) for v in cen[i]),
+                                                    float(rad[i])) for i in range(count)))
     return make_prn(spec, rocks, types, xyz, seed), spec
 
 

@@ -37,7 +37,7 @@ def _in3mg(d, spec, rocks, background, bodies, boxes, mode):
     M.write_init_t3c(os.path.join(d, "init.t3c"), spec, rocks, background, bodies, boxes)
     config.write_mode(os.path.join(d, "mode.t3c"), mode)
     config.write_file_t3c(os.path.join(d, "file.t3c"), 0)
-    r = subprocess.run([IN3MG], cwd=d, capture_output=True, text=True, timeout=600, stdin=subprocess.DEVNULL,
+    r = subprocess.run([IN3MG], cwd=d, capture_output=True, text=True, timeout=3600, stdin=subprocess.DEVNULL,
                        env=dict(os.environ, OMP_NUM_THREADS="1"))
     assert r.returncode == 0 and "OK!" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
     return os.path.join(d, "init0.prn"), P.read_prn(os.path.join(d, "init0.prn"))
@@ -86,6 +86,62 @@ def test_model_builder_gives_the_reference_first_prn(tmp_path):
         assert np.array_equal(ref.nodes[f], prep.nodes[f]), f
     for f in P.MARK_FIELDS + ("t",):
         assert np.array_equal(ref.marks[f], prep.marks[f]), f
+    with open(ref_path, "rb") as fa, open(str(b / "prep.prn"), "rb") as fb:
+        assert fa.read() == fb.read()
+
+
+def _full_case():
+    """The benchmark's own configuration (129^3 nodes, 27 markers per cell = 56.6 M markers, 100
+    inclusions, four coarse levels), without jitter: minutes of CPU time and about 12 GB of memory,
+    so only with I3G_IN3MG_FULL=1."""
+    sys.path.insert(0, ROOT)
+    import bench
+    w = bench.WORKLOADS["incl129"]
+    return pytest.param(w["n"], w["mnum"], w["multinum"], w["seed"], w["count"], (2.0, 8.0), id="incl129",
+                        marks=pytest.mark.skipif(not os.environ.get("I3G_IN3MG_FULL"),
+                                                 reason="full-size check: set I3G_IN3MG_FULL=1"))
+
+
+@pytest.mark.parametrize("n,mnum,multinum,seed,count,r_km", [(17, 2, 2, 5, 8, (15.0, 35.0)),
+                                                             (33, 2, 3, 7, 100, (2.0, 8.0)), _full_case()])
+def test_inclusion_builder_gives_the_reference_first_prn(tmp_path, n, mnum, multinum, seed, count, r_km):
+    """The benchmark's model family (``model.random_inclusions``: Arrhenius matrix, seeded
+    spherical inclusions binned into 12 rock types, 200 km cube), at 17^3 with 8 inclusions, at
+    33^3 with the benchmark's 100 inclusions of 2-8 km and (opt-in) at the benchmark's full size:
+    builder + the reference's initial passes == the reference's initial-condition program, byte
+    for byte."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cases
+    import oracle as O
+    from i3elvis_b200 import abi, config, model as M, prn as P
+    _, mode = cases.build("incl17")
+    mode.multinum = multinum
+    mode.multinnn = (tuple([8] * multinum + [0]), tuple([8] * multinum + [32]))
+    mode.files[0].multinum = mode.files[0].multinum2 = multinum
+    ours, spec = M.random_inclusions(n=n, size_km=200.0, mnum=mnum, multinum=multinum, seed=seed, count=count,
+                                     r_km=r_km, nonstab=0)
+    L = spec.size[0]
+    assert len(spec.spheres) == count
+    bodies = [abi.sphere_body(t, tuple(c / L for c in cen), (r / L,) * 3) for t, cen, r in spec.spheres]
+    types = [int(t) for t in np.nonzero(ours.rocks["ro"])[0]]
+    a = tmp_path / "in3mg"
+    a.mkdir()
+    ref_path, ref = _in3mg(str(a), spec, _rocks_of(ours, types), M.MATRIX, bodies,
+                           M.free_slip_boxes(n, n, n, spec.t_top, spec.t_bottom), mode)
+    assert np.count_nonzero(ref.marks["t"] != M.MATRIX) > 1000
+    b = tmp_path / "ours"
+    b.mkdir()
+    P.write_prn(str(b / "in0.prn"), ours)
+    mode.infile = "in0.prn"
+    config.write_mode(str(b / "mode.t3c"), mode)
+    config.write_file_t3c(str(b / "file.t3c"), 0)
+    O.run_reference(str(b), "prepare", "prep.prn")
+    prep = P.read_prn(str(b / "prep.prn"))
+    for f in P.MARK_FIELDS + ("t",):
+        assert np.array_equal(ref.marks[f], prep.marks[f]), f
+    for f in P.NODE_FIELDS:
+        assert np.array_equal(ref.nodes[f], prep.nodes[f]), f
     with open(ref_path, "rb") as fa, open(str(b / "prep.prn"), "rb") as fb:
         assert fa.read() == fb.read()
 
