@@ -48,18 +48,24 @@ def _rocks_of(p, types):
     return {t: M.Rock(**{f: float(p.rocks[f][t]) for f in P.ROCK_FIELDS}) for t in types}
 
 
-def test_model_builder_gives_the_reference_first_prn(tmp_path):
-    """The 17^3 sinking sphere (4 multigrid levels): builder + the reference's initial passes ==
-    the reference's initial-condition program, byte for byte."""
+@pytest.mark.parametrize("case", ["sphere17", "dp17"])
+def test_model_builder_gives_the_reference_first_prn(tmp_path, case):
+    """The 17^3 sinking sphere (4 multigrid levels), and the one of the Drucker-Prager fixture
+    (yielding matrix, dense sphere): builder + the reference's initial passes == the reference's
+    initial-condition program, byte for byte."""
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cases
     import oracle as O
     from i3elvis_b200 import abi, config, model as M, prn as P
-    _, mode = cases.build("sphere17")
+    _, mode = cases.build(case)
+    c = cases.CASES[case]
     n, L, R = 17, 100e3, 20e3
-    ours, spec = M.sinking_sphere(n=n, mnum=2, multinum=mode.multinum, seed=3, radius_km=R / 1e3, nonstab=0)
-    bodies = [abi.sphere_body(M.SPHERE, (0.5, 0.5, 0.5), (R / L,) * 3, 0.0, 1.0)]
+    ours, spec = M.sinking_sphere(n=n, mnum=2, multinum=mode.multinum, seed=c["seed"], radius_km=R / 1e3,
+                                  plastic=c.get("plastic"), sphere_rho=c.get("sphere_rho", 3400.0),
+                                  centre_frac=c.get("centre", (0.5, 0.5, 0.5)), nonstab=0)
+    centre = c.get("centre", (0.5, 0.5, 0.5))
+    bodies = [abi.sphere_body(M.SPHERE, centre, (R / L,) * 3, 0.0, 1.0)]
     boxes = M.free_slip_boxes(n, n, n, spec.t_top, spec.t_bottom)
     a = tmp_path / "in3mg"
     a.mkdir()
@@ -86,6 +92,11 @@ def test_model_builder_gives_the_reference_first_prn(tmp_path):
         assert np.array_equal(ref.nodes[f], prep.nodes[f]), f
     for f in P.MARK_FIELDS + ("t",):
         assert np.array_equal(ref.marks[f], prep.marks[f]), f
+    if c.get("plastic"):
+        # the Drucker-Prager columns (a0, a1, b0, b1) came through init.t3c into the compared table
+        a, bb = c["plastic"]
+        assert ref.rocks["a0"][M.MATRIX] == ref.rocks["a1"][M.MATRIX] == a
+        assert ref.rocks["b0"][M.MATRIX] == ref.rocks["b1"][M.MATRIX] == bb
     with open(ref_path, "rb") as fa, open(str(b / "prep.prn"), "rb") as fb:
         assert fa.read() == fb.read()
 
